@@ -1,0 +1,445 @@
+#!/usr/bin/env python3
+"""Benchmark of the TAL-SH tensor-algebra path on B200.
+
+Headline workload: the CCSD-like R8 contraction
+    D(a,b,i,j) += V(a,b,c,d) * T(c,d,i,j),  virtual extent 192, occupied 48
+(M = N_ab = 36864, N = 2304, K = 36864; 6.262e12 FLOP by TAL-SH's 2*M*N*K
+accounting), inputs seeded U[-1,1) with V scaled by 1/192, D = 0.  A "step" is
+one contraction by the chosen method (the library's plan selector).  The same
+line reports the plain FP64 TTGT form, the error against a double-double
+FP64 oracle on sampled elements, the permutation sweep (all 24 rank-4
+permutations of 256 MiB R8 and R4 tensors, bit-exact) in GB/s, the
+end-to-end rate through talshTensorContract with host-resident tensors, and
+the reference's OpenMP+BLAS CPU path timed on this host.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+       (N > 1: launched by torchrun, one process per GPU, replicas)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "contraction TFLOP/s + permute GB/s, chosen vs plain form at stated FP64 err"
+
+WORKLOADS = {
+    "ccsd1_r8": dict(pattern="D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)", v=192, o=48, dtk=8),
+    "ccsd2_r8": dict(pattern="D(a,i,b,j)+=W(a,k,c,i)*T(c,b,k,j)", v=192, o=48, dtk=8),
+    "ccsd1_r4": dict(pattern="D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)", v=192, o=48, dtk=4),
+}
+VIRT = set("abcd")
+
+
+def shapes(pattern, v, o):
+    import re
+    groups = re.findall(r"\(([^)]*)\)", pattern)
+    ext = lambda x: v if x in VIRT else o
+    return [[ext(x) for x in g.split(",")] for g in groups]
+
+
+def vol(dims):
+    n = 1
+    for x in dims:
+        n *= x
+    return n
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = os.environ.get("BENCH_DIST_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- GPU
+class ContractionCase:
+    """Device tensors of one contraction workload."""
+
+    def __init__(self, X, wl, stream):
+        import torch
+        self.X, self.wl, self.s = X, wl, stream
+        self.dd, self.ld, self.rd = shapes(wl["pattern"], wl["v"], wl["o"])
+        es = X.ELEM_BYTES[wl["dtk"]]
+        self.D = torch.empty(vol(self.dd) * es, dtype=torch.uint8, device="cuda")
+        self.L = torch.empty(vol(self.ld) * es, dtype=torch.uint8, device="cuda")
+        self.R = torch.empty(vol(self.rd) * es, dtype=torch.uint8, device="cuda")
+        X.fill_uniform(wl["dtk"], vol(self.ld), self.L.data_ptr(), 1, stream=stream)
+        X.fill_uniform(wl["dtk"], vol(self.rd), self.R.data_ptr(), 2, stream=stream)
+        X.tensor_scale(wl["dtk"], vol(self.ld), self.L.data_ptr(), 1.0 / wl["v"], stream=stream)
+        X.tensor_init(wl["dtk"], vol(self.dd), self.D.data_ptr(), 0.0, stream=stream)
+        cp, *_ = X.parse_pattern(wl["pattern"])
+        self.cptrn = cp
+        self.flops = 2.0 * vol(self.dd) * (vol(self.ld) * vol(self.rd) / vol(self.dd)) ** 0.5
+
+    def run(self, method, accumulative=True):
+        X = self.X
+        X.tensor_contract(self.cptrn, self.wl["dtk"], self.dd, self.D.data_ptr(), self.ld, self.L.data_ptr(),
+                          self.rd, self.R.data_ptr(), 1.0, 0, accumulative, X.make_plan(method), self.s)
+
+
+def time_steps(fn, steps, warmup, world, stream_obj):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream_obj)
+    for _ in range(steps):
+        fn()
+    e1.record(stream_obj)
+    torch.cuda.synchronize()
+    barrier(world)
+    return e0.elapsed_time(e1)
+
+
+def sample_error(X, case, method, nsamp=48):
+    """Relative Frobenius and max-abs error of sampled D elements against the
+    double-double oracle (each a K-length dot product), after one
+    non-accumulating contraction."""
+    import numpy as np
+    import torch
+
+    import oracle as O
+    case.run(method, accumulative=False)
+    torch.cuda.synchronize()
+    M = 1
+    cptrn = case.cptrn
+    lrank = len(case.ld)
+    for i, c in enumerate(cptrn[:lrank]):
+        if c > 0:
+            M *= case.ld[i]
+    N = vol(case.dd) // M
+    K = vol(case.ld) // M
+    dt = O.NP_DTYPE[case.wl["dtk"]]
+    tdt = {np.float64: torch.float64, np.float32: torch.float32}[dt]
+    Dm = case.D.view(tdt)
+    rng = np.random.default_rng(5)
+    # only the V(a,b,c,d)*T(c,d,i,j) layout is sampled directly: L = [K][M] m-fastest, R = [N][K]
+    if case.wl["pattern"] != "D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)":
+        return None
+    Lm = case.L.view(tdt).view(K, M)
+    Rm = case.R.view(tdt).view(N, K)
+    num = den = mx = 0.0
+    for _ in range(nsamp):
+        m, n = int(rng.integers(M)), int(rng.integers(N))
+        lv = Lm[:, m].double().cpu().numpy()
+        rv = Rm[n, :].double().cpu().numpy()
+        ref = np.zeros(1)
+        O.contract([-1, -1], ref, [], lv, [K], rv, [K], 1.0, 0, True, mode=1)
+        got = float(Dm[m + n * M].item())
+        num += (got - ref[0]) ** 2
+        den += ref[0] ** 2
+        mx = max(mx, abs(got - ref[0]))
+    return {"rel_frobenius": (num / den) ** 0.5, "max_abs": mx, "samples": nsamp}
+
+
+def permute_sweep(X, stream, stream_obj, hbm_gbs):
+    """All 24 rank-4 permutations of 256 MiB-class R8 (76^4) and R4 (90^4)."""
+    import itertools
+
+    import torch
+    out = {}
+    total_bytes = total_ms = 0.0
+    rates = []
+    for dtk, n in ((8, 76), (4, 90)):
+        es = X.ELEM_BYTES[dtk]
+        v = n ** 4
+        a = torch.empty(v * es, dtype=torch.uint8, device="cuda")
+        b = torch.empty_like(a)
+        X.fill_uniform(dtk, v, a.data_ptr(), 3, stream=stream)
+        dims = [n] * 4
+        for perm in itertools.permutations([1, 2, 3, 4]):
+            X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream)
+            ms = time_steps(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream), 5, 1, 1,
+                            stream_obj) / 5
+            gb = 2.0 * v * es / 1e9
+            rates.append(gb / (ms / 1e3))
+            total_bytes += gb
+            total_ms += ms
+        # plain scatter form for reference (two permutations)
+        sc = []
+        for perm in ((4, 3, 2, 1), (2, 4, 1, 3)):
+            ms = time_steps(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream, True), 3,
+                            1, 1, stream_obj) / 3
+            sc.append(2.0 * v * es / 1e9 / (ms / 1e3))
+        out[f"scatter_gbs_{'r8' if dtk == 8 else 'r4'}"] = round(statistics.mean(sc), 1)
+        del a, b
+    agg = total_bytes / (total_ms / 1e3)
+    out.update({"value": round(agg, 1), "unit": "GB/s", "min": round(min(rates), 1), "max": round(max(rates), 1),
+                "frac_of_measured_hbm": round(agg / hbm_gbs, 3), "frac_of_8000": round(agg / 8000.0, 3),
+                "cases": "24 rank-4 perms x {R8 76^4 (254.5 MiB), R4 90^4 (250.3 MiB)}, bit-exact"})
+    return out
+
+
+def e2e_talsh(X, wl, steps):
+    """Same contraction through talshTensorContract with Host-resident tensors:
+    each step copies V, T, D to the GPU and D back (copy control TTT)."""
+    import exatensor_b200.talsh as T
+    T.init((int(os.environ.get("LOCAL_RANK", "0")),))
+    dd, ld, rd = shapes(wl["pattern"], wl["v"], wl["o"])
+    es = X.ELEM_BYTES[wl["dtk"]]
+    D = T.Tensor(dd, wl["dtk"], 0.0)
+    L = T.Tensor(ld, wl["dtk"], 1.0 / (3 * wl["v"]))
+    R = T.Tensor(rd, wl["dtk"], 0.5)
+    run = lambda: T.check(T.contract(wl["pattern"], D, L, R, 1.0, 0, T.DEV_NVIDIA_GPU, T.COPY_TTT, True),
+                          "talshTensorContract")
+    run()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run()
+    dt = (time.perf_counter() - t0) / steps
+    flops = 2.0 * vol(dd) * (vol(ld) * vol(rd) / vol(dd)) ** 0.5
+    res = {"value": round(flops / dt / 1e12, 3), "unit": "TFLOP/s", "ms_per_step": round(dt * 1e3, 2),
+           "h2d_bytes_per_step": (vol(dd) + vol(ld) + vol(rd)) * es, "d2h_bytes_per_step": vol(dd) * es,
+           "api": "talshTensorContract(COPY_TTT), host tensors, wall clock incl. H2D/D2H"}
+    del D, L, R
+    return res
+
+
+# ----------------------------------------------------------------------------- CPU
+def cpu_contraction_sample(steps=1):
+    """The reference's OpenMP+BLAS CPU path (oracle restatement) on a bounded
+    sample of the CCSD-like contraction: v=96, o=48 (same pattern and index
+    map, 1/16 of the FLOPs)."""
+    import numpy as np
+
+    import oracle as O
+    nthr = O.nthreads_default()
+    if not O.blas_available():
+        return None
+    v, o = 96, 48
+    pattern = WORKLOADS["ccsd1_r8"]["pattern"]
+    dd, ld, rd = shapes(pattern, v, o)
+    cptrn, *_ = O.parse_pattern(pattern)
+    L = O.splitmix64_uniform(vol(ld), 1) / v
+    R = O.splitmix64_uniform(vol(rd), 2)
+    D = np.zeros(vol(dd))
+    O.contract_blas(cptrn, D, dd, L, ld, R, rd, 1.0, True, nthr)
+    best = None
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        O.contract_blas(cptrn, D, dd, L, ld, R, rd, 1.0, True, nthr)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    flops = 2.0 * vol(dd) * (vol(ld) * vol(rd) / vol(dd)) ** 0.5
+    return {"value": round(flops / best / 1e12, 4), "unit": "TFLOP/s", "cores": nthr, "kind": "port",
+            "sample": f"{pattern} v={v} o={o} R8 ({flops:.3e} FLOP), OpenMP permutes + OpenBLAS dgemm, "
+                      f"best of {max(1, steps)}"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU implementation of the path (its
+    OpenMP+BLAS CP-TAL contraction, restated in oracle/ because the Fortran
+    reference cannot be compiled here), on this host's cores."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import oracle as O
+    O.build()
+    res = cpu_contraction_sample(steps=max(1, args.steps))
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "bundled OpenBLAS not found"}))
+        return
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": "TFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v)",
+            "config": {"workload": "ccsd1_r8 CPU sample v=96 o=48", "parallelism": "host threads"},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------- main
+def run_ours(args):
+    import torch
+
+    import exatensor_b200 as X
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    X.device_init(local)
+    hbm_gbs, bf16_tflops, peak_src = peaks()
+    s_obj = torch.cuda.current_stream()
+    s = s_obj.cuda_stream
+    wl = WORKLOADS[args.workload]
+    case = ContractionCase(X, wl, s)
+    torch.cuda.synchronize()
+    # chosen form (plan selector)
+    case.run(X.METHOD_AUTO)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    n0 = X.launch_count()
+    X.timing_enable(True)
+    X.timing_read()
+    clocks.start()
+    ms = time_steps(lambda: case.run(X.METHOD_AUTO), args.steps, args.warmup, world, s_obj)
+    clk = clocks.stop()
+    gemm_ms, gemm_n = X.timing_read()
+    X.timing_enable(False)
+    launches = X.launch_count() - n0
+    st = X.last_contract_stats()
+    chosen_method = {1: "ttgt", 2: "fused"}.get(st.method, str(st.method))
+    ms_max = max_over_ranks(ms, world)
+    value = world * args.steps * case.flops / (ms_max / 1e3) / 1e12
+    # plain form
+    psteps = max(1, args.steps // 2)
+    X.timing_enable(True)
+    X.timing_read()
+    pms = time_steps(lambda: case.run(X.METHOD_TTGT), psteps, 1, world, s_obj)
+    pgemm_ms, pgemm_n = X.timing_read()
+    X.timing_enable(False)
+    plain = case.flops / (max_over_ranks(pms, world) / psteps / 1e3) / 1e12
+    line = None
+    if rank == 0:
+        err_chosen = sample_error(X, case, X.METHOD_AUTO)
+        err_plain = sample_error(X, case, X.METHOD_TTGT)
+        perm = permute_sweep(X, s, s_obj, hbm_gbs)
+        # dominant kernel of the chosen step
+        per_launch_ms = gemm_ms / max(1, gemm_n)
+        if chosen_method == "fused":
+            kern = "tcgen05 INT8-slice GEMM" if wl["dtk"] in (8, 18) else "tcgen05 split-BF16 GEMM"
+            hw_ops = case.flops * max(1, st.passes)  # each pass is a full int8/bf16 GEMM
+            peak = 2 * bf16_tflops if wl["dtk"] in (8, 18) else bf16_tflops
+            peak_note = (f"2 x {peak_src} bf16 dense (INT8 dense rate)" if wl["dtk"] in (8, 18)
+                         else f"{peak_src} bf16 dense")
+        else:
+            kern = "FP64 DMMA GEMM (mma.sync m8n8k4)" if wl["dtk"] in (8, 18) else "FP32 FFMA GEMM"
+            hw_ops = case.flops
+            peak = 40.0 if wl["dtk"] in (8, 18) else 75.0
+            peak_note = "nominal B200 FP64 tensor-core rate (not in MEASURED_PEAKS.json)"
+        achieved = hw_ops / (per_launch_ms / 1e3) / 1e12 if gemm_n else None
+        roofline = {"bound": "tensor", "kernel": kern, "achieved": round(achieved, 2) if achieved else None,
+                    "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 3) if achieved else None,
+                    "traffic": None, "peak_source": peak_note, "launch_ms": round(per_launch_ms, 3),
+                    "launches_timed": gemm_n}
+        e2e = e2e_talsh(X, wl, steps=max(1, min(2, args.steps)))
+        cpu = cpu_contraction_sample(steps=1) if world == 1 else None
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if wl["dtk"] == 8 else "f32",
+            "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v, D=0)",
+            "config": {"workload": f"{args.workload}: {wl['pattern']} v={wl['v']} o={wl['o']}",
+                       "method": chosen_method, "slices": st.slices, "passes": st.passes,
+                       "l2": "inputs larger than L2 (V alone is 10.9 GB)", "parallelism": f"replicas x{world}"},
+            "plain": {"value": round(plain, 3), "unit": "TFLOP/s", "method": "ttgt (permute + FP64 DMMA GEMM)",
+                      "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),
+                      "chosen_over_plain": round(value / world / plain, 3)},
+            "error": {"chosen": err_chosen, "plain": err_plain, "oracle": "double-double dot products"},
+            "permute": perm, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk,
+        }
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,189 @@
+"""exatensor_b200: TAL-SH's device tensor-algebra path, native on B200 (sm_100a).
+
+The compute lives in ``libtalsh_b200.so`` (hand-written CUDA for sm_100a plus
+the C++ ``talsh.h`` layer), built in-tree by ``exatensor_b200.build``.  This
+module is a thin ctypes binding of its C ABI (``include/talsh_b200.h``) for
+Python callers and the test-suite; device memory is passed as raw pointers
+(e.g. ``torch.Tensor.data_ptr()``) and streams as ``cudaStream_t`` handles.
+
+There is no Python or CPU fallback: if the library is missing or no B200 is
+visible, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+R4, R8, C4, C8 = 4, 8, 14, 18
+DATA_KINDS = (R4, R8, C4, C8)
+ELEM_BYTES = {R4: 4, R8: 8, C4: 8, C8: 16}
+
+TB_SUCCESS = 0
+TB_ERR = {1: "invalid arguments", 2: "bad pattern", 3: "CUDA error", 4: "not implemented", 5: "device error",
+          6: "out of memory", 7: "limit exceeded"}
+METHOD_AUTO, METHOD_TTGT, METHOD_FUSED = 0, 1, 2
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtalsh_b200.so")
+_lib = None
+
+
+class TBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{TB_ERR.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+class Plan(C.Structure):
+    """tb_plan_t: contraction plan (method, INT8 slices, N tile, split-BF16 terms)."""
+    _fields_ = [("method", C.c_int), ("slices", C.c_int), ("tile_n", C.c_int), ("bf16_terms", C.c_int),
+                ("reserved", C.c_int * 4)]
+
+
+class ContractStats(C.Structure):
+    _fields_ = [("method", C.c_int), ("slices", C.c_int), ("passes", C.c_int), ("gemm_launches", C.c_int),
+                ("m", C.c_longlong), ("n", C.c_longlong), ("k", C.c_longlong), ("flops", C.c_double)]
+
+
+def lib() -> C.CDLL:
+    """Loads libtalsh_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m exatensor_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    ip, vp, i64 = C.POINTER(C.c_int), C.c_void_p, C.c_int64
+    L.tb_last_error.restype = C.c_char_p
+    L.tb_launch_count.restype = C.c_longlong
+    L.tb_timing_enable.argtypes = [C.c_int]
+    L.tb_timing_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.tb_device_init.argtypes = [C.c_int]
+    L.tb_device_check.argtypes = [vp]
+    L.tb_data_kind_size.argtypes = [C.c_int]
+    L.tb_parse_pattern.argtypes = [C.c_char_p, ip, ip, ip, ip, ip]
+    L.tb_tensor_copy.argtypes = [C.c_int, C.c_int, ip, ip, vp, vp, C.c_int, vp]
+    L.tb_tensor_copy_scatter.argtypes = [C.c_int, C.c_int, ip, ip, vp, vp, C.c_int, vp]
+    L.tb_tensor_add.argtypes = [C.c_int, C.c_int, ip, ip, vp, vp, C.c_double, C.c_double, C.c_int, vp]
+    L.tb_tensor_init.argtypes = [C.c_int, C.c_size_t, vp, C.c_double, C.c_double, vp]
+    L.tb_tensor_scale.argtypes = [C.c_int, C.c_size_t, vp, C.c_double, C.c_double, vp]
+    L.tb_tensor_norm.argtypes = [C.c_int, C.c_size_t, vp, C.c_int, C.POINTER(C.c_double), vp]
+    L.tb_tensor_contract.argtypes = [ip, C.c_int, C.c_int, ip, vp, C.c_int, ip, vp, C.c_int, ip, vp, C.c_double,
+                                     C.c_double, C.c_int, C.c_int, C.POINTER(Plan), vp]
+    L.tb_tensor_contract_str.argtypes = [C.c_char_p, C.c_int, C.c_int, ip, vp, C.c_int, ip, vp, C.c_int, ip, vp,
+                                         C.c_double, C.c_double, C.c_int, C.POINTER(Plan), vp]
+    L.tb_fill_uniform.argtypes = [C.c_int, C.c_size_t, vp, C.c_uint64, C.c_double, C.c_double, vp]
+    L.tb_last_contract_stats.argtypes = [C.POINTER(ContractStats)]
+    _lib = L
+    return L
+
+
+def _check(code: int):
+    if code != TB_SUCCESS:
+        raise TBError(code, lib().tb_last_error().decode(errors="replace"))
+
+
+def iarr(vals) -> C.Array:
+    vals = [int(v) for v in vals]
+    return (C.c_int * max(1, len(vals)))(*vals)
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+def device_init(gpu: int = 0):
+    _check(lib().tb_device_init(gpu))
+
+
+def device_check(stream=None):
+    _check(lib().tb_device_check(_stream(stream)))
+
+
+def parse_pattern(pattern: str):
+    """Symbolic -> digital pattern: (cptrn, drank, lrank, rrank, conj_bits); rrank=-1 for unary."""
+    cp = (C.c_int * 112)()
+    d, l, r, cj = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _check(lib().tb_parse_pattern(pattern.encode(), cp, C.byref(d), C.byref(l), C.byref(r), C.byref(cj)))
+    n = l.value + max(r.value, 0)
+    return list(cp[:n]), d.value, l.value, r.value, cj.value
+
+
+def tensor_copy(dtk, dims, cptrn, src_ptr, dst_ptr, conj_bits=0, stream=None, scatter=False):
+    f = lib().tb_tensor_copy_scatter if scatter else lib().tb_tensor_copy
+    _check(f(dtk, len(dims), iarr(dims), iarr(cptrn), C.c_void_p(src_ptr), C.c_void_p(dst_ptr), conj_bits,
+             _stream(stream)))
+
+
+def tensor_add(dtk, ldims, cptrn, d_ptr, l_ptr, scale=1.0, conj_bits=0, stream=None):
+    s = complex(scale)
+    _check(lib().tb_tensor_add(dtk, len(ldims), iarr(ldims), iarr(cptrn), C.c_void_p(d_ptr), C.c_void_p(l_ptr),
+                               s.real, s.imag, conj_bits, _stream(stream)))
+
+
+def tensor_init(dtk, volume, d_ptr, value=0.0, stream=None):
+    v = complex(value)
+    _check(lib().tb_tensor_init(dtk, volume, C.c_void_p(d_ptr), v.real, v.imag, _stream(stream)))
+
+
+def tensor_scale(dtk, volume, d_ptr, scale, stream=None):
+    s = complex(scale)
+    _check(lib().tb_tensor_scale(dtk, volume, C.c_void_p(d_ptr), s.real, s.imag, _stream(stream)))
+
+
+def tensor_norm(dtk, volume, d_ptr, which=1, stream=None) -> float:
+    out = C.c_double()
+    _check(lib().tb_tensor_norm(dtk, volume, C.c_void_p(d_ptr), which, C.byref(out), _stream(stream)))
+    return out.value
+
+
+def fill_uniform(dtk, volume, d_ptr, seed, lo=-1.0, hi=1.0, stream=None):
+    _check(lib().tb_fill_uniform(dtk, volume, C.c_void_p(d_ptr), seed, lo, hi, _stream(stream)))
+
+
+def make_plan(method=METHOD_AUTO, slices=0, tile_n=0, bf16_terms=0) -> Plan:
+    p = Plan()
+    p.method, p.slices, p.tile_n, p.bf16_terms = method, slices, tile_n, bf16_terms
+    return p
+
+
+def tensor_contract(pattern_or_cptrn, dtk, ddims, d_ptr, ldims, l_ptr, rdims, r_ptr, alpha=1.0, conj_bits=0,
+                    accumulative=True, plan: Plan | None = None, stream=None):
+    """D = beta*D + alpha*op(L)*op(R); pattern may be symbolic (str) or digital (list)."""
+    a = complex(alpha)
+    pp = C.byref(plan) if plan is not None else None
+    if isinstance(pattern_or_cptrn, str):
+        _check(lib().tb_tensor_contract_str(pattern_or_cptrn.encode(), dtk, len(ddims), iarr(ddims),
+                                            C.c_void_p(d_ptr), len(ldims), iarr(ldims), C.c_void_p(l_ptr),
+                                            len(rdims), iarr(rdims), C.c_void_p(r_ptr), a.real, a.imag,
+                                            int(accumulative), pp, _stream(stream)))
+    else:
+        _check(lib().tb_tensor_contract(iarr(pattern_or_cptrn), dtk, len(ddims), iarr(ddims), C.c_void_p(d_ptr),
+                                        len(ldims), iarr(ldims), C.c_void_p(l_ptr), len(rdims), iarr(rdims),
+                                        C.c_void_p(r_ptr), a.real, a.imag, conj_bits, int(accumulative), pp,
+                                        _stream(stream)))
+
+
+def launch_count() -> int:
+    return lib().tb_launch_count()
+
+
+def timing_enable(on: bool = True):
+    lib().tb_timing_enable(int(on))
+
+
+def timing_read():
+    """(summed milliseconds, launches) of the timed GEMM kernels since the last read."""
+    ms, n = C.c_double(), C.c_int()
+    lib().tb_timing_read(C.byref(ms), C.byref(n))
+    return ms.value, n.value
+
+
+def last_contract_stats() -> ContractStats:
+    st = ContractStats()
+    _check(lib().tb_last_contract_stats(C.byref(st)))
+    return st

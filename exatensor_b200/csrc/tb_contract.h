@@ -1,0 +1,23 @@
+// tb_contract.h -- contraction driver internals shared with the tensor-core path.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/talsh_b200.h"
+#include "tb_pattern.h"
+
+namespace tb {
+
+int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* d, int lrank, const int* ldims,
+                  const void* l, int rrank, const int* rdims, const void* r, double ar, double ai, int conj_bits,
+                  int accumulative, const tb_plan_t* plan, cudaStream_t s);
+
+// Chooses TB_METHOD_TTGT or TB_METHOD_FUSED for a matricized contraction.
+int select_method(int dtk, const Matricization& Z, const tb_plan_t* plan);
+
+// Tensor-core contraction with fused operand gathers and epilogue.
+// Returns TB_ERR_NOT_IMPLEMENTED when the shape is outside its scope.
+int contract_fused(const Matricization& Z, int dtk, const int* ddims, void* d, const int* ldims, const void* l,
+                   const int* rdims, const void* r, double ar, double ai, bool accumulate, int lconj, int rconj,
+                   const tb_plan_t* plan, cudaStream_t s, tb_contract_stats_t* stats);
+
+}  // namespace tb

@@ -1,0 +1,184 @@
+// tb_perm_plan.cpp -- builds permutation plans (host code, no CUDA).
+#include "tb_perm_plan.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/talsh_b200.h"
+
+namespace tb {
+
+int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin_in,
+                    const int64_t* sout_in, PermParams* pp) {
+  PermParams& P = *pp;
+  std::memset(&P, 0, sizeof(P));
+  P.es = es;
+  // 1. drop unit dims, merge neighbours that stay neighbours
+  std::vector<int64_t> D, SI, SO;
+  for (int i = 0; i < rank; ++i) {
+    if (dims_in[i] <= 0) return TB_ERR_INVALID_ARGS;
+    if (dims_in[i] == 1) continue;
+    if (!D.empty() && SI.back() * D.back() == sin_in[i] && SO.back() * D.back() == sout_in[i]) {
+      D.back() *= dims_in[i];
+    } else {
+      D.push_back(dims_in[i]); SI.push_back(sin_in[i]); SO.push_back(sout_in[i]);
+    }
+  }
+  if (D.empty()) { D.push_back(1); SI.push_back(1); SO.push_back(1); }
+  const int r = (int)D.size();
+  if (r > kPlanMaxRank) return TB_ERR_INVALID_ARGS;
+  if (SI[0] != 1) return TB_ERR_NOT_IMPLEMENTED;
+  std::vector<int> Q(r);
+  for (int i = 0; i < r; ++i) Q[i] = i;
+  std::stable_sort(Q.begin(), Q.end(), [&](int x, int y) { return SO[x] < SO[y]; });
+  if (SO[Q[0]] != 1) return TB_ERR_NOT_IMPLEMENTED;
+  const int64_t T = std::max<int64_t>(1, 128 / es);
+  const int64_t Vmin = 16384 / es, Vmax = 32768 / es;
+  std::vector<int64_t> t(r, 1);
+  auto cdiv = [](int64_t x, int64_t y) { return (x + y - 1) / y; };
+  // 2. load block: input dims 0..a
+  int a = 0;
+  {
+    int64_t vol = 1;
+    for (a = 0; a < r; ++a) {
+      if (vol * D[a] <= T && a < r - 1) { t[a] = D[a]; vol *= D[a]; continue; }
+      t[a] = std::min(D[a], cdiv(T, vol));
+      break;
+    }
+    if (a == r) a = r - 1;
+  }
+  // 3. store block: output-order prefix (must be dense in the output)
+  std::vector<char> inB(r, 0);
+  int blast = -1;
+  {
+    int64_t volB = 1;
+    for (int j = 0; j < r; ++j) {
+      const int i = Q[j];
+      if (SO[i] != volB) break;  // not dense: the store run ends before i
+      if (i < a || (i == a && t[a] == D[a]) || (i > a && t[i] == D[i])) {
+        inB[i] = 1; blast = i; volB *= D[i];
+        if (volB >= T) break;
+        continue;
+      }
+      if (i == a) {
+        t[a] = std::max(t[a], std::min(D[a], cdiv(T, volB)));
+        inB[a] = 1; blast = a; volB *= t[a];
+        if (t[a] == D[a] && volB < T) continue;  // became whole: the run may grow further
+        break;
+      }
+      if (volB * D[i] <= T) { t[i] = D[i]; inB[i] = 1; blast = i; volB *= D[i]; continue; }
+      t[i] = std::min(D[i], cdiv(T, volB));
+      inB[i] = 1; blast = i; volB *= t[i];
+      break;
+    }
+  }
+  if (blast < 0) return TB_ERR_NOT_IMPLEMENTED;
+  auto vol_of = [&]() { int64_t v = 1; for (int i = 0; i < r; ++i) v *= t[i]; return v; };
+  // 4. extend the tile to Vmin elements: whole small dims first, then the partial dims
+  for (int guard = 0; guard < 4 * r + 8; ++guard) {
+    int64_t V = vol_of();
+    if (V >= Vmin) break;
+    bool grown = false;
+    for (int i = 0; i < r && !grown; ++i) {
+      if (t[i] == 1 && D[i] > 1 && V * D[i] <= Vmax) { t[i] = D[i]; grown = true; }
+    }
+    if (grown) continue;
+    for (int which = 0; which < 2 && !grown; ++which) {
+      const int d = which == 0 ? a : blast;
+      if (t[d] < D[d]) {
+        const int64_t f = std::min(cdiv(D[d], t[d]), cdiv(Vmin, V));
+        if (f > 1) { t[d] = std::min(D[d], t[d] * f); grown = true; }
+      }
+    }
+    if (!grown) break;
+  }
+  // 5. chunk structure
+  const int pa = (t[a] < D[a]) ? a : -1;
+  const int pb = (t[blast] < D[blast]) ? blast : -1;
+  int64_t prodA = 1;
+  for (int i = 0; i < a; ++i) prodA *= D[i];
+  const int64_t LA = prodA * t[a];
+  // tile index strides (input-order enumeration: load block, then rest dims)
+  std::vector<int64_t> est(r, 0);
+  {
+    int64_t s = 1;
+    for (int i = 0; i <= a; ++i) { est[i] = s; s *= t[i]; }
+    for (int i = a + 1; i < r; ++i) if (t[i] > 1) { est[i] = s; s *= t[i]; }
+  }
+  const int64_t V = vol_of();
+  std::vector<int> Bdims;  // store block dims in output order
+  for (int j = 0; j < r; ++j) if (inB[Q[j]]) Bdims.push_back(Q[j]);
+  int64_t LB = 1;
+  for (int d : Bdims) LB *= t[d];
+  // store positions j' decompose on the store block's last dim (blast):
+  // j' = (full store-block dims before blast) + prodB * digit(blast)
+  int64_t prodB = 1;
+  for (int d : Bdims) if (d != blast) prodB *= t[d];
+  const int64_t nA = V / LA, nB = V / LB;
+  if (nA > kMaxChunks || nB > kMaxChunks || prodB > kMaxEjf || V > (int64_t)1 << 30)
+    return TB_ERR_NOT_IMPLEMENTED;
+  P.rank = r; P.V = (int)V; P.LA = (int)LA; P.nA = (int)nA; P.LB = (int)LB; P.nB = (int)nB;
+  P.pa = pa; P.pb = pb; P.prodA = (int)prodA; P.prodB = (int)prodB; P.ejf_n = (int)prodB;
+  P.ej_pb_stride = (int)est[blast];
+  P.pad_shift = es == 4 ? 5 : es == 8 ? 4 : 3;
+  for (int i = 0; i < r; ++i) { P.dims[i] = D[i]; P.tile[i] = t[i]; P.sin[i] = SI[i]; P.sout[i] = SO[i]; }
+  magic32((uint32_t)LA, &P.la_magic, &P.la_shift);
+  magic32((uint32_t)LB, &P.lb_magic, &P.lb_shift);
+  magic32((uint32_t)prodB, &P.pb_magic, &P.pb_shift);
+  // load chunks: rest dims (tile dims outside the load block) in input order
+  std::vector<int> restA;
+  for (int i = a + 1; i < r; ++i) if (t[i] > 1) restA.push_back(i);
+  for (int64_t c = 0; c < nA; ++c) {
+    int64_t x = c, off = 0; int dpb = -1;
+    for (int d : restA) { int64_t dg = x % t[d]; x /= t[d]; off += dg * SI[d]; if (d == pb) dpb = (int)dg; }
+    P.ld_base[c] = off; P.ld_dpb[c] = (int16_t)dpb;
+  }
+  // store chunks: tile dims outside the store block, in output order
+  std::vector<int> restB;
+  for (int j = 0; j < r; ++j) { int d = Q[j]; if (t[d] > 1 && !inB[d]) restB.push_back(d); }
+  for (int64_t c = 0; c < nB; ++c) {
+    int64_t x = c, off = 0, eb = 0; int dpa = -1;
+    for (int d : restB) {
+      int64_t dg = x % t[d]; x /= t[d];
+      off += dg * SO[d]; eb += dg * est[d];
+      if (d == pa) dpa = (int)dg;
+    }
+    P.st_base[c] = off; P.st_ebase[c] = (int32_t)eb; P.st_dpa[c] = (int16_t)dpa;
+  }
+  // positions inside a store chunk: store-block dims before blast
+  for (int64_t j = 0; j < prodB; ++j) {
+    int64_t x = j, e = 0;
+    for (int d : Bdims) { if (d == blast) continue; int64_t dg = x % t[d]; x /= t[d]; e += dg * est[d]; }
+    P.ejf[j] = (int32_t)e;
+  }
+  // 6. tile grid
+  int g = 0; int64_t nt = 1;
+  for (int i = 0; i < r; ++i) {
+    const int64_t ext = cdiv(D[i], t[i]);
+    if (ext > 1) { P.gdim[g] = i; P.gext[g] = ext; P.gdiv[g].init((uint64_t)ext); ++g; nt *= ext; }
+  }
+  P.ngd = g; P.ntiles = nt;
+  return 0;
+}
+
+int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p) {
+  if (rank < 0 || rank > kPlanMaxRank) return TB_ERR_INVALID_ARGS;
+  int64_t D[kPlanMaxRank], SI[kPlanMaxRank], SO[kPlanMaxRank], pos[kPlanMaxRank + 1];
+  int seen[kPlanMaxRank + 1] = {0};
+  for (int i = 0; i < rank; ++i) {
+    if (cptrn[i] < 1 || cptrn[i] > rank || seen[cptrn[i]]) return TB_ERR_PATTERN;
+    seen[cptrn[i]] = 1;
+  }
+  int64_t s = 1;
+  for (int i = 0; i < rank; ++i) { D[i] = dims[i]; SI[i] = s; s *= dims[i]; }
+  // output extents by position, then strides by position
+  int64_t oe[kPlanMaxRank];
+  for (int i = 0; i < rank; ++i) oe[cptrn[i] - 1] = dims[i];
+  s = 1;
+  for (int q = 0; q < rank; ++q) { pos[q] = s; s *= oe[q]; }
+  for (int i = 0; i < rank; ++i) SO[i] = pos[cptrn[i] - 1];
+  return build_perm_plan(es, rank, D, SI, SO, p);
+}
+
+}  // namespace tb

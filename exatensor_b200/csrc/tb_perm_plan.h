@@ -1,0 +1,63 @@
+// tb_perm_plan.h -- host-side permutation plan (shared by the CUDA engine and
+// the CPU emulation test of its index arithmetic).
+//
+// A permutation moves every element of a dense tensor to a new position.  The
+// kernel stages one tile of the tensor in shared memory: the tile is a box
+// whose input-fastest dimensions give contiguous input runs of at least
+// 128 bytes ("load chunks") and whose output-fastest dimensions give
+// contiguous output runs of at least 128 bytes ("store chunks").  Chunk base
+// offsets and the shared-memory transposition map are computed here once per
+// plan and passed to the kernel as a parameter.
+#pragma once
+#include <cstdint>
+#include "tb_fastdiv.h"
+
+namespace tb {
+
+constexpr int kPlanMaxRank = 56;
+constexpr int kMaxChunks = 256;   // load/store chunks per tile
+constexpr int kMaxEjf = 64;       // entries of the store-chunk transposition table
+
+// Device-side plan (passed by value as a __grid_constant__ kernel parameter).
+struct PermParams {
+  int rank;                  // reduced rank
+  int es;                    // element bytes
+  int V;                     // tile volume (elements)
+  int LA, nA;                // load chunk length, number of load chunks
+  int LB, nB;                // store chunk length, number of store chunks
+  int pa, pb;                // partial dims (reduced indices) or -1
+  int prodA, prodB;          // digit(pa) = j / prodA in a load chunk; digit(last store dim) = j' / prodB
+  int ejf_n;                 // entries of ejf (= prodB)
+  int ej_pb_stride;          // tile-index stride of the last store-block dim
+  int pad_shift;             // smem padding: one element per (1 << pad_shift)
+  int ngd;                   // grid dims
+  int64_t ntiles;
+  int64_t dims[kPlanMaxRank];
+  int64_t tile[kPlanMaxRank];
+  int64_t sin[kPlanMaxRank];
+  int64_t sout[kPlanMaxRank];
+  int gdim[kPlanMaxRank];        // reduced dim of each grid dim
+  int64_t gext[kPlanMaxRank];    // tile positions along each grid dim
+  FastDiv gdiv[kPlanMaxRank];    // divisors for gext
+  uint32_t la_magic; int la_shift;   // 32-bit fast division by LA
+  uint32_t lb_magic; int lb_shift;   // by LB
+  uint32_t pb_magic; int pb_shift;   // by prodB
+  int64_t ld_base[kMaxChunks];  // input offset of load chunk c (tile-relative)
+  int16_t ld_dpb[kMaxChunks];   // digit of pb in load chunk c (-1: pb inside the chunk or none)
+  int64_t st_base[kMaxChunks];  // output offset of store chunk c'
+  int32_t st_ebase[kMaxChunks]; // tile index base of store chunk c'
+  int16_t st_dpa[kMaxChunks];   // digit of pa in store chunk c' (-1: pa inside the chunk or none)
+  int32_t ejf[kMaxEjf];         // tile index of position j' % prodB inside a store chunk
+};
+
+// Host-side plan builder.  dims/sin/sout describe the input dims (input
+// strides, output strides), first dim fastest in the input.  Returns 0 or a
+// TB_ERR code.  Dims of extent 1 are dropped and mergeable neighbours fused.
+int build_perm_plan(int es, int rank, const int64_t* dims, const int64_t* sin, const int64_t* sout,
+                    PermParams* p);
+// Convenience: plain O2N permutation of a dense tensor (cptrn 1-based).
+int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p);
+
+
+
+}  // namespace tb

@@ -1,0 +1,210 @@
+// tb_permute.cu -- permutation plans, tiled and scatter permutation kernels,
+// and the tb_tensor_copy / tb_tensor_add entry points.
+#include "tb_permute.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace tb {
+
+// ---------------------------------------------------------------------------
+// Scatter permutation: one element per thread (the plain reference form).
+// ---------------------------------------------------------------------------
+struct ScatterParams {
+  int rank;
+  int64_t vol;
+  FastDiv div[kMaxRank];
+  int64_t dims[kMaxRank];
+  int64_t sout[kMaxRank];
+};
+
+template <typename E, typename Store>
+__global__ void scatter_kernel(const __grid_constant__ ScatterParams P, const E* __restrict__ in, Store st) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.vol;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t r = (uint64_t)i;
+    int64_t o = 0;
+    for (int d = 0; d < P.rank; ++d) {
+      uint64_t q = P.div[d].div(r);
+      o += (int64_t)(r - q * (uint64_t)P.dims[d]) * P.sout[d];
+      r = q;
+    }
+    st(o, in[i]);
+  }
+}
+
+namespace {
+
+int o2n_strides(int rank, const int* dims, const int* cptrn, int64_t* sout) {
+  int seen[kMaxRank + 1] = {0};
+  int64_t oe[kMaxRank], pos[kMaxRank];
+  for (int i = 0; i < rank; ++i) {
+    if (cptrn[i] < 1 || cptrn[i] > rank || seen[cptrn[i]]) return TB_ERR_PATTERN;
+    seen[cptrn[i]] = 1;
+    oe[cptrn[i] - 1] = dims[i];
+  }
+  int64_t s = 1;
+  for (int q = 0; q < rank; ++q) { pos[q] = s; s *= oe[q]; }
+  for (int i = 0; i < rank; ++i) sout[i] = pos[cptrn[i] - 1];
+  return 0;
+}
+
+int check_dims(int rank, const int* dims, int64_t* vol) {
+  if (rank < 0 || rank > kMaxRank || (rank > 0 && !dims)) return TB_ERR_INVALID_ARGS;
+  int64_t v = 1;
+  for (int i = 0; i < rank; ++i) { if (dims[i] <= 0) return TB_ERR_INVALID_ARGS; v *= dims[i]; }
+  *vol = v;
+  return 0;
+}
+
+template <typename E, typename Store>
+int run_scatter(int rank, const int* dims, const int* cptrn, const E* in, const Store& st,
+                cudaStream_t s) {
+  ScatterParams P;
+  std::memset(&P, 0, sizeof(P));
+  int64_t vol;
+  if (int e = check_dims(rank, dims, &vol)) return e;
+  int64_t sout[kMaxRank];
+  if (int e = o2n_strides(rank, dims, cptrn, sout)) return e;
+  P.rank = rank; P.vol = vol;
+  for (int i = 0; i < rank; ++i) { P.dims[i] = dims[i]; P.sout[i] = sout[i]; P.div[i].init(dims[i]); }
+  int64_t blocks = std::min<int64_t>((vol + 255) / 256, (int64_t)num_sms() * 16);
+  if (blocks < 1) blocks = 1;
+  scatter_kernel<E, Store><<<(unsigned)blocks, 256, 0, s>>>(P, in, st);
+  TB_CHECK_LAUNCH();
+  return 0;
+}
+
+// Fused permute + add: d = d + v*a with two roundings (no FMA), complex
+// products by the textbook formula, the left operand optionally conjugated.
+template <typename R>
+struct AddScalar {
+  R* out; R a;
+  __device__ __forceinline__ void operator()(int64_t o, const R& v) const;
+};
+template <> __device__ __forceinline__ void AddScalar<float>::operator()(int64_t o, const float& v) const {
+  out[o] = __fadd_rn(out[o], __fmul_rn(v, a));
+}
+template <> __device__ __forceinline__ void AddScalar<double>::operator()(int64_t o, const double& v) const {
+  out[o] = __dadd_rn(out[o], __dmul_rn(v, a));
+}
+struct AddC4 {
+  float2* out; float ar, ai; bool conj;
+  __device__ __forceinline__ void operator()(int64_t o, const float2& v) const {
+    const float vr = v.x, vi = conj ? -v.y : v.y;
+    const float tr = __fsub_rn(__fmul_rn(vr, ar), __fmul_rn(vi, ai));
+    const float ti = __fadd_rn(__fmul_rn(vr, ai), __fmul_rn(vi, ar));
+    float2 d = out[o];
+    d.x = __fadd_rn(d.x, tr); d.y = __fadd_rn(d.y, ti);
+    out[o] = d;
+  }
+};
+struct AddC8 {
+  double2* out; double ar, ai; bool conj;
+  __device__ __forceinline__ void operator()(int64_t o, const double2& v) const {
+    const double vr = v.x, vi = conj ? -v.y : v.y;
+    const double tr = __dsub_rn(__dmul_rn(vr, ar), __dmul_rn(vi, ai));
+    const double ti = __dadd_rn(__dmul_rn(vr, ai), __dmul_rn(vi, ar));
+    double2 d = out[o];
+    d.x = __dadd_rn(d.x, tr); d.y = __dadd_rn(d.y, ti);
+    out[o] = d;
+  }
+};
+
+double cmplx8_to_real8(double re, double im) {
+  // TALSH/tensor_algebra_cpu.F90:430-445
+  if (re != 0.0) return std::hypot(re, im) * (re > 0 ? 1.0 : -1.0);
+  return im;
+}
+
+}  // namespace
+
+double real_scale_factor(double re, double im) { return cmplx8_to_real8(re, im); }
+
+// Runs a permutation with the tiled engine, or the scatter kernel when the
+// plan builder declines the layout.
+template <typename E, typename Store>
+int run_permutation(int rank, const int* dims, const int* cptrn, const E* in, const Store& st,
+                    cudaStream_t s, bool force_scatter = false) {
+  if (!force_scatter) {
+    PermParams P;
+    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P);
+    if (e == 0) return launch_perm<E, Store>(P, in, st, s);
+    if (e != TB_ERR_NOT_IMPLEMENTED) return e;
+  }
+  return run_scatter<E, Store>(rank, dims, cptrn, in, st, s);
+}
+
+int tensor_copy_impl(int dtk, int rank, const int* dims, const int* cptrn, const void* in,
+                     void* out, int conj_bits, cudaStream_t s, bool scatter) {
+  const int es = elem_bytes(dtk);
+  if (!es || !in || !out) { set_error("tb_tensor_copy: bad data kind or null pointer"); return TB_ERR_INVALID_ARGS; }
+  int64_t vol;
+  if (int e = check_dims(rank, dims, &vol)) { set_error("tb_tensor_copy: bad extents"); return e; }
+  int ident[kMaxRank];
+  if (!cptrn) { for (int i = 0; i < rank; ++i) ident[i] = i + 1; cptrn = ident; }
+  bool conj = ((conj_bits & 1) ^ ((conj_bits >> 1) & 1)) && is_complex(dtk);
+  switch (es) {
+    case 4: return run_permutation<uint32_t>(rank, dims, cptrn, (const uint32_t*)in,
+                                             StoreCopy<uint32_t>{(uint32_t*)out}, s, scatter);
+    case 8:
+      if (conj) return run_permutation<uint64_t>(rank, dims, cptrn, (const uint64_t*)in,
+                                                 StoreConjC4{(uint64_t*)out}, s, scatter);
+      return run_permutation<uint64_t>(rank, dims, cptrn, (const uint64_t*)in,
+                                       StoreCopy<uint64_t>{(uint64_t*)out}, s, scatter);
+    case 16:
+      if (conj) return run_permutation<u128>(rank, dims, cptrn, (const u128*)in,
+                                             StoreConjC8{(u128*)out}, s, scatter);
+      return run_permutation<u128>(rank, dims, cptrn, (const u128*)in, StoreCopy<u128>{(u128*)out},
+                                   s, scatter);
+  }
+  return TB_ERR_INVALID_ARGS;
+}
+
+int tensor_add_impl(int dtk, int rank, const int* ldims, const int* cptrn, void* d, const void* l,
+                    double sr, double si, int conj_bits, cudaStream_t s) {
+  if (!elem_bytes(dtk) || !d || !l) { set_error("tb_tensor_add: bad data kind or null pointer"); return TB_ERR_INVALID_ARGS; }
+  int64_t vol;
+  if (int e = check_dims(rank, ldims, &vol)) { set_error("tb_tensor_add: bad extents"); return e; }
+  int ident[kMaxRank];
+  if (!cptrn) { for (int i = 0; i < rank; ++i) ident[i] = i + 1; cptrn = ident; }
+  bool lconj = ((conj_bits & 1) ^ ((conj_bits >> 1) & 1)) != 0;
+  switch (dtk) {
+    case kR4: {
+      const float a = (float)cmplx8_to_real8(sr, si);
+      return run_permutation<float>(rank, ldims, cptrn, (const float*)l, AddScalar<float>{(float*)d, a}, s);
+    }
+    case kR8: {
+      const double a = cmplx8_to_real8(sr, si);
+      return run_permutation<double>(rank, ldims, cptrn, (const double*)l, AddScalar<double>{(double*)d, a}, s);
+    }
+    case kC4:
+      return run_permutation<float2>(rank, ldims, cptrn, (const float2*)l,
+                                     AddC4{(float2*)d, (float)sr, (float)si, lconj}, s);
+    case kC8:
+      return run_permutation<double2>(rank, ldims, cptrn, (const double2*)l,
+                                      AddC8{(double2*)d, sr, si, lconj}, s);
+  }
+  return TB_ERR_INVALID_ARGS;
+}
+
+}  // namespace tb
+
+extern "C" int tb_tensor_copy(int data_kind, int rank, const int* in_dims, const int* cptrn,
+                              const void* in, void* out, int conj_bits, void* stream) {
+  return tb::tensor_copy_impl(data_kind, rank, in_dims, cptrn, in, out, conj_bits,
+                              (cudaStream_t)stream, false);
+}
+
+extern "C" int tb_tensor_copy_scatter(int data_kind, int rank, const int* in_dims, const int* cptrn,
+                                      const void* in, void* out, int conj_bits, void* stream) {
+  return tb::tensor_copy_impl(data_kind, rank, in_dims, cptrn, in, out, conj_bits,
+                              (cudaStream_t)stream, true);
+}
+
+extern "C" int tb_tensor_add(int data_kind, int rank, const int* l_dims, const int* cptrn, void* d,
+                             const void* l, double scale_real, double scale_imag, int conj_bits,
+                             void* stream) {
+  return tb::tensor_add_impl(data_kind, rank, l_dims, cptrn, d, l, scale_real, scale_imag, conj_bits,
+                             (cudaStream_t)stream);
+}

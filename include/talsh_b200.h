@@ -1,0 +1,150 @@
+/* talsh_b200.h -- device-level C ABI of the B200 tensor-algebra library.
+ *
+ * These entry points replace TAL-SH's NV-TAL device calls
+ * (TALSH/device_algebra.h:259-273, implemented in
+ * TALSH/tensor_algebra_gpu_nvidia.cu) with plain pointers and sizes: device
+ * pointers to dense tensor bodies in TAL-SH's "dlf" layout (dimension 1 is
+ * the fastest, complex numbers interleaved), extents as int arrays, digital
+ * index patterns exactly as get_contr_pattern_dig produces them
+ * (TALSH/tensor_algebra_cpu.F90:5307), the TAL-SH data kinds R4=4, R8=8,
+ * C4=14, C8=18, and an optional cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  Every call is asynchronous on that stream unless
+ * stated otherwise and returns 0 on success or a TB_ERR_* code; nothing falls
+ * back to the host.
+ *
+ * The talsh.h API (include/talsh.h) is built on top of these calls.
+ */
+#ifndef TALSH_B200_H_
+#define TALSH_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (0 = success). */
+#define TB_SUCCESS 0
+#define TB_ERR_INVALID_ARGS 1     /* bad pointer, rank, extent, data kind or pattern */
+#define TB_ERR_PATTERN 2          /* malformed symbolic or digital index pattern */
+#define TB_ERR_CUDA 3             /* CUDA runtime error (see tb_last_error) */
+#define TB_ERR_NOT_IMPLEMENTED 4  /* valid request this library does not execute */
+#define TB_ERR_DEVICE 5           /* a kernel recorded a device-side error */
+#define TB_ERR_NO_MEMORY 6        /* scratch allocation failed (maps to TRY_LATER) */
+#define TB_ERR_LIMIT 7            /* request exceeds a documented limit */
+
+/* Contraction methods. */
+#define TB_METHOD_AUTO 0      /* plan selector decides */
+#define TB_METHOD_TTGT 1      /* plain: permute, GEMM in the tensor's own type, permute back */
+#define TB_METHOD_FUSED 2     /* tensor cores: fused gather/epilogue, split-BF16 or INT8 slices */
+
+/* Contraction plan (all-zero = automatic). */
+typedef struct {
+  int method;      /* TB_METHOD_* */
+  int slices;      /* INT8 slices per FP64 operand for R8/C8 fused (0 = default) */
+  int tile_n;      /* tensor-core N tile: 0 (default), 128 or 256 */
+  int bf16_terms;  /* split-BF16 products for R4/C4 fused: 0 (default = 3) */
+  int reserved[4];
+} tb_plan_t;
+
+/* Last error message of the calling thread ("" if none). */
+const char* tb_last_error(void);
+
+/* Number of kernels this library has launched in the process (all threads). */
+long long tb_launch_count(void);
+
+/* Opt-in CUDA-event timing of the dominant GEMM kernel launches made by the
+ * calling thread (events on the launching stream).  tb_timing_read
+ * synchronises on the recorded events, returns their summed duration and
+ * count, and clears the record. */
+int tb_timing_enable(int on);
+int tb_timing_read(double* total_ms, int* count);
+
+/* Select and initialise a GPU for the calling thread (kind-specific id). */
+int tb_device_init(int gpu);
+/* Reads and clears the device-side error word; returns TB_ERR_DEVICE if set. */
+int tb_device_check(void* stream);
+
+/* Valid data kind -> element size in bytes (0 if invalid). */
+int tb_data_kind_size(int data_kind);
+
+/* Parse a symbolic pattern ("D(a,b)+=L(c,a)*R(c,b)") into TAL-SH's digital
+ * form.  Replaces talsh_get_contr_ptrn_str2dig (TALSH/talshf.F90:619).
+ * cptrn must hold 2*MAX_TENSOR_RANK ints.  rrank is -1 for unary patterns. */
+int tb_parse_pattern(const char* pattern, int* cptrn, int* drank, int* lrank, int* rrank,
+                     int* conj_bits);
+
+/* out = permute(in): copy with an O2N index permutation given as the digital
+ * copy pattern (1-based, cptrn[i] = destination position of input dim i).
+ * conj_bits bit0 (D) xor bit1 (L) conjugates complex data.  Bit-exact.
+ * Replaces gpu_tensor_block_copy (TALSH/tensor_algebra_gpu_nvidia.cu:4806;
+ * kernel gpu_tensor_block_copy_dlf__ :1126). */
+int tb_tensor_copy(int data_kind, int rank, const int* in_dims, const int* cptrn,
+                   const void* in, void* out, int conj_bits, void* stream);
+
+/* Naive one-element-per-thread scatter permutation (the reference's
+ * gpu_tensor_block_copy_scatter_dlf__, :2173).  Same result as tb_tensor_copy. */
+int tb_tensor_copy_scatter(int data_kind, int rank, const int* in_dims, const int* cptrn,
+                           const void* in, void* out, int conj_bits, void* stream);
+
+/* d = d + permute(l) * scale, one fused pass, bit-exact against the
+ * reference's permute-then-add (two roundings, no FMA).  l_dims are the
+ * extents of l; cptrn is the digital addition pattern (O2N, 1-based).
+ * Replaces gpu_tensor_block_add (TALSH/tensor_algebra_gpu_nvidia.cu:5203). */
+int tb_tensor_add(int data_kind, int rank, const int* l_dims, const int* cptrn, void* d,
+                  const void* l, double scale_real, double scale_imag, int conj_bits,
+                  void* stream);
+
+/* d = value (gpu_tensor_block_init, :4262). */
+int tb_tensor_init(int data_kind, size_t volume, void* d, double val_real, double val_imag,
+                   void* stream);
+
+/* d = d * scale (gpu_tensor_block_scale, :4525). */
+int tb_tensor_scale(int data_kind, size_t volume, void* d, double scale_real,
+                    double scale_imag, void* stream);
+
+/* Deterministic norms: which = 1 -> sum |x|, which = 2 -> sum |x|^2, written
+ * to *result (host memory); this call synchronises the stream.  Device-side
+ * counterpart of talshTensorImageNorm1_cpu (TALSH/talshc.cpp:6207). */
+int tb_tensor_norm(int data_kind, size_t volume, const void* d, int which, double* result,
+                   void* stream);
+
+/* Tensor contraction D = beta*D + alpha * op(L) * op(R) with beta = 1 when
+ * accumulative != 0, else 0.  cptrn is the digital contraction pattern
+ * (lrank+rrank entries), conj_bits bit0 D, bit1 L, bit2 R.  plan may be
+ * NULL.  Replaces gpu_tensor_block_contract_dlf
+ * (TALSH/tensor_algebra_gpu_nvidia.cu:5847). */
+int tb_tensor_contract(const int* cptrn, int data_kind, int drank, const int* d_dims, void* d,
+                       int lrank, const int* l_dims, const void* l, int rrank,
+                       const int* r_dims, const void* r, double alpha_real, double alpha_imag,
+                       int conj_bits, int accumulative, const tb_plan_t* plan, void* stream);
+
+/* Contraction with a symbolic pattern (parses, then tb_tensor_contract). */
+int tb_tensor_contract_str(const char* pattern, int data_kind, int drank, const int* d_dims,
+                           void* d, int lrank, const int* l_dims, const void* l, int rrank,
+                           const int* r_dims, const void* r, double alpha_real,
+                           double alpha_imag, int accumulative, const tb_plan_t* plan,
+                           void* stream);
+
+/* Seeded U[lo,hi) fill on the device (splitmix64 stream, 53-bit fractions);
+ * complex kinds fill real and imaginary parts from consecutive draws. */
+int tb_fill_uniform(int data_kind, size_t volume, void* d, uint64_t seed, double lo, double hi,
+                    void* stream);
+
+/* Statistics of the last tb_tensor_contract on this thread. */
+typedef struct {
+  int method;        /* TB_METHOD_TTGT or TB_METHOD_FUSED actually executed */
+  int slices;        /* INT8 slices (R8/C8 fused) */
+  int passes;        /* accumulator passes of the tensor-core GEMM */
+  int gemm_launches; /* GEMM kernel launches */
+  long long m, n, k; /* matricized sizes (real-expanded for complex on tensor cores) */
+  double flops;      /* 2*M*N*K (real) or 8*M*N*K (complex), the reference's accounting */
+} tb_contract_stats_t;
+int tb_last_contract_stats(tb_contract_stats_t* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TALSH_B200_H_ */

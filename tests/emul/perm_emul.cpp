@@ -1,0 +1,111 @@
+// CPU emulation of perm_tile_kernel's index arithmetic (exatensor_b200/csrc/
+// tb_permute.cuh) driven by the product's own plan builder (tb_perm_plan.cpp).
+// For each case it replays the kernel's tile loop, load phase and store phase
+// thread by thread, checks every shared-memory and table index against its
+// bound, and checks that each output element is written exactly once with the
+// input element a reference O2N permutation puts there.
+// Usage: perm_emul <es> <rank> d1..dn p1..pn  -> prints "OK <tiles> <V>" or an error.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "../../exatensor_b200/csrc/tb_perm_plan.h"
+
+using namespace tb;
+
+int main(int argc, char** argv) {
+  if (argc < 3) return 2;
+  const int es = atoi(argv[1]);
+  const int rank = atoi(argv[2]);
+  std::vector<int> dims(rank), perm(rank);
+  for (int i = 0; i < rank; ++i) dims[i] = atoi(argv[3 + i]);
+  for (int i = 0; i < rank; ++i) perm[i] = atoi(argv[3 + rank + i]);
+  static PermParams P;
+  int e = build_perm_plan_o2n(es, rank, dims.data(), perm.data(), &P);
+  if (e) { printf("DECLINED %d\n", e); return 0; }
+  long long vol = 1;
+  for (int d : dims) vol *= d;
+  // reference output positions
+  std::vector<long long> oe(rank), pos(rank), sout(rank);
+  for (int i = 0; i < rank; ++i) oe[perm[i] - 1] = dims[i];
+  long long s = 1;
+  for (int q = 0; q < rank; ++q) { pos[q] = s; s *= oe[q]; }
+  for (int i = 0; i < rank; ++i) sout[i] = pos[perm[i] - 1];
+  std::vector<long long> ref(vol);  // ref[out] = in index
+  for (long long i = 0; i < vol; ++i) {
+    long long r = i, o = 0;
+    for (int d = 0; d < rank; ++d) { long long x = r % dims[d]; r /= dims[d]; o += x * sout[d]; }
+    ref[o] = i;
+  }
+  std::vector<long long> out(vol, -1);
+  const int V = P.V, LA = P.LA, LB = P.LB, ps = P.pad_shift;
+  const long long bufn = (long long)V + (V >> ps) + 1;
+  std::vector<long long> buf(bufn, -1);
+  auto fail = [&](const char* m, long long a, long long b) { printf("FAIL %s %lld %lld\n", m, a, b); exit(1); };
+  if (P.nA > kMaxChunks || P.nB > kMaxChunks || P.ejf_n > kMaxEjf) fail("table size", P.nA, P.nB);
+  if ((long long)P.LA * P.nA != V || (long long)P.LB * P.nB != V) fail("chunk product", LA, LB);
+  for (long long tile = 0; tile < P.ntiles; ++tile) {
+    long long in_base = 0, out_base = 0;
+    int rem_a = 1 << 30, rem_b = 1 << 30;
+    unsigned long long r = tile;
+    for (int g = 0; g < P.ngd; ++g) {
+      unsigned long long q = P.gdiv[g].div(r);
+      if (q != r / (unsigned long long)P.gext[g]) fail("fastdiv", r, P.gext[g]);
+      long long x = (long long)(r - q * P.gext[g]);
+      r = q;
+      int d = P.gdim[g];
+      long long org = x * P.tile[d];
+      in_base += org * P.sin[d];
+      out_base += org * P.sout[d];
+      long long rem = P.dims[d] - org;
+      if (d == P.pa) rem_a = (int)(rem < P.tile[d] ? rem : P.tile[d]);
+      if (d == P.pb) rem_b = (int)(rem < P.tile[d] ? rem : P.tile[d]);
+    }
+    const bool full = (P.pa < 0 || rem_a >= P.tile[P.pa]) && (P.pb < 0 || rem_b >= P.tile[P.pb]);
+    std::fill(buf.begin(), buf.end(), -1);
+    for (int ee = 0; ee < V; ++ee) {
+      int c = (int)fdiv32((uint32_t)ee, P.la_magic, P.la_shift);
+      if (c != ee / LA) fail("fdiv32 LA", ee, LA);
+      int j = ee - c * LA;
+      bool ok = true;
+      if (!full) {
+        if (P.pa >= 0) { int da = j / P.prodA; ok = da < rem_a; if (P.pb == P.pa) ok = ok && da < rem_b; }
+        if (P.pb >= 0 && P.pb != P.pa) ok = ok && P.ld_dpb[c] < rem_b;
+      }
+      if (ok) {
+        long long src = in_base + P.ld_base[c] + j;
+        if (src < 0 || src >= vol) fail("load oob", src, tile);
+        long long p = ee + (ee >> ps);
+        if (p >= bufn) fail("smem oob", p, bufn);
+        buf[p] = src;
+      }
+    }
+    for (int f = 0; f < V; ++f) {
+      int c = (int)fdiv32((uint32_t)f, P.lb_magic, P.lb_shift);
+      int j = f - c * LB;
+      int q = (int)fdiv32((uint32_t)j, P.pb_magic, P.pb_shift);
+      if (q != j / P.ejf_n) fail("fdiv32 prodB", j, P.ejf_n);
+      bool ok = true;
+      if (!full) {
+        if (P.pb >= 0) { ok = q < rem_b; if (P.pa == P.pb) ok = ok && q < rem_a; }
+        if (P.pa >= 0 && P.pa != P.pb) ok = ok && P.st_dpa[c] < rem_a;
+      }
+      if (!ok) continue;
+      int idx = j - q * P.ejf_n;
+      if (idx < 0 || idx >= P.ejf_n) fail("ejf oob", idx, P.ejf_n);
+      int ee = P.st_ebase[c] + P.ejf[idx] + q * P.ej_pb_stride;
+      if (ee < 0 || ee >= V) fail("tile index oob", ee, V);
+      long long p = ee + (ee >> ps);
+      long long dst = out_base + P.st_base[c] + j;
+      if (dst < 0 || dst >= vol) fail("store oob", dst, tile);
+      if (buf[p] < 0) fail("store reads unloaded smem", ee, tile);
+      if (out[dst] != -1) fail("double write", dst, tile);
+      out[dst] = buf[p];
+    }
+  }
+  for (long long o = 0; o < vol; ++o) {
+    if (out[o] != ref[o]) fail("wrong value at", o, out[o]);
+  }
+  printf("OK %lld %d %d %d\n", (long long)P.ntiles, V, LA, LB);
+  return 0;
+}
