@@ -33,17 +33,23 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   for (int i = 0; i < r; ++i) Q[i] = i;
   std::stable_sort(Q.begin(), Q.end(), [&](int x, int y) { return SO[x] < SO[y]; });
   if (SO[Q[0]] != 1) return TB_ERR_NOT_IMPLEMENTED;
-  const int64_t T = std::max<int64_t>(1, 128 / es);
+  const int64_t T = std::max<int64_t>(1, 256 / es);
   const int64_t Vmin = 16384 / es, Vmax = 32768 / es;
   std::vector<int64_t> t(r, 1);
   auto cdiv = [](int64_t x, int64_t y) { return (x + y - 1) / y; };
+  // Even split: the smallest extent >= want that tiles D in the same number
+  // of pieces as want does (76 with want 32 -> 26: 26+26+24, not 32+32+12).
+  auto even = [&](int64_t D, int64_t want) {
+    want = std::max<int64_t>(1, std::min(D, want));
+    return cdiv(D, cdiv(D, want));
+  };
   // 2. load block: input dims 0..a
   int a = 0;
   {
     int64_t vol = 1;
     for (a = 0; a < r; ++a) {
       if (vol * D[a] <= T && a < r - 1) { t[a] = D[a]; vol *= D[a]; continue; }
-      t[a] = std::min(D[a], cdiv(T, vol));
+      t[a] = even(D[a], cdiv(T, vol));
       break;
     }
     if (a == r) a = r - 1;
@@ -62,13 +68,13 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
         continue;
       }
       if (i == a) {
-        t[a] = std::max(t[a], std::min(D[a], cdiv(T, volB)));
+        t[a] = std::max(t[a], even(D[a], cdiv(T, volB)));
         inB[a] = 1; blast = a; volB *= t[a];
         if (t[a] == D[a] && volB < T) continue;  // became whole: the run may grow further
         break;
       }
       if (volB * D[i] <= T) { t[i] = D[i]; inB[i] = 1; blast = i; volB *= D[i]; continue; }
-      t[i] = std::min(D[i], cdiv(T, volB));
+      t[i] = even(D[i], cdiv(T, volB));
       inB[i] = 1; blast = i; volB *= t[i];
       break;
     }
@@ -88,22 +94,59 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
       const int d = which == 0 ? a : blast;
       if (t[d] < D[d]) {
         const int64_t f = std::min(cdiv(D[d], t[d]), cdiv(Vmin, V));
-        if (f > 1) { t[d] = std::min(D[d], t[d] * f); grown = true; }
+        if (f > 1) { const int64_t nt = even(D[d], t[d] * f); if (nt > t[d]) { t[d] = nt; grown = true; } }
       }
     }
     if (!grown) break;
   }
-  // 5. chunk structure
+  // 5. bulk-copy alignment: when the load block ends on a whole dimension and
+  // its rows are not a multiple of 16 bytes, extend it into the next input
+  // dimension by the smallest extent that makes them so (shrinking the store
+  // block's partial extent if the tile would grow past Vmax).
+  {
+    int64_t pA = 1;
+    for (int i = 0; i < a; ++i) pA *= D[i];
+    if ((pA * t[a] * es) % 16 != 0 && t[a] == D[a] && a + 1 < r) {
+      const int64_t pA2 = pA * D[a];
+      int64_t g = 16, x = pA2 * es;
+      while (x % 2 == 0 && g > 1) { x /= 2; g /= 2; }  // g = 16 / gcd(pA2*es, 16)
+      int64_t nt = t[a + 1] > 1 ? cdiv(t[a + 1], g) * g : g;
+      if (nt <= D[a + 1]) {
+        int64_t Vn = vol_of() / t[a + 1] * nt;
+        if (Vn > Vmax && blast > a + 1 && t[blast] > 1) {  // only a store dim outside the load block
+          const int64_t pBfull = [&]() { int64_t p = 1; for (int j = 0; j < r; ++j) if (inB[j] && j != blast) p *= t[j]; return p; }();
+          const int64_t tb = std::max<int64_t>(cdiv(T, pBfull), t[blast] * Vmax / Vn);
+          if (tb < t[blast]) { t[blast] = tb; Vn = vol_of() / t[a + 1] * nt; }
+        }
+        if (Vn <= Vmax) { t[a + 1] = nt; a = a + 1; }
+      }
+    }
+  }
+  // 6. chunk structure
   const int pa = (t[a] < D[a]) ? a : -1;
   const int pb = (t[blast] < D[blast]) ? blast : -1;
   int64_t prodA = 1;
   for (int i = 0; i < a; ++i) prodA *= D[i];
   const int64_t LA = prodA * t[a];
-  // tile index strides (input-order enumeration: load block, then rest dims)
+  // Shared-memory layout: load chunk c occupies row c with stride lap.  The
+  // row stride is padded so that transposed reads (consecutive output
+  // elements one row apart) spread over the banks: an odd number of 4-byte
+  // words per row, or for bulk-copy rows an odd number of 16-byte units.
+  const bool bulk_rows = (LA * es) % 16 == 0;
+  int64_t lap;
+  if (bulk_rows) {
+    const int64_t u = 16 / es;  // elements per 16 bytes (>= 1)
+    lap = LA;
+    if (((lap * es) / 16) % 2 == 0) lap += u;
+  } else {
+    lap = (LA % 2 == 1) ? LA : LA + 1;
+  }
+  // position strides (load block within a row, rest dims across rows)
   std::vector<int64_t> est(r, 0);
   {
     int64_t s = 1;
     for (int i = 0; i <= a; ++i) { est[i] = s; s *= t[i]; }
+    s = lap;
     for (int i = a + 1; i < r; ++i) if (t[i] > 1) { est[i] = s; s *= t[i]; }
   }
   const int64_t V = vol_of();
@@ -116,12 +159,23 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   int64_t prodB = 1;
   for (int d : Bdims) if (d != blast) prodB *= t[d];
   const int64_t nA = V / LA, nB = V / LB;
-  if (nA > kMaxChunks || nB > kMaxChunks || prodB > kMaxEjf || V > (int64_t)1 << 30)
+  if (nA > kMaxChunks || nB > kMaxChunks || prodB > kMaxEjf || V > (int64_t)1 << 28)
     return TB_ERR_NOT_IMPLEMENTED;
   P.rank = r; P.V = (int)V; P.LA = (int)LA; P.nA = (int)nA; P.LB = (int)LB; P.nB = (int)nB;
   P.pa = pa; P.pb = pb; P.prodA = (int)prodA; P.prodB = (int)prodB; P.ejf_n = (int)prodB;
   P.ej_pb_stride = (int)est[blast];
-  P.pad_shift = es == 4 ? 5 : es == 8 ? 4 : 3;
+  P.lap = (int)lap;
+  {
+    // bulk-copy eligibility: rows of whole 16-byte units that start on 16-byte
+    // boundaries everywhere, and a tensor whose byte size is a multiple of 16
+    // (so rounding a partial row up to 16 bytes never leaves the tensor)
+    int64_t tot = 1;
+    for (int i = 0; i < r; ++i) tot *= D[i];
+    P.total = tot;
+    bool ok = bulk_rows && (tot * es) % 16 == 0 && (prodA * t[a] * es) % 16 == 0;
+    for (int i = a + 1; i < r; ++i) if ((SI[i] * es) % 16 != 0) ok = false;
+    P.tma_ok = ok ? 1 : 0;
+  }
   for (int i = 0; i < r; ++i) { P.dims[i] = D[i]; P.tile[i] = t[i]; P.sin[i] = SI[i]; P.sout[i] = SO[i]; }
   magic32((uint32_t)LA, &P.la_magic, &P.la_shift);
   magic32((uint32_t)LB, &P.lb_magic, &P.lb_shift);

@@ -29,7 +29,9 @@ struct PermParams {
   int prodA, prodB;          // digit(pa) = j / prodA in a load chunk; digit(last store dim) = j' / prodB
   int ejf_n;                 // entries of ejf (= prodB)
   int ej_pb_stride;          // tile-index stride of the last store-block dim
-  int pad_shift;             // smem padding: one element per (1 << pad_shift)
+  int lap;                   // shared-memory row stride (elements) of a load chunk
+  int tma_ok;                // 1: load chunks can be moved by 16-byte-aligned bulk copies
+  int64_t total;             // tensor volume (elements)
   int ngd;                   // grid dims
   int64_t ntiles;
   int64_t dims[kPlanMaxRank];
@@ -45,9 +47,9 @@ struct PermParams {
   int64_t ld_base[kMaxChunks];  // input offset of load chunk c (tile-relative)
   int16_t ld_dpb[kMaxChunks];   // digit of pb in load chunk c (-1: pb inside the chunk or none)
   int64_t st_base[kMaxChunks];  // output offset of store chunk c'
-  int32_t st_ebase[kMaxChunks]; // tile index base of store chunk c'
+  int32_t st_ebase[kMaxChunks]; // shared-memory position base of store chunk c'
   int16_t st_dpa[kMaxChunks];   // digit of pa in store chunk c' (-1: pa inside the chunk or none)
-  int32_t ejf[kMaxEjf];         // tile index of position j' % prodB inside a store chunk
+  int32_t ejf[kMaxEjf];         // shared-memory position of j' % prodB inside a store chunk
 };
 
 // Host-side plan builder.  dims/sin/sout describe the input dims (input
@@ -55,6 +57,8 @@ struct PermParams {
 // TB_ERR code.  Dims of extent 1 are dropped and mergeable neighbours fused.
 int build_perm_plan(int es, int rank, const int64_t* dims, const int64_t* sin, const int64_t* sout,
                     PermParams* p);
+// Bytes of one pipeline stage (a tile in shared memory).
+inline int64_t perm_stage_bytes(const PermParams& P) { return (int64_t)P.nA * P.lap * P.es; }
 // Convenience: plain O2N permutation of a dense tensor (cptrn 1-based).
 int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p);
 

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+#include <algorithm>
 #include "../../exatensor_b200/csrc/tb_perm_plan.h"
 
 using namespace tb;
@@ -38,10 +39,11 @@ int main(int argc, char** argv) {
     ref[o] = i;
   }
   std::vector<long long> out(vol, -1);
-  const int V = P.V, LA = P.LA, LB = P.LB, ps = P.pad_shift;
-  const long long bufn = (long long)V + (V >> ps) + 1;
+  const int V = P.V, LA = P.LA, LB = P.LB;
+  const long long bufn = (long long)P.nA * P.lap;
   std::vector<long long> buf(bufn, -1);
   auto fail = [&](const char* m, long long a, long long b) { printf("FAIL %s %lld %lld\n", m, a, b); exit(1); };
+  if (P.lap < LA) fail("row stride", P.lap, LA);
   if (P.nA > kMaxChunks || P.nB > kMaxChunks || P.ejf_n > kMaxEjf) fail("table size", P.nA, P.nB);
   if ((long long)P.LA * P.nA != V || (long long)P.LB * P.nB != V) fail("chunk product", LA, LB);
   for (long long tile = 0; tile < P.ntiles; ++tile) {
@@ -75,37 +77,64 @@ int main(int argc, char** argv) {
       if (ok) {
         long long src = in_base + P.ld_base[c] + j;
         if (src < 0 || src >= vol) fail("load oob", src, tile);
-        long long p = ee + (ee >> ps);
+        long long p = (long long)c * P.lap + j;
         if (p >= bufn) fail("smem oob", p, bufn);
         buf[p] = src;
       }
     }
-    for (int f = 0; f < V; ++f) {
-      int c = (int)fdiv32((uint32_t)f, P.lb_magic, P.lb_shift);
-      int j = f - c * LB;
-      int q = (int)fdiv32((uint32_t)j, P.pb_magic, P.pb_shift);
-      if (q != j / P.ejf_n) fail("fdiv32 prodB", j, P.ejf_n);
-      bool ok = true;
-      if (!full) {
-        if (P.pb >= 0) { ok = q < rem_b; if (P.pa == P.pb) ok = ok && q < rem_a; }
-        if (P.pa >= 0 && P.pa != P.pb) ok = ok && P.st_dpa[c] < rem_a;
+    if (P.tma_ok) {
+      // bulk-copy replay: each valid row is copied with its byte length rounded
+      // up to 16; the copy must stay inside the tensor and inside its smem row
+      for (int c = 0; c < P.nA; ++c) {
+        bool ok = true;
+        if (!full && P.pb >= 0 && P.pb != P.pa) ok = P.ld_dpb[c] < rem_b;
+        if (!ok) continue;
+        long long len = (!full && P.pa >= 0) ? (long long)P.prodA * std::min(rem_a, P.pb == P.pa ? rem_b : rem_a)
+                                              : (long long)LA;
+        long long bytes = (len * es + 15) / 16 * 16;
+        long long src = in_base + P.ld_base[c];
+        if ((src * es) % 16 != 0) fail("bulk source misaligned", src, c);
+        if (src * es + bytes > vol * es) fail("bulk copy leaves the tensor", src, bytes);
+        if (bytes > (long long)P.lap * es) fail("bulk copy overflows its row", bytes, P.lap);
+        if (((long long)c * P.lap * es) % 16 != 0) fail("bulk destination misaligned", c, P.lap);
       }
-      if (!ok) continue;
-      int idx = j - q * P.ejf_n;
-      if (idx < 0 || idx >= P.ejf_n) fail("ejf oob", idx, P.ejf_n);
-      int ee = P.st_ebase[c] + P.ejf[idx] + q * P.ej_pb_stride;
-      if (ee < 0 || ee >= V) fail("tile index oob", ee, V);
-      long long p = ee + (ee >> ps);
-      long long dst = out_base + P.st_base[c] + j;
-      if (dst < 0 || dst >= vol) fail("store oob", dst, tile);
-      if (buf[p] < 0) fail("store reads unloaded smem", ee, tile);
-      if (out[dst] != -1) fail("double write", dst, tile);
-      out[dst] = buf[p];
+    }
+    // store phase as perm_store: 8 warps, (chunk, block) units, strided positions
+    {
+      const int lpc = P.LB >= 24 ? 32 : (P.LB >= 12 ? 16 : 8), cpw = 32 / lpc;
+      const int blk = P.LB <= 512 ? P.LB : (512 / P.ejf_n) * P.ejf_n;
+      if (blk < 1 || (blk != P.LB && blk % P.ejf_n != 0)) fail("block not a multiple of prodB", blk, P.ejf_n);
+      const int nblk = (P.LB + blk - 1) / blk;
+      const int qlim = (!full && P.pb >= 0) ? (P.pa == P.pb ? std::min(rem_a, rem_b) : rem_b) : (1 << 30);
+      const bool dpa_check = !full && P.pa >= 0 && P.pa != P.pb;
+      const int units = P.nB * nblk;
+      for (int warp = 0; warp < 8; ++warp)
+        for (int lane = 0; lane < 32; ++lane) {
+          const int sub = lane / lpc, l = lane % lpc;
+          for (int u = warp * cpw + sub; u < units; u += 8 * cpw) {
+            const int c = u / nblk, j0 = (u - c * nblk) * blk;
+            if (dpa_check && P.st_dpa[c] >= rem_a) continue;
+            const int jmax = std::min(j0 + blk, LB);
+            for (int j = j0 + l; j < jmax; j += lpc) {
+              const int q = (int)fdiv32((uint32_t)j, P.pb_magic, P.pb_shift);
+              if (q != j / P.ejf_n) fail("fdiv32 prodB", j, P.ejf_n);
+              if (q >= qlim) break;
+              const long long ee = (long long)P.st_ebase[c] + P.ejf[j - q * P.ejf_n] + (long long)q * P.ej_pb_stride;
+              if (P.ejf_n == 1 && ee != (long long)P.st_ebase[c] + (long long)j * P.ej_pb_stride) fail("pB1 form", j, c);
+              if (ee < 0 || ee >= bufn) fail("smem position oob", ee, bufn);
+              const long long dst = out_base + P.st_base[c] + j;
+              if (dst < 0 || dst >= vol) fail("store oob", dst, tile);
+              if (buf[ee] < 0) fail("store reads unloaded smem", ee, tile);
+              if (out[dst] != -1) fail("double write", dst, tile);
+              out[dst] = buf[ee];
+            }
+          }
+        }
     }
   }
   for (long long o = 0; o < vol; ++o) {
     if (out[o] != ref[o]) fail("wrong value at", o, out[o]);
   }
-  printf("OK %lld %d %d %d\n", (long long)P.ntiles, V, LA, LB);
+  printf("OK %lld %d %d %d tma=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok);
   return 0;
 }

@@ -44,7 +44,7 @@ def test_all_rank4_perms(emul, es):
 @pytest.mark.parametrize("es", [4, 8, 16])
 def test_random_shapes(emul, es):
     rng = random.Random(1234 + es)
-    for _ in range(60):
+    for _ in range(150):
         rank = rng.randint(1, 6)
         dims = []
         for _ in range(rank):
@@ -71,3 +71,4 @@ def test_skewed_and_large_leading(emul):
     run(emul, 4, [5000, 7, 3], [1, 3, 2])
     run(emul, 8, [4099, 5], [2, 1])
     run(emul, 16, [1, 33, 1, 17], [2, 4, 1, 3])
+    run(emul, 8, [13, 5, 5, 16, 10, 5], [2, 5, 3, 4, 6, 1])  # store block inside the load block
