@@ -66,8 +66,8 @@ __device__ __forceinline__ double pow2d(int e) {
 template <int BN, bool I8, int EPI>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_constant__ TcGemmParams P) {
   using namespace sm100;
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* smA = base;                                    // [stages][128 rows][128 B]
   unsigned char* smB = base + (size_t)kStagesTC * 128 * 128;    // [stages][BN rows][128 B]
   TcSmemBarriers* bars = (TcSmemBarriers*)(smB + (size_t)kStagesTC * BN * 128);

@@ -1,0 +1,101 @@
+"""GPU parity of the tensor-core contraction (TB_METHOD_FUSED): INT8-slice
+FP64 (R8/C8) and split-BF16 FP32 (R4/C4) through tcgen05, against the
+double-double FP64 oracle.
+
+Tolerances (relative Frobenius error vs the oracle), stated per data kind:
+  R8/C8: 1e-12 with the default 7 slices
+  R4/C4: 1e-4  (3-term split-BF16; its products keep about 16 mantissa bits)
+"""
+import numpy as np
+import pytest
+
+import exatensor_b200 as XB
+import oracle as O
+from tests.test_gpu_contract import oracle_dd, run_gpu, shapes
+from tests.test_gpu_permute import rand_host
+
+pytestmark = pytest.mark.gpu
+TOL = {O.R8: 1e-12, O.C8: 1e-12, O.R4: 1e-4, O.C4: 1e-4}
+
+
+def fused(xt, dev, pattern, ext, dtk, alpha=1.0, accumulative=True, plan=None, seed=1):
+    ddims, ldims, rdims = shapes(pattern, ext)
+    vol = lambda s: int(np.prod(s)) if s else 1
+    d, l, r = rand_host(dtk, vol(ddims), seed), rand_host(dtk, vol(ldims), seed + 1), rand_host(dtk, vol(rdims), seed + 2)
+    ref = oracle_dd(pattern, d, ddims, l, ldims, r, rdims, alpha, accumulative)
+    dd, ld, rd = dev.put(d), dev.put(l), dev.put(r)
+    xt.tensor_contract(pattern, dtk, ddims, dd.data_ptr(), ldims, ld.data_ptr(), rdims, rd.data_ptr(), alpha,
+                       accumulative=accumulative, plan=plan or xt.make_plan(XB.METHOD_FUSED), stream=dev.stream())
+    got = dev.get(dd, d.dtype, d.size)
+    xt.device_check(dev.stream())
+    st = xt.last_contract_stats()
+    assert st.method == XB.METHOD_FUSED
+    return O.rel_frobenius(got, ref), st
+
+
+def test_fused_r8_square(xt, dev):
+    err, st = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 256, "j": 256, "k": 256}, O.R8)
+    assert err <= TOL[O.R8], err
+    assert st.slices == 7 and st.passes >= 7
+
+
+@pytest.mark.parametrize("dtk", [O.R8, O.R4, O.C8, O.C4])
+def test_fused_padded_shapes(xt, dev, dtk):
+    err, _ = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 130, "j": 70, "k": 200}, dtk, alpha=0.75)
+    assert err <= TOL[dtk], err
+
+
+@pytest.mark.parametrize("dtk", [O.R8, O.R4, O.C8, O.C4])
+@pytest.mark.parametrize("pattern,ext", [
+    ("D(a,b,c,d)+=L(c,k,a,l)*R(l,d,k,b)", {"a": 12, "b": 11, "c": 13, "d": 10, "k": 9, "l": 14}),
+    ("D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)", {"a": 16, "b": 16, "c": 16, "d": 16, "i": 8, "j": 8}),
+    ("D(a,i,b,j)+=L(a,k,c,i)*R(c,b,k,j)", {"a": 16, "b": 16, "c": 16, "i": 8, "j": 8, "k": 8}),
+    ("D(j,i)+=L(i,k)*R(j,k)", {"i": 300, "j": 200, "k": 128}),
+])
+def test_fused_tensor_patterns(xt, dev, dtk, pattern, ext):
+    for accumulative, alpha in ((True, 0.5), (False, -1.25 + (0.5j if dtk in (O.C4, O.C8) else 0))):
+        err, _ = fused(xt, dev, pattern, ext, dtk, alpha, accumulative)
+        assert err <= TOL[dtk], (pattern, accumulative, err)
+
+
+@pytest.mark.parametrize("dtk", [O.C8, O.C4])
+@pytest.mark.parametrize("pattern", ["D(a,b)+=L+(k,a)*R(k,b)", "D(a,b)+=L(k,a)*R+(k,b)", "D+(a,b)+=L(k,a)*R(k,b)"])
+def test_fused_conjugation(xt, dev, dtk, pattern):
+    err, _ = fused(xt, dev, pattern, {"a": 150, "b": 90, "k": 170}, dtk, alpha=0.7 - 0.2j)
+    assert err <= TOL[dtk], err
+
+
+@pytest.mark.parametrize("slices,bound", [(4, 1e-6), (5, 1e-8), (6, 1e-10), (8, 1e-13)])
+def test_slice_count_accuracy(xt, dev, slices, bound):
+    """Fewer slices trade accuracy for speed; every count stays within its bound."""
+    err, st = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 256, "j": 192, "k": 320}, O.R8,
+                    plan=xt.make_plan(XB.METHOD_FUSED, slices=slices))
+    assert st.slices == slices
+    assert err <= bound, err
+
+
+def test_bf16_three_and_four_terms(xt, dev):
+    """The hi*lo cross terms carry the accuracy; the lo*lo term adds nothing
+    measurable because the two-part split itself keeps ~16 mantissa bits."""
+    e3, _ = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 256, "j": 256, "k": 512}, O.R4,
+                  plan=xt.make_plan(XB.METHOD_FUSED, bf16_terms=3))
+    e4, _ = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 256, "j": 256, "k": 512}, O.R4,
+                  plan=xt.make_plan(XB.METHOD_FUSED, bf16_terms=4))
+    assert e3 <= 1e-4 and e4 <= 1e-4
+    assert e4 <= 1.2 * e3
+
+
+def test_tile_n_128_and_256_agree(xt, dev):
+    ext = {"i": 256, "j": 512, "k": 256}
+    e1, _ = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", ext, O.R8, plan=xt.make_plan(XB.METHOD_FUSED, tile_n=128))
+    e2, _ = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", ext, O.R8, plan=xt.make_plan(XB.METHOD_FUSED, tile_n=256))
+    assert e1 <= TOL[O.R8] and e2 <= TOL[O.R8]
+
+
+def test_kat_single_block_40(xt, dev):
+    """The 40^4 single-block contraction with constant inputs (closed form)."""
+    pattern = "D(a,b,c,d)+=L(c,k,a,l)*R(l,d,k,b)"
+    dims = [40] * 4
+    d = np.zeros(40 ** 4); l = np.full(40 ** 4, 0.01); r = np.full(40 ** 4, 0.001)
+    got = run_gpu(xt, dev, pattern, d, dims, l, dims, r, dims, 0.5, True, XB.METHOD_FUSED)
+    assert np.allclose(got, 1600 * 0.01 * 0.001 * 0.5, rtol=1e-12, atol=0)
