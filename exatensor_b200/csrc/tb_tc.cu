@@ -14,8 +14,9 @@
 // along K, B' rows (2n, 2n+1) = ([Br, -Bi], [Bi, Br]), so that columns (2n,
 // 2n+1) of the product hold the real and imaginary parts of C(m, n).
 //
-// The operand preparation reads the tensors in their own layouts through the
-// permutation engine (the input permutations are fused into the conversion),
+// The operand preparation reads the tensors in their own layouts through
+// per-row and per-index offset tables (the input permutations are fused into
+// the conversion to slices or BF16 parts),
 // and the epilogue writes D through per-row and per-column offset tables (the
 // output permutation) with alpha and beta applied.
 #include <cudaTypedefs.h>
@@ -106,38 +107,9 @@ int build_offsets(const std::vector<MGroup>& groups, bool use_s2, int64_t* out, 
   return 0;
 }
 
-// ---- operand preparation functors (applied by the permutation engine) ----------
-// Output offsets o address a virtual [row][kpad] matrix (complex: complex units).
+// ---- operand conversion helpers --------------------------------------------------
 __device__ __forceinline__ unsigned exp_field(double x) {
   return (unsigned)((__double_as_longlong(x) >> 52) & 0x7FF);
-}
-__device__ __forceinline__ void row_max_exp(unsigned* rowE, uint64_t m, unsigned E) {
-  if (E > *(volatile unsigned*)&rowE[m]) atomicMax(&rowE[m], E);
-}
-
-struct RowExpR8 {
-  unsigned* rowE; FastDiv kdiv;
-  __device__ __forceinline__ void operator()(int64_t o, const double& v) const {
-    row_max_exp(rowE, kdiv.div((uint64_t)o), exp_field(v));
-  }
-};
-struct RowExpC8 {
-  unsigned* rowE; FastDiv kdiv;
-  __device__ __forceinline__ void operator()(int64_t o, const double2& v) const {
-    row_max_exp(rowE, kdiv.div((uint64_t)o), max(exp_field(v.x), exp_field(v.y)));
-  }
-};
-
-// s signed 7-bit digits of x in (-1, 1): x = sum_i d_i 2^(-7 i) + remainder.
-template <int S>
-__device__ __forceinline__ void digits(double x, int8_t (&d)[S]) {
-#pragma unroll
-  for (int i = 0; i < S; ++i) {
-    x *= 128.0;
-    const double t = trunc(x);
-    d[i] = (int8_t)(int)t;
-    x -= t;
-  }
 }
 
 __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
@@ -145,45 +117,197 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
-struct SplitR4 {
-  __nv_bfloat16* planes; int64_t pstride;
-  __device__ __forceinline__ void operator()(int64_t o, const float& v) const {
-    __nv_bfloat16 h, l;
-    split_bf16(v, h, l);
-    planes[o] = h;
-    planes[pstride + o] = l;
-  }
+// ---- operand gather: 64 x 64 tiles through source offset tables ----------------
+// Element (m, k) of a matricized operand lives at src[lm[m] + lk[k]].  A tile
+// is read with lanes along whichever index is contiguous in the source, staged
+// in shared memory, and converted with lanes along k so that every thread
+// writes 4 consecutive K positions of each output plane in one store.
+// Tiles cover [0, rows_pad) x [0, kpad_src): padding is written as zeros.
+constexpr int kGThreads = 256;
+constexpr int kMaxSlicesDev = 8;
+template <typename E> constexpr int gather_rows() { return sizeof(E) == 16 ? 32 : 64; }  // 32-34 KB tiles
+constexpr int kGK = 64;
+
+enum GatherMode { G_EXP_R8, G_EXP_C8, G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A, G_SPLIT_C4B };
+
+struct GatherParams {
+  const void* src;
+  const int64_t* lm;   // source offset of row m (m < rows)
+  const int64_t* lk;   // source offset of contracted index k (k < K)
+  int64_t rows, K;     // valid extents
+  int64_t kpad;        // real row length of the output planes (elements)
+  int64_t pstride;     // elements per plane
+  void* planes;
+  unsigned* rowE;      // exponent fields (exp modes write, slice modes read)
+  int slices;
+  int lanes_on_k;      // 1: consecutive k are contiguous in the source
+  double isign;        // -1 conjugates the imaginary part
 };
-struct SplitC4A {
-  __nv_bfloat16* planes; int64_t pstride; float isign;
-  __device__ __forceinline__ void operator()(int64_t o, const float2& v) const {
-    __nv_bfloat16 hr, lr, hi, li;
-    split_bf16(v.x, hr, lr);
-    split_bf16(isign * v.y, hi, li);
-    __nv_bfloat162 a; a.x = hr; a.y = hi;
-    __nv_bfloat162 b; b.x = lr; b.y = li;
-    *reinterpret_cast<__nv_bfloat162*>(planes + 2 * o) = a;
-    *reinterpret_cast<__nv_bfloat162*>(planes + pstride + 2 * o) = b;
+
+// Signed base-128 digits of x in (-1, 1), most significant first: the digits
+// of trunc(x * 2^56) in sign-magnitude form (identical to repeatedly taking
+// trunc(128 x) and keeping the remainder, which is exact in FP64).
+__device__ __forceinline__ void digits8(double x, int8_t (&d)[kMaxSlicesDev]) {
+  const long long X = __double2ll_rz(x * 72057594037927936.0);  // 2^56
+  const unsigned long long U = (unsigned long long)(X < 0 ? -X : X);
+  const bool neg = X < 0;
+#pragma unroll
+  for (int i = 0; i < kMaxSlicesDev; ++i) {
+    const int v = (int)((U >> (49 - 7 * i)) & 127ull);
+    d[i] = (int8_t)(neg ? -v : v);
   }
-};
-struct SplitC4B {
-  __nv_bfloat16* planes; int64_t pstride; int64_t kcpad; FastDiv kdiv; float isign;
-  __device__ __forceinline__ void operator()(int64_t o, const float2& v) const {
-    const uint64_t n = kdiv.div((uint64_t)o);
-    const int64_t k = o - (int64_t)n * kcpad;
-    const int64_t r0 = (int64_t)(2 * n) * (2 * kcpad) + 2 * k, r1 = r0 + 2 * kcpad;
-    const float br = v.x, bi = isign * v.y;
-    __nv_bfloat16 hr, lr, hi, li, nhi, nli;
-    split_bf16(br, hr, lr);
-    split_bf16(bi, hi, li);
-    split_bf16(-bi, nhi, nli);
-    __nv_bfloat162 w;
-    w.x = hr; w.y = nhi; *reinterpret_cast<__nv_bfloat162*>(planes + r0) = w;
-    w.x = hi; w.y = hr;  *reinterpret_cast<__nv_bfloat162*>(planes + r1) = w;
-    w.x = lr; w.y = nli; *reinterpret_cast<__nv_bfloat162*>(planes + pstride + r0) = w;
-    w.x = li; w.y = lr;  *reinterpret_cast<__nv_bfloat162*>(planes + pstride + r1) = w;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant__ GatherParams P) {
+  constexpr bool CPLX = MODE == G_EXP_C8 || MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A ||
+                        MODE == G_SPLIT_C4B;
+  constexpr bool F32 = MODE == G_SPLIT_R4 || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
+  constexpr bool EXP = MODE == G_EXP_R8 || MODE == G_EXP_C8;
+  using R = typename std::conditional<F32, float, double>::type;
+  using E = typename std::conditional<CPLX, typename std::conditional<F32, float2, double2>::type, R>::type;
+  constexpr int TM = gather_rows<E>(), TK = kGK;
+  __shared__ E tile[TM][TK + 1];
+  __shared__ int64_t sm_lm[TM], sm_lk[TK];
+  __shared__ unsigned sm_max[TM];
+  __shared__ double sm_sc[TM];
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  const int tid = threadIdx.x;
+  if (tid < TM) {
+    sm_lm[tid] = (m0 + tid < P.rows) ? P.lm[m0 + tid] : -1;
+    sm_max[tid] = 0;
+    if constexpr (!EXP && !F32) sm_sc[tid] = pow2d(1022 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1022u));
   }
-};
+  const E* src = (const E*)P.src;
+  const int64_t nkt = (P.K + TK - 1) / TK;                   // tiles with data
+  const int64_t ntiles = EXP ? nkt : (P.kpad / (CPLX ? 2 : 1)) / TK;  // conversion also writes the padding
+  for (int64_t kt = blockIdx.y; kt < ntiles; kt += gridDim.y) {
+    const int64_t k0 = kt * TK;
+    __syncthreads();  // previous tile consumed
+    if (tid < TK) sm_lk[tid] = (k0 + tid < P.K) ? P.lk[k0 + tid] : -1;
+    __syncthreads();
+#pragma unroll 4
+    for (int idx = tid; idx < TM * TK; idx += kGThreads) {
+      const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+      E v;
+      if constexpr (CPLX) { v.x = 0; v.y = 0; } else { v = 0; }
+      if (sm_lm[mm] >= 0 && sm_lk[kk] >= 0) v = src[sm_lm[mm] + sm_lk[kk]];
+      tile[mm][kk] = v;
+    }
+    __syncthreads();
+    if constexpr (EXP) {
+      // row maxima of the exponent field: TPR threads per row
+      constexpr int TPR = kGThreads / TM;
+      const int mm = tid / TPR, part = tid % TPR;
+      unsigned e = 0;
+      for (int kk = part; kk < TK; kk += TPR) {
+        const E v = tile[mm][kk];
+        if constexpr (CPLX) e = max(e, max(exp_field(v.x), exp_field(v.y)));
+        else e = max(e, exp_field(v));
+      }
+#pragma unroll
+      for (int w = 1; w < TPR; w <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, w));
+      if (part == 0 && e > sm_max[mm]) sm_max[mm] = e;  // one writer per row
+    } else {
+      // convert: thread -> (row mm, 4 consecutive k)
+      for (int idx = tid; idx < TM * (TK / 4); idx += kGThreads) {
+        const int mm = idx / (TK / 4), kq = (idx % (TK / 4)) * 4;
+        const int64_t m = m0 + mm, k = k0 + kq;
+        if constexpr (MODE == G_SLICE_R8) {
+          const double sc = sm_sc[mm];
+          int8_t d[4][kMaxSlicesDev];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) digits8(tile[mm][kq + t] * sc, d[t]);
+          int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
+#pragma unroll
+          for (int i = 0; i < kMaxSlicesDev; ++i)
+            if (i < P.slices) {
+              char4 w; w.x = d[0][i]; w.y = d[1][i]; w.z = d[2][i]; w.w = d[3][i];
+              *reinterpret_cast<char4*>(base + i * P.pstride) = w;
+            }
+        } else if constexpr (MODE == G_SLICE_C8A || MODE == G_SLICE_C8B) {
+          const double sc = sm_sc[mm];
+          int8_t dr[4][kMaxSlicesDev], di[4][kMaxSlicesDev];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const E v = tile[mm][kq + t];
+            digits8(v.x * sc, dr[t]);
+            digits8(P.isign * v.y * sc, di[t]);
+          }
+          if constexpr (MODE == G_SLICE_C8A) {
+            int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
+#pragma unroll
+            for (int i = 0; i < kMaxSlicesDev; ++i)
+              if (i < P.slices) {
+                char4 w0; w0.x = dr[0][i]; w0.y = di[0][i]; w0.z = dr[1][i]; w0.w = di[1][i];
+                char4 w1; w1.x = dr[2][i]; w1.y = di[2][i]; w1.z = dr[3][i]; w1.w = di[3][i];
+                *reinterpret_cast<char4*>(base + i * P.pstride) = w0;
+                *reinterpret_cast<char4*>(base + i * P.pstride + 4) = w1;
+              }
+          } else {
+            int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
+            int8_t* b1 = b0 + P.kpad;
+#pragma unroll
+            for (int i = 0; i < kMaxSlicesDev; ++i)
+              if (i < P.slices) {
+                char4 a0, a1, c0, c1;
+                a0.x = dr[0][i]; a0.y = (int8_t)-di[0][i]; a0.z = dr[1][i]; a0.w = (int8_t)-di[1][i];
+                a1.x = dr[2][i]; a1.y = (int8_t)-di[2][i]; a1.z = dr[3][i]; a1.w = (int8_t)-di[3][i];
+                c0.x = di[0][i]; c0.y = dr[0][i]; c0.z = di[1][i]; c0.w = dr[1][i];
+                c1.x = di[2][i]; c1.y = dr[2][i]; c1.z = di[3][i]; c1.w = dr[3][i];
+                *reinterpret_cast<char4*>(b0 + i * P.pstride) = a0;
+                *reinterpret_cast<char4*>(b0 + i * P.pstride + 4) = a1;
+                *reinterpret_cast<char4*>(b1 + i * P.pstride) = c0;
+                *reinterpret_cast<char4*>(b1 + i * P.pstride + 4) = c1;
+              }
+          }
+        } else if constexpr (MODE == G_SPLIT_R4) {
+          __nv_bfloat16 h[4], l[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) split_bf16(tile[mm][kq + t], h[t], l[t]);
+          __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + k;
+          __nv_bfloat162 hh[2] = {{h[0], h[1]}, {h[2], h[3]}}, ll[2] = {{l[0], l[1]}, {l[2], l[3]}};
+          *reinterpret_cast<uint2*>(base) = *reinterpret_cast<uint2*>(hh);
+          *reinterpret_cast<uint2*>(base + P.pstride) = *reinterpret_cast<uint2*>(ll);
+        } else {
+          // complex FP32: A' rows (re, im); B' rows 2n (re, -im), 2n+1 (im, re)
+          __nv_bfloat16 hr[4], lr[4], hi[4], li[4], nhi[4], nli[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const E v = tile[mm][kq + t];
+            const float im = (float)P.isign * v.y;
+            split_bf16(v.x, hr[t], lr[t]);
+            split_bf16(im, hi[t], li[t]);
+            split_bf16(-im, nhi[t], nli[t]);
+          }
+          if constexpr (MODE == G_SPLIT_C4A) {
+            __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + 2 * k;
+            __nv_bfloat162 H[4] = {{hr[0], hi[0]}, {hr[1], hi[1]}, {hr[2], hi[2]}, {hr[3], hi[3]}};
+            __nv_bfloat162 L[4] = {{lr[0], li[0]}, {lr[1], li[1]}, {lr[2], li[2]}, {lr[3], li[3]}};
+            *reinterpret_cast<uint4*>(base) = *reinterpret_cast<uint4*>(H);
+            *reinterpret_cast<uint4*>(base + P.pstride) = *reinterpret_cast<uint4*>(L);
+          } else {
+            __nv_bfloat16* b0 = (__nv_bfloat16*)P.planes + (2 * m) * P.kpad + 2 * k;
+            __nv_bfloat16* b1 = b0 + P.kpad;
+            __nv_bfloat162 H0[4] = {{hr[0], nhi[0]}, {hr[1], nhi[1]}, {hr[2], nhi[2]}, {hr[3], nhi[3]}};
+            __nv_bfloat162 L0[4] = {{lr[0], nli[0]}, {lr[1], nli[1]}, {lr[2], nli[2]}, {lr[3], nli[3]}};
+            __nv_bfloat162 H1[4] = {{hi[0], hr[0]}, {hi[1], hr[1]}, {hi[2], hr[2]}, {hi[3], hr[3]}};
+            __nv_bfloat162 L1[4] = {{li[0], lr[0]}, {li[1], lr[1]}, {li[2], lr[2]}, {li[3], lr[3]}};
+            *reinterpret_cast<uint4*>(b0) = *reinterpret_cast<uint4*>(H0);
+            *reinterpret_cast<uint4*>(b0 + P.pstride) = *reinterpret_cast<uint4*>(L0);
+            *reinterpret_cast<uint4*>(b1) = *reinterpret_cast<uint4*>(H1);
+            *reinterpret_cast<uint4*>(b1 + P.pstride) = *reinterpret_cast<uint4*>(L1);
+          }
+        }
+      }
+    }
+  }
+  if constexpr (EXP) {
+    __syncthreads();
+    if (tid < TM && sm_max[tid] && m0 + tid < P.rows) atomicMax(&P.rowE[m0 + tid], sm_max[tid]);
+  }
+}
 
 // exponents: rowexp[r] = rowE[r / rep] - 1022 (rep = 2 for complex B' rows)
 __global__ void exps_kernel(const unsigned* __restrict__ rowE, int* __restrict__ out, int64_t n, int rep) {
@@ -198,87 +322,25 @@ constexpr int kMaxSlices = 8;
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 // One operand of the GEMM: a source tensor, its row groups and its contracted
-// dims (positions and extents in Z.k order).
+// dims (Z.k order), each with strides in this tensor (s1) and in D (s2).
 struct Operand {
   const void* ptr;
-  int rank;
-  const int* dims;
   std::vector<MGroup> rows;   // uncontracted groups: s1 = stride in this tensor, s2 = stride in D
-  std::vector<int> kpos;      // position of each contracted dim (Z.k order) in this tensor
+  std::vector<MGroup> ks;     // contracted groups: s1 = stride in this tensor
   bool conj;
 };
 
-// Permutation-engine strides that map the tensor onto a virtual [row][rowlen]
-// matrix (K fastest, contracted dims in Z.k order, rows in group order).
-void gather_plan_dims(const Operand& op, const Matricization& Z, int64_t rowlen, int64_t* D, int64_t* SI,
-                      int64_t* SO) {
-  int64_t s = 1;
-  for (int i = 0; i < op.rank; ++i) { D[i] = op.dims[i]; SI[i] = s; s *= op.dims[i]; }
-  int64_t ks = 1;
-  for (size_t q = 0; q < Z.k.size(); ++q) { SO[op.kpos[q]] = ks; ks *= Z.k[q].ext; }
-  int64_t rs = rowlen;
-  for (auto& g : op.rows) { SO[g.src] = rs; rs *= g.ext; }
+template <int MODE>
+int run_gather(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStream_t s) {
+  if (grid_rows <= 0 || grid_k <= 0) return 0;
+  if (grid_rows > INT32_MAX) { set_error("gather grid too large"); return TB_ERR_LIMIT; }
+  // enough CTAs to fill the GPU several times over; each walks a strided set of K tiles
+  int64_t gy = std::max<int64_t>(1, std::min<int64_t>(grid_k, (int64_t)num_sms() * 16 / std::max<int64_t>(1, grid_rows)));
+  gy = std::min<int64_t>(gy, 65535);
+  gather_kernel<MODE><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+  TB_CHECK_LAUNCH();
+  return 0;
 }
-
-template <typename E, typename F>
-int gather(const Operand& op, const Matricization& Z, int64_t rowlen, const F& f, cudaStream_t s) {
-  int64_t D[kMaxRank], SI[kMaxRank], SO[kMaxRank];
-  gather_plan_dims(op, Z, rowlen, D, SI, SO);
-  PermParams P;
-  if (int e = build_perm_plan((int)sizeof(E), op.rank, D, SI, SO, &P)) {
-    set_error("operand gather plan declined (%d)", e);
-    return e == TB_ERR_NOT_IMPLEMENTED ? TB_ERR_NOT_IMPLEMENTED : e;
-  }
-  return launch_perm<E, F>(P, (const E*)op.ptr, f, s);
-}
-
-// Real and complex slice functors with a runtime slice count (<= kMaxSlices).
-struct SliceR8R {
-  int8_t* planes; int64_t pstride; const unsigned* rowE; FastDiv kdiv; int s;
-  __device__ __forceinline__ void operator()(int64_t o, const double& v) const {
-    const uint64_t m = kdiv.div((uint64_t)o);
-    int8_t d[kMaxSlices];
-    digits<kMaxSlices>(v * pow2d(1022 - (int)rowE[m]), d);
-#pragma unroll
-    for (int i = 0; i < kMaxSlices; ++i) if (i < s) planes[i * pstride + o] = d[i];
-  }
-};
-struct SliceC8AR {
-  int8_t* planes; int64_t pstride; const unsigned* rowE; FastDiv kdiv; double isign; int s;
-  __device__ __forceinline__ void operator()(int64_t o, const double2& v) const {
-    const uint64_t m = kdiv.div((uint64_t)o);
-    const double sc = pow2d(1022 - (int)rowE[m]);
-    int8_t dr[kMaxSlices], di[kMaxSlices];
-    digits<kMaxSlices>(v.x * sc, dr);
-    digits<kMaxSlices>(isign * v.y * sc, di);
-#pragma unroll
-    for (int i = 0; i < kMaxSlices; ++i)
-      if (i < s) {
-        char2 w; w.x = dr[i]; w.y = di[i];
-        *reinterpret_cast<char2*>(planes + i * pstride + 2 * o) = w;
-      }
-  }
-};
-struct SliceC8BR {
-  int8_t* planes; int64_t pstride; int64_t kcpad; const unsigned* rowE; FastDiv kdiv; double isign; int s;
-  __device__ __forceinline__ void operator()(int64_t o, const double2& v) const {
-    const uint64_t n = kdiv.div((uint64_t)o);
-    const int64_t k = o - (int64_t)n * kcpad;
-    const double sc = pow2d(1022 - (int)rowE[n]);
-    int8_t dr[kMaxSlices], di[kMaxSlices];
-    digits<kMaxSlices>(v.x * sc, dr);
-    digits<kMaxSlices>(isign * v.y * sc, di);
-    const int64_t r0 = (int64_t)(2 * n) * (2 * kcpad) + 2 * k, r1 = r0 + 2 * kcpad;
-#pragma unroll
-    for (int i = 0; i < kMaxSlices; ++i)
-      if (i < s) {
-        char2 a; a.x = dr[i]; a.y = (int8_t)(-di[i]);
-        char2 b; b.x = di[i]; b.y = dr[i];
-        *reinterpret_cast<char2*>(planes + i * pstride + r0) = a;
-        *reinterpret_cast<char2*>(planes + i * pstride + r1) = b;
-      }
-  }
-};
 
 template <int BN, bool I8, int EPI>
 int launch_tc(const TcGemmParams& P, cudaStream_t s) {
@@ -330,8 +392,12 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   std::stable_sort(Z.n.begin(), Z.n.end(), by_d);
   // the operand holding D's fastest dimension plays the row (M) role
   const bool swap = !Z.n.empty() && (Z.m.empty() || Z.n[0].s2 < Z.m[0].s2);
-  Operand Lop{l, Z.lrank, ldims, Z.m, {}, lconj != 0}, Rop{r, Z.rrank, rdims, Z.n, {}, rconj != 0};
-  for (auto& g : Z.k) { Lop.kpos.push_back(g.dpos); Rop.kpos.push_back(g.src); }
+  Operand Lop{l, Z.m, {}, lconj != 0}, Rop{r, Z.n, {}, rconj != 0};
+  for (auto g : Z.k) {
+    Lop.ks.push_back(g);                       // s1 = L stride
+    MGroup h = g; h.s1 = g.s2; Rop.ks.push_back(h);  // R stride
+  }
+  (void)ldims; (void)rdims;
   const Operand& A = swap ? Rop : Lop;
   const Operand& B = swap ? Lop : Rop;
   const bool cplx = is_complex(dtk), i8 = is_double(dtk);
@@ -379,8 +445,9 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   const size_t bytesA = (size_t)npa * Mpad * Kpad * oes, bytesB = (size_t)npb * Npad * Kpad * oes;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t offA = 0, offB = al(bytesA), offDm = offB + al(bytesB), offDn = offDm + al(M * 8),
-               offRE = offDn + al(Nc * 8), offCE = offRE + al(M * 4), offRX = offCE + al(Nc * 4),
-               offCX = offRX + al(M * 4), total = offCX + al(Nr * 4);
+               offLA = offDn + al(Nc * 8), offLB = offLA + al(M * 8), offKA = offLB + al(Nc * 8),
+               offKB = offKA + al(K * 8), offRE = offKB + al(K * 8), offCE = offRE + al(M * 4),
+               offRX = offCE + al(Nc * 4), offCX = offRX + al(M * 4), total = offCX + al(Nr * 4);
   unsigned char* ws = nullptr;
   if (int e = scratch_alloc((void**)&ws, total, s)) return e;
   int err = 0;
@@ -388,51 +455,60 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   int8_t* Bp = (int8_t*)(ws + offB);
   int64_t* dm = (int64_t*)(ws + offDm);
   int64_t* dn = (int64_t*)(ws + offDn);
+  int64_t* lmA = (int64_t*)(ws + offLA);
+  int64_t* lmB = (int64_t*)(ws + offLB);
+  int64_t* lkA = (int64_t*)(ws + offKA);
+  int64_t* lkB = (int64_t*)(ws + offKB);
   unsigned* rowE = (unsigned*)(ws + offRE);
   unsigned* colE = (unsigned*)(ws + offCE);
   int* rowx = (int*)(ws + offRX);
   int* colx = (int*)(ws + offCX);
-  const bool padded = Mpad != M || Npad != Nr || Kpad != Kr;
-  const int64_t rowlen = cplx ? Kpad / 2 : Kpad;  // gather row length in source elements
+  const int64_t ksrc_pad = cplx ? Kpad / 2 : Kpad;  // padded K in source elements
   do {
-    if (padded && (cudaMemsetAsync(ws, 0, offDm, s) != cudaSuccess)) { err = TB_ERR_CUDA; break; }
     if ((err = build_offsets(A.rows, true, dm, s))) break;
     if ((err = build_offsets(B.rows, true, dn, s))) break;
+    if ((err = build_offsets(A.rows, false, lmA, s))) break;
+    if ((err = build_offsets(B.rows, false, lmB, s))) break;
+    if ((err = build_offsets(A.ks, false, lkA, s))) break;
+    if ((err = build_offsets(B.ks, false, lkB, s))) break;
+    GatherParams GA{}, GB{};
+    GA.src = A.ptr; GA.lm = lmA; GA.lk = lkA; GA.rows = M; GA.K = K; GA.kpad = Kpad; GA.pstride = Mpad * Kpad;
+    GA.planes = Ap; GA.rowE = rowE; GA.slices = S; GA.isign = A.conj ? -1.0 : 1.0;
+    GA.lanes_on_k = (A.ks[0].s1 == 1 || A.rows.empty() || A.rows[0].s1 != 1) ? 1 : 0;
+    GB.src = B.ptr; GB.lm = lmB; GB.lk = lkB; GB.rows = Nc; GB.K = K; GB.kpad = Kpad; GB.pstride = Npad * Kpad;
+    GB.planes = Bp; GB.rowE = colE; GB.slices = S; GB.isign = B.conj ? -1.0 : 1.0;
+    GB.lanes_on_k = (B.ks[0].s1 == 1 || B.rows.empty() || B.rows[0].s1 != 1) ? 1 : 0;
+    const int tmr = i8 && cplx ? 32 : 64;               // gather tile rows (16-byte elements: 32)
+    const int64_t gA = Mpad / tmr, gB = (cplx ? Npad / 2 : Npad) / tmr, gk = ksrc_pad / kGK;
     if (i8) {
       if (cudaMemsetAsync(rowE, 0, offRX - offRE, s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
-      const FastDiv kd((uint64_t)rowlen);
+      const int64_t eA = (M + tmr - 1) / tmr, eB = (Nc + tmr - 1) / tmr, ek = (K + kGK - 1) / kGK;
       if (!cplx) {
-        if ((err = gather<double>(A, Z, rowlen, RowExpR8{rowE, kd}, s))) break;
-        if ((err = gather<double>(B, Z, rowlen, RowExpR8{colE, kd}, s))) break;
+        if ((err = run_gather<G_EXP_R8>(GA, eA, ek, s))) break;
+        if ((err = run_gather<G_EXP_R8>(GB, eB, ek, s))) break;
       } else {
-        if ((err = gather<double2>(A, Z, rowlen, RowExpC8{rowE, kd}, s))) break;
-        if ((err = gather<double2>(B, Z, rowlen, RowExpC8{colE, kd}, s))) break;
+        if ((err = run_gather<G_EXP_C8>(GA, eA, ek, s))) break;
+        if ((err = run_gather<G_EXP_C8>(GB, eB, ek, s))) break;
       }
       exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 4096)), 256, 0, s>>>(rowE, rowx, M, 1);
       exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((Nr + 255) / 256, 4096)), 256, 0, s>>>(colE, colx, Nr,
                                                                                                   cplx ? 2 : 1);
       count_launch();
       count_launch();
-      const int64_t psA = Mpad * Kpad, psB = Npad * Kpad;
       if (!cplx) {
-        if ((err = gather<double>(A, Z, rowlen, SliceR8R{Ap, psA, rowE, kd, S}, s))) break;
-        if ((err = gather<double>(B, Z, rowlen, SliceR8R{Bp, psB, colE, kd, S}, s))) break;
+        if ((err = run_gather<G_SLICE_R8>(GA, gA, gk, s))) break;
+        if ((err = run_gather<G_SLICE_R8>(GB, gB, gk, s))) break;
       } else {
-        if ((err = gather<double2>(A, Z, rowlen, SliceC8AR{Ap, psA, rowE, kd, A.conj ? -1.0 : 1.0, S}, s))) break;
-        if ((err = gather<double2>(B, Z, rowlen, SliceC8BR{Bp, psB, rowlen, colE, kd, B.conj ? -1.0 : 1.0, S}, s)))
-          break;
+        if ((err = run_gather<G_SLICE_C8A>(GA, gA, gk, s))) break;
+        if ((err = run_gather<G_SLICE_C8B>(GB, gB, gk, s))) break;
       }
     } else {
-      __nv_bfloat16* Ah = (__nv_bfloat16*)Ap;
-      __nv_bfloat16* Bh = (__nv_bfloat16*)Bp;
-      const int64_t psA = Mpad * Kpad, psB = Npad * Kpad;
       if (!cplx) {
-        if ((err = gather<float>(A, Z, rowlen, SplitR4{Ah, psA}, s))) break;
-        if ((err = gather<float>(B, Z, rowlen, SplitR4{Bh, psB}, s))) break;
+        if ((err = run_gather<G_SPLIT_R4>(GA, gA, gk, s))) break;
+        if ((err = run_gather<G_SPLIT_R4>(GB, gB, gk, s))) break;
       } else {
-        const FastDiv kd((uint64_t)rowlen);
-        if ((err = gather<float2>(A, Z, rowlen, SplitC4A{Ah, psA, A.conj ? -1.f : 1.f}, s))) break;
-        if ((err = gather<float2>(B, Z, rowlen, SplitC4B{Bh, psB, rowlen, kd, B.conj ? -1.f : 1.f}, s))) break;
+        if ((err = run_gather<G_SPLIT_C4A>(GA, gA, gk, s))) break;
+        if ((err = run_gather<G_SPLIT_C4B>(GB, gB, gk, s))) break;
       }
     }
     // GEMM parameters
