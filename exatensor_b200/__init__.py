@@ -72,6 +72,8 @@ def lib() -> C.CDLL:
                                      C.c_double, C.c_int, C.c_int, C.POINTER(Plan), vp]
     L.tb_tensor_contract_str.argtypes = [C.c_char_p, C.c_int, C.c_int, ip, vp, C.c_int, ip, vp, C.c_int, ip, vp,
                                          C.c_double, C.c_double, C.c_int, C.POINTER(Plan), vp]
+    L.tb_tensor_contract_noalloc.argtypes = [ip, C.c_int, C.c_int, ip, vp, C.c_int, ip, vp, C.c_int, ip, vp,
+                                             C.c_double, C.c_double, C.c_int, C.c_int, vp]
     L.tb_fill_uniform.argtypes = [C.c_int, C.c_size_t, vp, C.c_uint64, C.c_double, C.c_double, vp]
     L.tb_last_contract_stats.argtypes = [C.POINTER(ContractStats)]
     _lib = L
@@ -166,6 +168,28 @@ def tensor_contract(pattern_or_cptrn, dtk, ddims, d_ptr, ldims, l_ptr, rdims, r_
                                         len(ldims), iarr(ldims), C.c_void_p(l_ptr), len(rdims), iarr(rdims),
                                         C.c_void_p(r_ptr), a.real, a.imag, conj_bits, int(accumulative), pp,
                                         _stream(stream)))
+
+
+NOALLOC_ARENA_BYTES = 64 << 20  # TB_NOALLOC_ARENA_BYTES
+
+
+def tensor_contract_noalloc(pattern_or_cptrn, dtk, ddims, d_ptr, ldims, l_ptr, rdims, r_ptr, alpha=1.0,
+                            conj_bits=0, accumulative=True, stream=None):
+    """Plain (TTGT) contraction that allocates no device memory: its scratch is
+    a fixed static array of NOALLOC_ARENA_BYTES per device, so larger requests
+    raise TBError (TB_ERR_LIMIT).  Same arguments as tensor_contract without a
+    plan; calls that overlap on the GPU share the array and race."""
+    a = complex(alpha)
+    if isinstance(pattern_or_cptrn, str):
+        cptrn, dr, lr, rr, conj_bits = parse_pattern(pattern_or_cptrn)
+        if (dr, lr, rr) != (len(ddims), len(ldims), len(rdims)):
+            raise TBError(1, "pattern ranks do not match the tensors")
+    else:
+        cptrn = pattern_or_cptrn
+    _check(lib().tb_tensor_contract_noalloc(iarr(cptrn), dtk, len(ddims), iarr(ddims), C.c_void_p(d_ptr),
+                                            len(ldims), iarr(ldims), C.c_void_p(l_ptr), len(rdims), iarr(rdims),
+                                            C.c_void_p(r_ptr), a.real, a.imag, conj_bits, int(accumulative),
+                                            _stream(stream)))
 
 
 def launch_count() -> int:

@@ -63,6 +63,7 @@ __device__ __forceinline__ void record_device_error(unsigned int* flag, unsigned
   if (flag) atomicCAS(flag, 0u, code);
 }
 unsigned int* device_error_word();  // per-device word, zero when healthy
+unsigned int* device_error_word_if_created();  // the same word, or null; never allocates
 
 }  // namespace tb
 

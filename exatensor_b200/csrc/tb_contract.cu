@@ -18,6 +18,8 @@
 #include "tb_permute.cuh"
 
 #include <cmath>
+#include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace tb {
@@ -350,4 +352,200 @@ extern "C" int tb_last_contract_stats(tb_contract_stats_t* stats) {
   if (!stats) return TB_ERR_INVALID_ARGS;
   *stats = tb::g_stats;
   return 0;
+}
+
+// ---- no-allocation variant of the plain (TTGT) contraction ---------------------
+// Same kernels as the TTGT path above, but every temporary buffer is carved
+// from one static device array instead of the stream-ordered pool, so a call
+// makes no allocation.  Nothing in the array has to start at zero: every byte
+// a kernel reads there is written earlier in the same call (the GEMM does not
+// read its output when beta is 0), so no clear is queued.  The array keeps the
+// previous call's data; calls on one stream are ordered by the stream, calls
+// that overlap on the GPU race.
+static __device__ __align__(256) unsigned char tb_noalloc_arena[TB_NOALLOC_ARENA_BYTES];
+
+namespace tb {
+namespace {
+
+unsigned char* g_arena_addr[64] = {nullptr};
+std::mutex g_arena_mu;
+
+// Device address of the array on the current device, looked up once per
+// device (with that device current); the host-side name is not a device
+// address and is never passed to a kernel.
+int noalloc_arena(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    set_error("tb_tensor_contract_noalloc: no usable current device (%s)", cudaGetErrorString(e));
+    return TB_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lk(g_arena_mu);
+  if (!g_arena_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, tb_noalloc_arena);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      set_error("tb_tensor_contract_noalloc: cannot look up the scratch array on device %d (%s)", dev,
+                cudaGetErrorString(e));
+      return TB_ERR_CUDA;
+    }
+    g_arena_addr[dev] = (unsigned char*)p;
+  }
+  *out = g_arena_addr[dev];
+  return 0;
+}
+
+uint64_t round256(unsigned __int128 b) { return (uint64_t)((b + 255) / 256 * 256); }
+
+template <typename E, bool CPLX>
+int dot_noalloc(const Matricization& Z, void* d, const void* l, const void* r, double ar, double ai, double br,
+                int lconj, int rconj, unsigned char* arena, cudaStream_t s) {
+  DotParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.nk = (int)Z.k.size();
+  P.K = Z.K;
+  for (int i = 0; i < P.nk; ++i) {
+    P.ext[i] = Z.k[i].ext; P.div[i].init((uint64_t)Z.k[i].ext);
+    P.ls[i] = Z.k[i].s1; P.rs[i] = Z.k[i].s2;
+  }
+  double2* partial = (double2*)arena;  // every block writes its own entry
+  dot_pass1<E, CPLX><<<kDotBlocks, kDotThreads, 0, s>>>(P, (const E*)l, (const E*)r, lconj, rconj, partial);
+  dot_pass2<E, CPLX><<<1, kDotThreads, 0, s>>>(partial, kDotBlocks, (E*)d, ar, ai, br, 0.0);
+  count_launch();
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_error("dot kernels: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
+  return 0;
+}
+
+template <typename E>
+int ttgt_noalloc(const Matricization& Z, int dtk, const int* ldims, const void* l, const int* rdims, const void* r,
+                 void* d, double ar, double ai, bool accumulate, int lconj, int rconj, unsigned char* arena,
+                 cudaStream_t s) {
+  const size_t es = sizeof(E);
+  int64_t dd[kMaxRank], si[kMaxRank], so[kMaxRank];
+  E* Lt = (E*)arena;
+  E* Rt = (E*)(arena + round256((unsigned __int128)Z.M * Z.K * es));
+  E* Ct = (E*)((unsigned char*)Rt + round256((unsigned __int128)Z.N * Z.K * es));
+  const void* A = l;
+  const void* B = r;
+  int err = 0;
+  matrix_strides(Z, true, Z.lrank, ldims, dd, si, so);
+  if (!is_identity(Z.lrank, si, so)) {
+    if ((err = permute_general<E>(Z.lrank, dd, si, so, (const E*)l, StoreCopy<E>{Lt}, s))) return err;
+    A = Lt;
+  }
+  matrix_strides(Z, false, Z.rrank, rdims, dd, si, so);
+  if (!is_identity(Z.rrank, si, so)) {
+    if ((err = permute_general<E>(Z.rrank, dd, si, so, (const E*)r, StoreCopy<E>{Rt}, s))) return err;
+    B = Rt;
+  }
+  const int nm = (int)Z.m.size(), nn = (int)Z.n.size();
+  int64_t cs = 1;
+  for (int i = 0; i < nm; ++i) { dd[i] = Z.m[i].ext; si[i] = cs; so[i] = Z.m[i].s2; cs *= Z.m[i].ext; }
+  for (int i = 0; i < nn; ++i) { dd[nm + i] = Z.n[i].ext; si[nm + i] = cs; so[nm + i] = Z.n[i].s2; cs *= Z.n[i].ext; }
+  const bool cplx = is_complex(dtk);
+  const double realpha = cplx ? ar : real_alpha(ar, ai);
+  if (is_identity(nm + nn, si, so)) {  // D is already the product matrix
+    return gemm_plain_tn(dtk, Z.M, Z.N, Z.K, A, Z.K, B, Z.K, d, Z.M, realpha, cplx ? ai : 0.0,
+                         accumulate ? 1.0 : 0.0, 0.0, lconj, rconj, s);
+  }
+  if ((err = gemm_plain_tn(dtk, Z.M, Z.N, Z.K, A, Z.K, B, Z.K, Ct, Z.M, 1.0, 0.0, 0.0, 0.0, lconj, rconj, s)))
+    return err;
+  const int rk = nm + nn;
+  switch (dtk) {
+    case kR4: {
+      const float a = (float)realpha;
+      return accumulate ? permute_general<float>(rk, dd, si, so, (const float*)Ct, StoreAxpy<float>{(float*)d, a}, s)
+                        : permute_general<float>(rk, dd, si, so, (const float*)Ct, StoreScaled<float>{(float*)d, a}, s);
+    }
+    case kR8:
+      return accumulate
+                 ? permute_general<double>(rk, dd, si, so, (const double*)Ct, StoreAxpy<double>{(double*)d, realpha}, s)
+                 : permute_general<double>(rk, dd, si, so, (const double*)Ct,
+                                           StoreScaled<double>{(double*)d, realpha}, s);
+    case kC4:
+      return permute_general<float2>(rk, dd, si, so, (const float2*)Ct,
+                                     StoreAxpyC<float2, float>{(float2*)d, (float)ar, (float)ai,
+                                                               accumulate ? 1.f : 0.f, 0.f}, s);
+    case kC8:
+      return permute_general<double2>(rk, dd, si, so, (const double2*)Ct,
+                                      StoreAxpyC<double2, double>{(double2*)d, ar, ai, accumulate ? 1.0 : 0.0, 0.0},
+                                      s);
+  }
+  return TB_ERR_INVALID_ARGS;
+}
+
+}  // namespace
+
+int contract_noalloc_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* d, int lrank,
+                          const int* ldims, const void* l, int rrank, const int* rdims, const void* r, double ar,
+                          double ai, int conj_bits, int accumulative, cudaStream_t s) {
+  std::memset(&g_stats, 0, sizeof(g_stats));
+  if (!elem_bytes(dtk)) {
+    set_error("tb_tensor_contract_noalloc: invalid data kind %d", dtk);
+    return TB_ERR_INVALID_ARGS;
+  }
+  if (!cptrn || !d || !l || !r) { set_error("tb_tensor_contract_noalloc: null argument"); return TB_ERR_INVALID_ARGS; }
+  Matricization Z;
+  int e = matricize(cptrn, drank, ddims, lrank, ldims, rrank, rdims, &Z);
+  if (e) { set_error("tb_tensor_contract_noalloc: pattern does not match the shapes (code %d)", e); return e; }
+  // Scratch bound: permuted L and R plus the product matrix (or the dot
+  // partials), each rounded up to 256 bytes; checked before anything is queued.
+  const unsigned __int128 es = (unsigned)elem_bytes(dtk);
+  const unsigned __int128 M = (uint64_t)Z.M, N = (uint64_t)Z.N, K = (uint64_t)Z.K;
+  const unsigned __int128 need = drank == 0 ? (unsigned __int128)round256(kDotBlocks * sizeof(double2))
+                                            : (unsigned __int128)round256(M * K * es) + round256(N * K * es) +
+                                                  round256(M * N * es);
+  if (need > (unsigned __int128)TB_NOALLOC_ARENA_BYTES) {
+    set_error("tb_tensor_contract_noalloc: this contraction needs %.0f bytes of scratch (permuted L and R and the "
+              "product matrix), more than the %llu-byte static scratch array; use tb_tensor_contract",
+              (double)need, (unsigned long long)TB_NOALLOC_ARENA_BYTES);
+    return TB_ERR_LIMIT;
+  }
+  if (!device_error_word_if_created()) {
+    set_error("tb_tensor_contract_noalloc: call tb_device_init on this device first");
+    return TB_ERR_INVALID_ARGS;
+  }
+  unsigned char* arena = nullptr;
+  if ((e = noalloc_arena(&arena))) return e;
+  int lconj = 0, rconj = 0;
+  if (is_complex(dtk)) {
+    lconj = (conj_bits >> 1) & 1; rconj = (conj_bits >> 2) & 1;
+    if (conj_bits & 1) { lconj ^= 1; rconj ^= 1; }
+  }
+  const bool cplx = is_complex(dtk), acc = accumulative != 0;
+  g_stats.m = Z.M; g_stats.n = Z.N; g_stats.k = Z.K;
+  g_stats.flops = (cplx ? 8.0 : 2.0) * (double)Z.M * (double)Z.N * (double)Z.K;
+  g_stats.method = TB_METHOD_TTGT;
+  if (drank == 0) {
+    const double br = acc ? 1.0 : 0.0;
+    const double ra = cplx ? ar : real_alpha(ar, ai), ia = cplx ? ai : 0.0;
+    switch (dtk) {
+      case kR4: return dot_noalloc<float, false>(Z, d, l, r, ra, ia, br, 0, 0, arena, s);
+      case kR8: return dot_noalloc<double, false>(Z, d, l, r, ra, ia, br, 0, 0, arena, s);
+      case kC4: return dot_noalloc<float2, true>(Z, d, l, r, ra, ia, br, lconj, rconj, arena, s);
+      case kC8: return dot_noalloc<double2, true>(Z, d, l, r, ra, ia, br, lconj, rconj, arena, s);
+    }
+  }
+  g_stats.gemm_launches = 1;
+  switch (dtk) {
+    case kR4: return ttgt_noalloc<float>(Z, dtk, ldims, l, rdims, r, d, ar, ai, acc, 0, 0, arena, s);
+    case kR8: return ttgt_noalloc<double>(Z, dtk, ldims, l, rdims, r, d, ar, ai, acc, 0, 0, arena, s);
+    case kC4: return ttgt_noalloc<float2>(Z, dtk, ldims, l, rdims, r, d, ar, ai, acc, lconj, rconj, arena, s);
+    case kC8: return ttgt_noalloc<double2>(Z, dtk, ldims, l, rdims, r, d, ar, ai, acc, lconj, rconj, arena, s);
+  }
+  return TB_ERR_INVALID_ARGS;
+}
+
+}  // namespace tb
+
+extern "C" int tb_tensor_contract_noalloc(const int* cptrn, int data_kind, int drank, const int* d_dims, void* d,
+                                          int lrank, const int* l_dims, const void* l, int rrank,
+                                          const int* r_dims, const void* r, double alpha_real, double alpha_imag,
+                                          int conj_bits, int accumulative, void* stream) {
+  return tb::contract_noalloc_impl(cptrn, data_kind, drank, d_dims, d, lrank, l_dims, l, rrank, r_dims, r,
+                                   alpha_real, alpha_imag, conj_bits, accumulative, (cudaStream_t)stream);
 }

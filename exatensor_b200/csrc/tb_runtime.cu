@@ -72,6 +72,12 @@ unsigned int* device_error_word() {
   return g_err_word[d];
 }
 
+unsigned int* device_error_word_if_created() {
+  const int d = current_device();
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_err_word[d];
+}
+
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
   *p = nullptr;
   if (bytes == 0) return 0;

@@ -127,6 +127,35 @@ int tb_tensor_contract_str(const char* pattern, int data_kind, int drank, const 
                            double alpha_imag, int accumulative, const tb_plan_t* plan,
                            void* stream);
 
+/* Size of the static per-device scratch array of tb_tensor_contract_noalloc. */
+#define TB_NOALLOC_ARENA_BYTES (64ull << 20)
+
+/* Plain (TTGT) contraction that allocates no memory.  It has no counterpart in
+ * the reference, whose contractions always draw their scratch from TAL-SH's
+ * device buffer pool.  It is for callers that may not allocate device memory
+ * while they run: code that has reserved all device memory up front, or that
+ * runs where an allocation would synchronise the device or is not permitted.
+ * Arguments and results are those of tb_tensor_contract, with the method
+ * fixed to TTGT (permute, GEMM in the tensor's own type, permute back).
+ *   - The permuted copies of L and R, the product matrix and the dot-product
+ *     partials live in one static device array of TB_NOALLOC_ARENA_BYTES,
+ *     which every GPU that loads this library holds until the process exits.
+ *     A contraction whose (M*K + N*K + M*N) * element size, each term rounded
+ *     up to 256 bytes, exceeds it is rejected with TB_ERR_LIMIT before any
+ *     work is queued; tb_tensor_contract has no such limit.
+ *   - tb_device_init must have run on the device first (it creates the
+ *     device error word this call reports through); else TB_ERR_INVALID_ARGS.
+ *   - The first call on each device looks up the array's device address (and
+ *     may load the library's GPU code there); make that first call before any
+ *     stream capture.
+ *   - Every call uses the same array and finds the previous call's data in
+ *     it.  Calls queued on one stream run in order and are safe; calls that
+ *     can overlap on the GPU (different streams, other host threads) race. */
+int tb_tensor_contract_noalloc(const int* cptrn, int data_kind, int drank, const int* d_dims,
+                               void* d, int lrank, const int* l_dims, const void* l, int rrank,
+                               const int* r_dims, const void* r, double alpha_real,
+                               double alpha_imag, int conj_bits, int accumulative, void* stream);
+
 /* Seeded U[lo,hi) fill on the device (splitmix64 stream, 53-bit fractions);
  * complex kinds fill real and imaginary parts from consecutive draws. */
 int tb_fill_uniform(int data_kind, size_t volume, void* d, uint64_t seed, double lo, double hi,
