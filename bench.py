@@ -388,7 +388,7 @@ def run_ours(args):
         per_launch_ms = gemm_ms / max(1, gemm_n)
         if chosen_method == "fused":
             kern = "tcgen05 INT8-slice GEMM" if wl["dtk"] in (8, 18) else "tcgen05 split-BF16 GEMM"
-            hw_ops = case.flops * max(1, st.passes)  # each pass is a full int8/bf16 GEMM
+            hw_ops = case.flops * max(1, st.products)  # each slice pair / BF16 term is a full GEMM
             peak = 2 * bf16_tflops if wl["dtk"] in (8, 18) else bf16_tflops
             peak_note = (f"2 x {peak_src} bf16 dense (INT8 dense rate)" if wl["dtk"] in (8, 18)
                          else f"{peak_src} bf16 dense")
@@ -410,7 +410,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if wl["dtk"] == 8 else "f32",
             "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v, D=0)",
             "config": {"workload": f"{args.workload}: {wl['pattern']} v={wl['v']} o={wl['o']}",
-                       "method": chosen_method, "slices": st.slices, "passes": st.passes,
+                       "method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products,
                        "l2": "inputs larger than L2 (V alone is 10.9 GB)", "parallelism": f"replicas x{world}"},
             "plain": {"value": round(plain, 3), "unit": "TFLOP/s", "method": "ttgt (permute + FP64 DMMA GEMM)",
                       "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),

@@ -539,6 +539,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     if (stats) {
       stats->slices = S;
       stats->passes = (int)passes.size();
+      stats->products = q;
       stats->gemm_launches = 1;
       stats->m = M; stats->n = Nr; stats->k = Kr;
     }

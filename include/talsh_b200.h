@@ -169,6 +169,8 @@ typedef struct {
   int gemm_launches; /* GEMM kernel launches */
   long long m, n, k; /* matricized sizes (real-expanded for complex on tensor cores) */
   double flops;      /* 2*M*N*K (real) or 8*M*N*K (complex), the reference's accounting */
+  int products;      /* plane products the tensor-core GEMM ran (INT8 slice pairs or BF16
+                        terms); its tensor-core work is products * flops */
 } tb_contract_stats_t;
 int tb_last_contract_stats(tb_contract_stats_t* stats);
 
