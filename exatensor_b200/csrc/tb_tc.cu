@@ -1,13 +1,14 @@
 // tb_tc.cu -- the tensor-core contraction path (TB_METHOD_FUSED).
 //
-// FP64 (R8, C8): Ozaki-style splitting into INT8 slices.  Each row m of the
+// FP64 (R8, C8): Ozaki-style splitting into 8-bit slices.  Each row m of the
 // matricized left operand is scaled by 2^-e_m (e_m from the row's largest
-// exponent) into (-1, 1) and written as s signed 7-bit digits
-// a = 2^e_m * sum_i A_i 2^(-7i) (truncation, exact in FP64); the right
+// exponent) into (-1/2, 1/2) and cut into s balanced signed 8-bit digits of
+// weight 2^-(8i+7), i = 0..s-1 (exact in FP64; see fixed55); the right
 // operand likewise per column.  The tcgen05 GEMM (tb_tc_gemm.cuh) multiplies
-// slice pairs (i, j) with i + j <= s + 1 exactly in INT32, grouping pairs with
-// the same i + j into one TMEM accumulator as long as no INT32 overflow is
-// possible, and the epilogue adds 2^(e_m + f_n - 7(i+j)) * acc in FP64 into D.
+// slice pairs (i, j) with i + j <= s - 1 exactly in INT32 (kind::i8),
+// grouping pairs of equal i + j, split along K where needed, into one TMEM
+// accumulator while no INT32 overflow is possible, and the epilogue adds
+// 2^(e_m + f_n - 8(i+j) - 14) * acc in FP64 into D.
 // FP32 (R4, C4): each value splits into BF16 high and low parts; the three
 // products hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM.
 // Complex data runs as a real GEMM of twice the size: A' = [Ar Ai] interleaved
@@ -124,7 +125,7 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
 // writes 4 consecutive K positions of each output plane in one store.
 // Tiles cover [0, rows_pad) x [0, kpad_src): padding is written as zeros.
 constexpr int kGThreads = 256;
-constexpr int kMaxSlicesDev = 8;
+constexpr int kMaxSlicesDev = 7;
 template <typename E> constexpr int gather_rows() { return sizeof(E) == 16 ? 32 : 64; }  // 32-34 KB tiles
 constexpr int kGK = 64;
 
@@ -144,18 +145,24 @@ struct GatherParams {
   double isign;        // -1 conjugates the imaginary part
 };
 
-// Signed base-128 digits of x in (-1, 1), most significant first: the digits
-// of trunc(x * 2^56) in sign-magnitude form (identical to repeatedly taking
-// trunc(128 x) and keeping the remainder, which is exact in FP64).
-__device__ __forceinline__ void digits8(double x, int8_t (&d)[kMaxSlicesDev]) {
-  const long long X = __double2ll_rz(x * 72057594037927936.0);  // 2^56
-  const unsigned long long U = (unsigned long long)(X < 0 ? -X : X);
-  const bool neg = X < 0;
-#pragma unroll
-  for (int i = 0; i < kMaxSlicesDev; ++i) {
-    const int v = (int)((U >> (49 - 7 * i)) & 127ull);
-    d[i] = (int8_t)(neg ? -v : v);
-  }
+// Slices of x in (-1/2, 1/2): balanced signed base-256 digits of the fixed-point
+// value X = floor(x * 2^55) = sum_i d_i 2^(48-8i), d_i in [-128, 127] for
+// i >= 1 and |d_0| <= 64.  With Y = X + 0x808080808080 the low bytes of Y are
+// d_i + 128 and Y >> 48 = d_0, so each slice is one byte of Y (bit 7 flipped
+// for i >= 1).  Digit i has weight 2^-(8i+7); the digits are centred on zero,
+// so the parts dropped by keeping s slices or slice pairs do not accumulate a
+// bias over K.  The scaling by 2^55 is exact and the conversion rounds toward
+// minus infinity.
+__device__ __forceinline__ long long fixed55(double x) {
+  return __double2ll_rd(x * 36028797018963968.0) + 0x808080808080ll;  // 2^55; Y
+}
+// Slice i of four consecutive values, packed little-endian into one word.
+__device__ __forceinline__ uint32_t slice4(long long y0, long long y1, long long y2, long long y3, int i) {
+  const int sh = 48 - 8 * i;
+  const uint32_t flip = i == 0 ? 0u : 0x80808080u;
+  return ((uint32_t)((y0 >> sh) & 255) | ((uint32_t)((y1 >> sh) & 255) << 8) |
+          ((uint32_t)((y2 >> sh) & 255) << 16) | ((uint32_t)((y3 >> sh) & 255) << 24)) ^
+         flip;
 }
 
 template <int MODE>
@@ -170,13 +177,13 @@ __global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant
   __shared__ E tile[TM][TK + 1];
   __shared__ int64_t sm_lm[TM], sm_lk[TK];
   __shared__ unsigned sm_max[TM];
-  __shared__ double sm_sc[TM];
+  __shared__ int sm_se[TM];  // slice modes: the row's scale exponent
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   const int tid = threadIdx.x;
   if (tid < TM) {
     sm_lm[tid] = (m0 + tid < P.rows) ? P.lm[m0 + tid] : -1;
     sm_max[tid] = 0;
-    if constexpr (!EXP && !F32) sm_sc[tid] = pow2d(1022 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1022u));
+    if constexpr (!EXP && !F32) sm_se[tid] = 1021 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1021u);
   }
   const E* src = (const E*)P.src;
   const int64_t nkt = (P.K + TK - 1) / TK;                   // tiles with data
@@ -215,53 +222,53 @@ __global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant
         const int mm = idx / (TK / 4), kq = (idx % (TK / 4)) * 4;
         const int64_t m = m0 + mm, k = k0 + kq;
         if constexpr (MODE == G_SLICE_R8) {
-          const double sc = sm_sc[mm];
-          int8_t d[4][kMaxSlicesDev];
+          const int se = sm_se[mm];
+          long long X[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) digits8(tile[mm][kq + t] * sc, d[t]);
+          for (int t = 0; t < 4; ++t) X[t] = fixed55(scale2(tile[mm][kq + t], se));
           int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
 #pragma unroll
           for (int i = 0; i < kMaxSlicesDev; ++i)
-            if (i < P.slices) {
-              char4 w; w.x = d[0][i]; w.y = d[1][i]; w.z = d[2][i]; w.w = d[3][i];
-              *reinterpret_cast<char4*>(base + i * P.pstride) = w;
-            }
-        } else if constexpr (MODE == G_SLICE_C8A || MODE == G_SLICE_C8B) {
-          const double sc = sm_sc[mm];
-          int8_t dr[4][kMaxSlicesDev], di[4][kMaxSlicesDev];
+            if (i < P.slices) *reinterpret_cast<uint32_t*>(base + i * P.pstride) = slice4(X[0], X[1], X[2], X[3], i);
+        } else if constexpr (MODE == G_SLICE_C8A) {
+          // A' row m: (re, im) interleaved along K
+          const int se = sm_se[mm];
+          long long R[4], I[4];
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
             const E v = tile[mm][kq + t];
-            digits8(v.x * sc, dr[t]);
-            digits8(P.isign * v.y * sc, di[t]);
+            R[t] = fixed55(scale2(v.x, se));
+            I[t] = fixed55(scale2(P.isign * v.y, se));
           }
-          if constexpr (MODE == G_SLICE_C8A) {
-            int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
+          int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
 #pragma unroll
-            for (int i = 0; i < kMaxSlicesDev; ++i)
-              if (i < P.slices) {
-                char4 w0; w0.x = dr[0][i]; w0.y = di[0][i]; w0.z = dr[1][i]; w0.w = di[1][i];
-                char4 w1; w1.x = dr[2][i]; w1.y = di[2][i]; w1.z = dr[3][i]; w1.w = di[3][i];
-                *reinterpret_cast<char4*>(base + i * P.pstride) = w0;
-                *reinterpret_cast<char4*>(base + i * P.pstride + 4) = w1;
-              }
-          } else {
-            int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
-            int8_t* b1 = b0 + P.kpad;
+          for (int i = 0; i < kMaxSlicesDev; ++i)
+            if (i < P.slices) {
+              uint2 w = make_uint2(slice4(R[0], I[0], R[1], I[1], i), slice4(R[2], I[2], R[3], I[3], i));
+              *reinterpret_cast<uint2*>(base + i * P.pstride) = w;
+            }
+        } else if constexpr (MODE == G_SLICE_C8B) {
+          // B' rows 2n = (re, -im), 2n+1 = (im, re) interleaved along K
+          const int se = sm_se[mm];
+          long long R[4], I[4], NI[4];
 #pragma unroll
-            for (int i = 0; i < kMaxSlicesDev; ++i)
-              if (i < P.slices) {
-                char4 a0, a1, c0, c1;
-                a0.x = dr[0][i]; a0.y = (int8_t)-di[0][i]; a0.z = dr[1][i]; a0.w = (int8_t)-di[1][i];
-                a1.x = dr[2][i]; a1.y = (int8_t)-di[2][i]; a1.z = dr[3][i]; a1.w = (int8_t)-di[3][i];
-                c0.x = di[0][i]; c0.y = dr[0][i]; c0.z = di[1][i]; c0.w = dr[1][i];
-                c1.x = di[2][i]; c1.y = dr[2][i]; c1.z = di[3][i]; c1.w = dr[3][i];
-                *reinterpret_cast<char4*>(b0 + i * P.pstride) = a0;
-                *reinterpret_cast<char4*>(b0 + i * P.pstride + 4) = a1;
-                *reinterpret_cast<char4*>(b1 + i * P.pstride) = c0;
-                *reinterpret_cast<char4*>(b1 + i * P.pstride + 4) = c1;
-              }
+          for (int t = 0; t < 4; ++t) {
+            const E v = tile[mm][kq + t];
+            const double im = scale2(P.isign * v.y, se);
+            R[t] = fixed55(scale2(v.x, se));
+            I[t] = fixed55(im);
+            NI[t] = fixed55(-im);
           }
+          int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
+          int8_t* b1 = b0 + P.kpad;
+#pragma unroll
+          for (int i = 0; i < kMaxSlicesDev; ++i)
+            if (i < P.slices) {
+              *reinterpret_cast<uint2*>(b0 + i * P.pstride) =
+                  make_uint2(slice4(R[0], NI[0], R[1], NI[1], i), slice4(R[2], NI[2], R[3], NI[3], i));
+              *reinterpret_cast<uint2*>(b1 + i * P.pstride) =
+                  make_uint2(slice4(I[0], R[0], I[1], R[1], i), slice4(I[2], R[2], I[3], R[3], i));
+            }
         } else if constexpr (MODE == G_SPLIT_R4) {
           __nv_bfloat16 h[4], l[4];
 #pragma unroll
@@ -309,15 +316,15 @@ __global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant
   }
 }
 
-// exponents: rowexp[r] = rowE[r / rep] - 1022 (rep = 2 for complex B' rows)
+// exponents: rowexp[r] = rowE[r / rep] - 1021 (rep = 2 for complex B' rows)
 __global__ void exps_kernel(const unsigned* __restrict__ rowE, int* __restrict__ out, int64_t n, int rep) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int)rowE[i / rep] - 1022;
+    out[i] = (int)rowE[i / rep] - 1021;
 }
 
 // ---- driver ----------------------------------------------------------------------
-constexpr int kDefaultSlices = 7;
-constexpr int kMaxSlices = 8;
+constexpr int kDefaultSlices = 6;
+constexpr int kMaxSlices = 7;  // 7 slices hold all 55 bits of the fixed-point value
 
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
@@ -410,36 +417,55 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   const int BN = (plan && plan->tile_n == 128) ? 128 : (plan && plan->tile_n == 256) ? 256 : (Nr >= 192 ? 256 : 128);
   const int64_t Mpad = round_up(M, 128), Npad = round_up(Nr, BN);
   if (Mpad / 128 * (Npad / BN) > INT32_MAX || M > INT32_MAX || Nr > INT32_MAX) return TB_ERR_LIMIT;
-  // products and passes
-  std::vector<std::vector<std::pair<int, int>>> passes;
+  // products and passes: an entry multiplies plane a of A by plane b of B over
+  // a K-block range; the entries of a pass share one exact INT32 accumulator.
+  struct Entry { int a, b, kb0, kb1; };
+  std::vector<std::vector<Entry>> passes;
   std::vector<int> shifts;
+  const int kblocks = (int)(Kpad * (i8 ? 1 : 2) / 128);  // 128-byte K blocks
   int S = 0, npa = 2, npb = 2;
   if (i8) {
     S = (plan && plan->slices > 0) ? plan->slices : kDefaultSlices;
     if (S < 2 || S > kMaxSlices) { set_error("slice count %d outside 2..%d", S, kMaxSlices); return TB_ERR_INVALID_ARGS; }
-    const int64_t per = (int64_t)127 * 127 * Kr;
-    const int64_t cap = (int64_t)INT32_MAX / per;
-    if (cap < 1) return TB_ERR_NOT_IMPLEMENTED;  // K too long for exact INT32 accumulation
-    for (int dsum = 2; dsum <= S + 1; ++dsum) {
-      std::vector<std::pair<int, int>> diag;
-      for (int i = 1; i < dsum; ++i)
-        if (i <= S && dsum - i <= S) diag.push_back({i - 1, dsum - i - 1});
-      for (size_t b = 0; b < diag.size(); b += cap) {
-        passes.emplace_back(diag.begin() + b, diag.begin() + std::min(diag.size(), (size_t)(b + cap)));
-        shifts.push_back(7 * dsum);
+    // |slice| <= 128, so one K block (128 products) adds at most 128^3.
+    const int64_t cap = INT32_MAX;
+    for (int dsum = 2; dsum <= S + 1; ++dsum) {   // 1-based slice indices with i + j = dsum
+      std::vector<Entry> cur;
+      int64_t load = 0;
+      for (int i = 1; i < dsum; ++i) {
+        const int j = dsum - i;
+        if (i > S || j > S) continue;
+        const int64_t per_block = (int64_t)128 * 128 * 128;
+        const int64_t max_blocks = cap / per_block;
+        for (int kb = 0; kb < kblocks;) {
+          int64_t room = (cap - load) / per_block;
+          if (room < 1) { passes.push_back(cur); shifts.push_back(8 * dsum - 2); cur.clear(); load = 0; room = max_blocks; }
+          const int n = (int)std::min<int64_t>(room, kblocks - kb);
+          cur.push_back({i - 1, j - 1, kb, kb + n});
+          load += per_block * n;
+          kb += n;
+        }
       }
+      if (!cur.empty()) { passes.push_back(cur); shifts.push_back(8 * dsum - 2); }
     }
     npa = npb = S;
   } else {
     const int terms = (plan && plan->bf16_terms == 4) ? 4 : 3;
-    std::vector<std::pair<int, int>> p3 = {{0, 0}, {0, 1}, {1, 0}};
-    if (terms == 4) p3.push_back({1, 1});
+    std::vector<Entry> p3 = {{0, 0, 0, kblocks}, {0, 1, 0, kblocks}, {1, 0, 0, kblocks}};
+    if (terms == 4) p3.push_back({1, 1, 0, kblocks});
     passes.push_back(p3);
     shifts.push_back(0);
   }
-  int nprod = 0;
-  for (auto& p : passes) nprod += (int)p.size();
-  if (nprod > kMaxProducts || (int)passes.size() > kMaxProducts) return TB_ERR_NOT_IMPLEMENTED;
+  int nprod = 0, nplane_products = 0;
+  for (auto& p : passes) {
+    nprod += (int)p.size();
+    for (auto& e : p) nplane_products += (e.kb0 == 0);  // count each plane pair once
+  }
+  if (nprod > kMaxProducts || (int)passes.size() > kMaxProducts) {
+    set_error("tensor-core plan needs %d GEMM entries in %d passes (limit %d)", nprod, (int)passes.size(),
+              kMaxProducts);
+    return TB_ERR_NOT_IMPLEMENTED;
+  }
   // scratch: operand planes, offset tables, exponents
   const int oes = i8 ? 1 : 2;
   const size_t bytesA = (size_t)npa * Mpad * Kpad * oes, bytesB = (size_t)npb * Npad * Kpad * oes;
@@ -524,7 +550,10 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     for (size_t p = 0; p < passes.size(); ++p) {
       P.pass_first[p] = q;
       P.pass_shift[p] = shifts[p];
-      for (auto& pr : passes[p]) { P.prod_a[q] = pr.first; P.prod_b[q] = pr.second; ++q; }
+      for (auto& e : passes[p]) {
+        P.prod_a[q] = e.a; P.prod_b[q] = e.b; P.prod_kb0[q] = e.kb0; P.prod_kb1[q] = e.kb1;
+        ++q;
+      }
     }
     P.pass_first[passes.size()] = q;
     P.D = d; P.dm = dm; P.dn = dn; P.rowexp = rowx; P.colexp = colx;
@@ -539,7 +568,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     if (stats) {
       stats->slices = S;
       stats->passes = (int)passes.size();
-      stats->products = q;
+      stats->products = nplane_products;
       stats->gemm_launches = 1;
       stats->m = M; stats->n = Nr; stats->k = Kr;
     }

@@ -1,7 +1,7 @@
 // tb_tc_gemm.cuh -- persistent tcgen05 GEMM with multi-pass accumulation and
 // a fused tensor epilogue.
 //
-//   C[m][n] = sum over passes p of  scale_p(m,n) * sum_{(a,b) in p} sum_k A_a[m][k] * B_b[n][k]
+//   C[m][n] = sum over passes p of  scale_p(m,n) * sum_{(a,b,k0,k1) in p} sum_{k0<=k<k1} A_a[m][k] * B_b[n][k]
 //   D[dm[m] + dn[n]] = beta*D + alpha*C    (dm/dn: the output permutation)
 //
 // A_a / B_b are planes of K-major operands (INT8 slices of FP64 data, or
@@ -20,7 +20,7 @@
 namespace tb {
 
 constexpr int kStagesTC = 4;
-constexpr int kMaxProducts = 64;
+constexpr int kMaxProducts = 64;  // entries (plane pair and K range) over all passes
 constexpr int kTcThreads = 192;
 
 enum TcEpilogue { EPI_OZAKI_R = 0, EPI_OZAKI_C = 1, EPI_BF16_R = 2, EPI_BF16_C = 3 };
@@ -32,9 +32,10 @@ struct __align__(64) TcGemmParams {
   int mtiles, ntiles;         // tiles of 128 rows x BN columns
   int kblocks;                // 128-byte K blocks
   int npass;
-  int pass_first[kMaxProducts + 1];
-  int prod_a[kMaxProducts], prod_b[kMaxProducts];
-  int pass_shift[kMaxProducts];      // INT8 slices: 7*(i+j) of the pass
+  int pass_first[kMaxProducts + 1];  // entries of pass p: [pass_first[p], pass_first[p+1])
+  int prod_a[kMaxProducts], prod_b[kMaxProducts];    // plane of A and of B
+  int prod_kb0[kMaxProducts], prod_kb1[kMaxProducts];  // K-block range
+  int pass_shift[kMaxProducts];      // INT8 slices: the pass's weight is 2^-pass_shift
   void* D;
   const int64_t* dm;          // D offset of row m (elements of D's data kind)
   const int64_t* dn;          // D offset of column n (complex: of column pair n/2)
@@ -58,9 +59,13 @@ __host__ __device__ constexpr size_t tc_smem_bytes() {
 }
 
 __device__ __forceinline__ double pow2d(int e) {
-  // exact 2^e for the exponent range of these scales
+  // exact 2^e for -1022 <= e <= 1023 (clamped outside)
   e = e < -1022 ? -1022 : (e > 1023 ? 1023 : e);
   return __longlong_as_double((long long)(e + 1023) << 52);
+}
+// x * 2^e with one rounding, also when the result is subnormal (e >= -2100).
+__device__ __forceinline__ double scale2(double x, int e) {
+  return e >= -1022 ? x * pow2d(e) : (x * pow2d(e + 1022)) * pow2d(-1022);
 }
 
 template <int BN, bool I8, int EPI>
@@ -100,7 +105,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
       for (int t = blockIdx.x; t < ntile_total && ok; t += gridDim.x) {
         const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
         for (int q = 0; q < nprod && ok; ++q) {
-          for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+          for (int kb = P.prod_kb0[q]; kb < P.prod_kb1[q]; ++kb, ++it) {
             const int s = it % kStagesTC;
             const uint32_t ph = (it / kStagesTC) & 1;
             if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err))) break;
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
           const uint32_t dcol = tmem + (uint32_t)(a * BN);
           bool first = true;
           for (int q = P.pass_first[p]; q < P.pass_first[p + 1] && ok; ++q) {
-            for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+            for (int kb = P.prod_kb0[q]; kb < P.prod_kb1[q]; ++kb, ++it) {
               const int s = it % kStagesTC;
               const uint32_t ph = (it / kStagesTC) & 1;
               if (!(ok = mbar_wait(&bars->full[s], ph, P.err))) break;
@@ -156,8 +161,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
       const int m = mb * 128 + quad * 32 + lane;
       const bool mval = m < P.M;
       const int64_t dmo = mval ? P.dm[m] : 0;
-      double rs = 1.0;
-      if (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) rs = mval ? pow2d(P.rowexp[m]) : 0.0;
+      const int re = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) && mval ? P.rowexp[m] : 0;
       for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
@@ -177,8 +181,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
             for (int j = 0; j < 32; ++j) {
               const int n = n0 + j;
               if (n >= P.N) break;
-              const double sc = pow2d(P.colexp[n] - shift) * rs;
-              const double v = P.ar * ((double)(int)r[j] * sc);
+              const double v = P.ar * scale2((double)(int)r[j], re + P.colexp[n] - shift);
               double* dp = D + dmo + P.dn[n];
               *dp = first ? (P.br == 0.0 ? v : fma(P.br, *dp, v)) : (*dp + v);
             }
@@ -188,8 +191,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
             for (int j = 0; j < 32; j += 2) {
               const int n = n0 + j;
               if (n >= P.N) break;
-              const double sc = pow2d(P.colexp[n] - shift) * rs;
-              const double xr = (double)(int)r[j] * sc, xi = (double)(int)r[j + 1] * sc;
+              const int e = re + P.colexp[n] - shift;
+              const double xr = scale2((double)(int)r[j], e), xi = scale2((double)(int)r[j + 1], e);
               double2 v = make_double2(P.ar * xr - P.ai * xi, P.ar * xi + P.ai * xr);
               double2* dp = D + dmo + P.dn[n >> 1];
               double2 d = *dp;
