@@ -35,9 +35,9 @@ class TBError(RuntimeError):
 
 
 class Plan(C.Structure):
-    """tb_plan_t: contraction plan (method, INT8 slices, N tile, split-BF16 terms)."""
+    """tb_plan_t: contraction plan (method, INT8 slices, N tile, split-BF16 terms, M tile)."""
     _fields_ = [("method", C.c_int), ("slices", C.c_int), ("tile_n", C.c_int), ("bf16_terms", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("tile_m", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class ContractStats(C.Structure):
@@ -148,9 +148,9 @@ def fill_uniform(dtk, volume, d_ptr, seed, lo=-1.0, hi=1.0, stream=None):
     _check(lib().tb_fill_uniform(dtk, volume, C.c_void_p(d_ptr), seed, lo, hi, _stream(stream)))
 
 
-def make_plan(method=METHOD_AUTO, slices=0, tile_n=0, bf16_terms=0) -> Plan:
+def make_plan(method=METHOD_AUTO, slices=0, tile_n=0, bf16_terms=0, tile_m=0) -> Plan:
     p = Plan()
-    p.method, p.slices, p.tile_n, p.bf16_terms = method, slices, tile_n, bf16_terms
+    p.method, p.slices, p.tile_n, p.bf16_terms, p.tile_m = method, slices, tile_n, bf16_terms, tile_m
     return p
 
 

@@ -366,8 +366,49 @@ int launch_tc(const TcGemmParams& P, cudaStream_t s) {
   return 0;
 }
 
+// CTA-pair kernel: grid = 2 x (pairs that can be resident at once, capped by the tiles).
+template <int BN, bool I8, int EPI>
+int launch_tc2(const TcGemmParams& P, cudaStream_t s) {
+  constexpr size_t smem = tc2_smem_bytes<BN>();
+  static int max_pairs = 0;
+  if (!max_pairs) {
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm2_kernel<BN, I8, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) { set_error("tcgen05 pair GEMM smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * (unsigned)num_sms(), 1, 1);
+    cfg.blockDim = dim3(kTcThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 2; attr.val.clusterDim.y = 1; attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    e = cudaOccupancyMaxActiveClusters(&n, tc_gemm2_kernel<BN, I8, EPI>, &cfg);
+    if (e != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      n = num_sms() / 2;
+    }
+    max_pairs = n;
+  }
+  const int tiles = P.mtiles * P.ntiles;
+  const int pairs = std::max(1, std::min(tiles, max_pairs));
+  tc_gemm2_kernel<BN, I8, EPI><<<2 * pairs, kTcThreads, smem, s>>>(P);
+  TB_CHECK_LAUNCH();
+  return 0;
+}
+
 template <int BN>
-int launch_tc_epi(const TcGemmParams& P, int epi, cudaStream_t s) {
+int launch_tc_epi(const TcGemmParams& P, int epi, bool pair, cudaStream_t s) {
+  if (pair) {
+    switch (epi) {
+      case EPI_OZAKI_R: return launch_tc2<BN, true, EPI_OZAKI_R>(P, s);
+      case EPI_OZAKI_C: return launch_tc2<BN, true, EPI_OZAKI_C>(P, s);
+      case EPI_BF16_R: return launch_tc2<BN, false, EPI_BF16_R>(P, s);
+      default: return launch_tc2<BN, false, EPI_BF16_C>(P, s);
+    }
+  }
   switch (epi) {
     case EPI_OZAKI_R: return launch_tc<BN, true, EPI_OZAKI_R>(P, s);
     case EPI_OZAKI_C: return launch_tc<BN, true, EPI_OZAKI_C>(P, s);
@@ -415,7 +456,12 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   const int64_t Kr = cplx ? 2 * K : K, Nr = cplx ? 2 * Nc : Nc;
   const int64_t Kpad = round_up(Kr, 128);
   const int BN = (plan && plan->tile_n == 128) ? 128 : (plan && plan->tile_n == 256) ? 256 : (Nr >= 192 ? 256 : 128);
-  const int64_t Mpad = round_up(M, 128), Npad = round_up(Nr, BN);
+  // M tile: one SM per 128-row tile unless the plan asks for SM pairs (256
+  // rows); the pair kernel halves the B traffic per SM but measured no faster
+  // on the CCSD-like shapes, whose GEMMs run at the power cap.
+  const bool pair = plan && plan->tile_m == 256;
+  const int TM = pair ? 256 : 128;
+  const int64_t Mpad = round_up(M, TM), Npad = round_up(Nr, BN);
   if (Mpad / 128 * (Npad / BN) > INT32_MAX || M > INT32_MAX || Nr > INT32_MAX) return TB_ERR_LIMIT;
   // products and passes: an entry multiplies plane a of A by plane b of B over
   // a K-block range; the entries of a pass share one exact INT32 accumulator.
@@ -541,9 +587,9 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     static TcGemmParams P;  // large: kept off the stack
     std::memset(&P, 0, sizeof(P));
     if ((err = make_operand_map(&P.tmA, Ap, i8, Kpad, Mpad, npa, 128))) break;
-    if ((err = make_operand_map(&P.tmB, Bp, i8, Kpad, Npad, npb, BN))) break;
+    if ((err = make_operand_map(&P.tmB, Bp, i8, Kpad, Npad, npb, pair ? BN / 2 : BN))) break;
     P.M = (int)M; P.N = (int)Nr;
-    P.mtiles = (int)(Mpad / 128); P.ntiles = (int)(Npad / BN);
+    P.mtiles = (int)(Mpad / TM); P.ntiles = (int)(Npad / BN);
     P.kblocks = (int)(Kpad * oes / 128);
     P.npass = (int)passes.size();
     int q = 0;
@@ -563,7 +609,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     P.err = device_error_word();
     const int epi = i8 ? (cplx ? EPI_OZAKI_C : EPI_OZAKI_R) : (cplx ? EPI_BF16_C : EPI_BF16_R);
     const int ts = timed_begin(s);
-    err = BN == 256 ? launch_tc_epi<256>(P, epi, s) : launch_tc_epi<128>(P, epi, s);
+    err = BN == 256 ? launch_tc_epi<256>(P, epi, pair, s) : launch_tc_epi<128>(P, epi, pair, s);
     timed_end(ts, s);
     if (stats) {
       stats->slices = S;

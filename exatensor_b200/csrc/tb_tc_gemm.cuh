@@ -17,6 +17,8 @@
 #include "tb_common.cuh"
 #include "tb_sm100.cuh"
 
+#include <type_traits>
+
 namespace tb {
 
 constexpr int kStagesTC = 4;
@@ -66,6 +68,97 @@ __device__ __forceinline__ double pow2d(int e) {
 // x * 2^e with one rounding, also when the result is subnormal (e >= -2100).
 __device__ __forceinline__ double scale2(double x, int e) {
   return e >= -1022 ? x * pow2d(e) : (x * pow2d(e + 1022)) * pow2d(-1022);
+}
+
+// One accumulator pass of the epilogue for the row held by this thread: reads
+// the BN accumulator columns of TMEM lane `tcol` (lane and column base
+// encoded) 32 at a time, scales them and updates D through the offset tables.
+// Column metadata (D offset, scale exponent) is loaded once per 32 columns, one
+// column per lane, and broadcast with shuffles; all 32 loads of D of a chunk
+// are issued before any of them is used, so that a warp keeps 1024 loads in
+// flight instead of waiting on each one.
+template <int BN, int EPI>
+__device__ __forceinline__ void epilogue_pass(const TcGemmParams& P, uint32_t tcol, bool mval, int64_t dmo, int re,
+                                              int nb, bool first, int shift) {
+  using namespace sm100;
+  constexpr bool OZ = EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C;
+  constexpr bool CPLX = EPI == EPI_OZAKI_C || EPI == EPI_BF16_C;
+  const int lane = threadIdx.x & 31;
+  const bool load_d = !(first && P.br == 0.0 && P.bi == 0.0);
+#pragma unroll 1
+  for (int c = 0; c < BN / 32; ++c) {
+    uint32_t r[32];
+    tmem_ld32(tcol + (uint32_t)(c * 32), r);
+    const int n0 = nb * BN + c * 32;
+    // lane j: metadata of column n0 + j (complex: of column pair (n0 + j) / 2)
+    const int nl = n0 + lane;
+    const bool lvalid = nl < P.N;
+    const int64_t dn_l = lvalid ? P.dn[CPLX ? (nl >> 1) : nl] : 0;
+    const int ce_l = (OZ && lvalid) ? P.colexp[nl] : 0;
+    if (!CPLX) {
+      using T = typename std::conditional<OZ, double, float>::type;
+      T* D = (T*)P.D;
+      T old[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int64_t dn = __shfl_sync(0xffffffffu, dn_l, j);
+        old[j] = (load_d && mval && n0 + j < P.N) ? D[dmo + dn] : (T)0;
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int64_t dn = __shfl_sync(0xffffffffu, dn_l, j);
+        const int ce = __shfl_sync(0xffffffffu, ce_l, j);
+        if (!mval || n0 + j >= P.N) continue;
+        T v;
+        if (OZ) v = (T)(P.ar * scale2((double)(int)r[j], re + ce - shift));
+        else v = (T)P.ar * __uint_as_float(r[j]);
+        T o;
+        if (!first) o = old[j] + v;
+        else if (P.br == 0.0) o = v;
+        else if (OZ) o = fma((double)P.br, (double)old[j], (double)v);
+        else o = fmaf((float)P.br, (float)old[j], (float)v);
+        D[dmo + dn] = o;
+      }
+    } else {
+      using T2 = typename std::conditional<OZ, double2, float2>::type;
+      using T = typename std::conditional<OZ, double, float>::type;
+      T2* D = (T2*)P.D;
+      T2 old[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int64_t dn = __shfl_sync(0xffffffffu, dn_l, 2 * j);
+        T2 z; z.x = 0; z.y = 0;
+        old[j] = (load_d && mval && n0 + 2 * j < P.N) ? D[dmo + dn] : z;
+      }
+      const T ar = (T)P.ar, ai = (T)P.ai, br = (T)P.br, bi = (T)P.bi;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int64_t dn = __shfl_sync(0xffffffffu, dn_l, 2 * j);
+        const int ce = __shfl_sync(0xffffffffu, ce_l, 2 * j);
+        if (!mval || n0 + 2 * j >= P.N) continue;
+        T xr, xi;
+        if (OZ) {
+          const int e = re + ce - shift;
+          xr = (T)scale2((double)(int)r[2 * j], e);
+          xi = (T)scale2((double)(int)r[2 * j + 1], e);
+        } else {
+          xr = __uint_as_float(r[2 * j]);
+          xi = __uint_as_float(r[2 * j + 1]);
+        }
+        T2 v;
+        v.x = ar * xr - ai * xi;
+        v.y = ar * xi + ai * xr;
+        const T2 d = old[j];
+        if (first) {
+          v.x += br * d.x - bi * d.y;
+          v.y += br * d.y + bi * d.x;
+        } else {
+          v.x += d.x; v.y += d.y;
+        }
+        D[dmo + dn] = v;
+      }
+    }
+  }
 }
 
 template <int BN, bool I8, int EPI>
@@ -169,73 +262,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
         tc_fence_after();
         const bool first = (p == 0);
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) ? P.pass_shift[p] : 0;
-#pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
-          uint32_t r[32];
-          tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN + c * 32), r);
-          const int n0 = nb * BN + c * 32;
-          if (!mval) continue;
-          if (EPI == EPI_OZAKI_R) {
-            double* D = (double*)P.D;
-#pragma unroll 8
-            for (int j = 0; j < 32; ++j) {
-              const int n = n0 + j;
-              if (n >= P.N) break;
-              const double v = P.ar * scale2((double)(int)r[j], re + P.colexp[n] - shift);
-              double* dp = D + dmo + P.dn[n];
-              *dp = first ? (P.br == 0.0 ? v : fma(P.br, *dp, v)) : (*dp + v);
-            }
-          } else if (EPI == EPI_OZAKI_C) {
-            double2* D = (double2*)P.D;
-#pragma unroll 4
-            for (int j = 0; j < 32; j += 2) {
-              const int n = n0 + j;
-              if (n >= P.N) break;
-              const int e = re + P.colexp[n] - shift;
-              const double xr = scale2((double)(int)r[j], e), xi = scale2((double)(int)r[j + 1], e);
-              double2 v = make_double2(P.ar * xr - P.ai * xi, P.ar * xi + P.ai * xr);
-              double2* dp = D + dmo + P.dn[n >> 1];
-              double2 d = *dp;
-              if (first) {
-                v.x += P.br * d.x - P.bi * d.y;
-                v.y += P.br * d.y + P.bi * d.x;
-              } else {
-                v.x += d.x; v.y += d.y;
-              }
-              *dp = v;
-            }
-          } else if (EPI == EPI_BF16_R) {
-            float* D = (float*)P.D;
-            const float ar = (float)P.ar, br = (float)P.br;
-#pragma unroll 8
-            for (int j = 0; j < 32; ++j) {
-              const int n = n0 + j;
-              if (n >= P.N) break;
-              const float v = ar * __uint_as_float(r[j]);
-              float* dp = D + dmo + P.dn[n];
-              *dp = first ? (br == 0.f ? v : fmaf(br, *dp, v)) : (*dp + v);
-            }
-          } else {
-            float2* D = (float2*)P.D;
-            const float ar = (float)P.ar, ai = (float)P.ai, br = (float)P.br, bi = (float)P.bi;
-#pragma unroll 4
-            for (int j = 0; j < 32; j += 2) {
-              const int n = n0 + j;
-              if (n >= P.N) break;
-              const float xr = __uint_as_float(r[j]), xi = __uint_as_float(r[j + 1]);
-              float2 v = make_float2(ar * xr - ai * xi, ar * xi + ai * xr);
-              float2* dp = D + dmo + P.dn[n >> 1];
-              float2 d = *dp;
-              if (first) {
-                v.x += br * d.x - bi * d.y;
-                v.y += br * d.y + bi * d.x;
-              } else {
-                v.x += d.x; v.y += d.y;
-              }
-              *dp = v;
-            }
-          }
-        }
+        epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, nb, first,
+                               shift);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&bars->acc_empty[a]);
@@ -247,6 +275,157 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
     tc_fence_after();
     tmem_dealloc(tmem, 2 * BN);
   }
+}
+
+// ---------------------------------------------------------------------------
+// CTA-pair variant (cluster of 2, tcgen05 cta_group::2): one 256 x BN output
+// tile per pair iteration.  CTA r of the pair stages rows [128r, 128r+128) of
+// the A tile and rows [r*BN/2, (r+1)*BN/2) of the B tile in its own shared
+// memory; CTA 0's MMA thread issues M = 256 MMAs that read both CTAs' halves
+// and accumulate rows 128r.. into CTA r's TMEM.  Each CTA stages half as many
+// B bytes per MMA as the single-CTA kernel, which halves the L2-to-SM traffic
+// for B and leaves room for deeper pipelines.  Barriers:
+//   full[s]     CTA 0 only: CTA 0's expect_tx (both halves) + both CTAs' TMA
+//   empty[s]    both CTAs: the MMA commit arrives on both (multicast commit)
+//   acc_full[a] both CTAs: MMA commit multicast at the end of a pass
+//   acc_empty[a] CTA 0: one arrival from each epilogue warp of both CTAs
+// TMA loads carry no multicast; every wait is bounded.
+template <int BN>
+__host__ __device__ constexpr int pair_stages() { return BN == 256 ? 6 : 8; }
+
+struct TcPairBarriers {
+  uint64_t full[8];
+  uint64_t empty[8];
+  uint64_t acc_full[2];
+  uint64_t acc_empty[2];
+  uint32_t tmem_base;
+};
+
+template <int BN>
+__host__ __device__ constexpr size_t tc2_smem_bytes() {
+  return 1024 + (size_t)pair_stages<BN>() * (128 * 128 + (BN / 2) * 128) + sizeof(TcPairBarriers) + 64;
+}
+
+template <int BN, bool I8, int EPI>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
+    tc_gemm2_kernel(const __grid_constant__ TcGemmParams P) {
+  using namespace sm100;
+  constexpr int ST = pair_stages<BN>();
+  constexpr uint32_t kA = 128 * 128, kB = (BN / 2) * 128;
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* smA = base;                          // [ST][128 rows][128 B]
+  unsigned char* smB = base + (size_t)ST * kA;        // [ST][BN/2 rows][128 B]
+  TcPairBarriers* bars = (TcPairBarriers*)(smB + (size_t)ST * kB);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = (int)(blockIdx.x >> 1), npairs = (int)(gridDim.x >> 1);
+  const int ntile_total = P.mtiles * P.ntiles;  // mtiles counts 256-row tiles here
+  const int nprod = P.pass_first[P.npass];
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) { mbar_init(&bars->full[s], 1); mbar_init(&bars->empty[s], 1); }
+    for (int a = 0; a < 2; ++a) { mbar_init(&bars->acc_full[a], 1); mbar_init(&bars->acc_empty[a], 8); }
+    fence_barrier_init();
+    prefetch_tmap(&P.tmA);
+    prefetch_tmap(&P.tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc2(&bars->tmem_base, 2 * BN);
+    tmem_relinquish2();
+  }
+  tc_fence_before();
+  cluster_sync();  // both CTAs' barriers initialised, TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem = bars->tmem_base;
+  bool ok = true;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      const uint32_t full0 = mapa_shared(smem_u32(&bars->full[0]), 0);  // CTA 0's full barriers
+      uint32_t it = 0;
+      for (int t = pair; t < ntile_total && ok; t += npairs) {
+        const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
+        for (int q = 0; q < nprod && ok; ++q) {
+          for (int kb = P.prod_kb0[q]; kb < P.prod_kb1[q]; ++kb, ++it) {
+            const int s = (int)(it % ST);
+            const uint32_t ph = (it / ST) & 1;
+            if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err))) break;
+            if (rank == 0) mbar_expect_tx(&bars->full[s], 2 * (kA + kB));
+            const uint32_t fb = full0 + (uint32_t)(s * sizeof(uint64_t));
+            tma_load_3d_pair(smA + (size_t)s * kA, &P.tmA, kb * (I8 ? 128 : 64), mb * 256 + (int)rank * 128,
+                             P.prod_a[q], fb);
+            tma_load_3d_pair(smB + (size_t)s * kB, &P.tmB, kb * (I8 ? 128 : 64), nb * BN + (int)rank * (BN / 2),
+                             P.prod_b[q], fb);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (CTA 0 only) ----------------
+    if (rank == 0 && lane == 0) {
+      constexpr uint32_t kIdesc = idesc(I8, BN, 256);
+      uint32_t it = 0, acc_it = 0;
+      for (int t = pair; t < ntile_total && ok; t += npairs) {
+        for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
+          const int a = acc_it & 1;
+          const uint32_t aph = (acc_it >> 1) & 1;
+          if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err))) break;
+          tc_fence_after();
+          const uint32_t dcol = tmem + (uint32_t)(a * BN);
+          bool first = true;
+          for (int q = P.pass_first[p]; q < P.pass_first[p + 1] && ok; ++q) {
+            for (int kb = P.prod_kb0[q]; kb < P.prod_kb1[q]; ++kb, ++it) {
+              const int s = (int)(it % ST);
+              const uint32_t ph = (it / ST) & 1;
+              if (!(ok = mbar_wait(&bars->full[s], ph, P.err))) break;
+              tc_fence_after();
+              const uint32_t sa = smem_u32(smA + (size_t)s * kA);
+              const uint32_t sb = smem_u32(smB + (size_t)s * kB);
+#pragma unroll
+              for (int kk = 0; kk < 4; ++kk) {
+                mma2<I8>(dcol, sdesc_k128(sa + kk * 32), sdesc_k128(sb + kk * 32), kIdesc,
+                         (first && kk == 0) ? 0u : 1u);
+              }
+              first = false;
+              mma_commit2_both(&bars->empty[s]);
+            }
+          }
+          mma_commit2_both(&bars->acc_full[a]);
+        }
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5 of both CTAs) ----------------
+    const int quad = warp & 3;
+    const uint32_t acc_empty0 = mapa_shared(smem_u32(&bars->acc_empty[0]), 0);
+    uint32_t acc_it = 0;
+    for (int t = pair; t < ntile_total && ok; t += npairs) {
+      const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
+      const int m = mb * 256 + (int)rank * 128 + quad * 32 + lane;
+      const bool mval = m < P.M;
+      const int64_t dmo = mval ? P.dm[m] : 0;
+      const int re = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) && mval ? P.rowexp[m] : 0;
+      for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
+        const int a = acc_it & 1;
+        const uint32_t aph = (acc_it >> 1) & 1;
+        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err))) break;
+        tc_fence_after();
+        const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) ? P.pass_shift[p] : 0;
+        epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, nb,
+                               p == 0, shift);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(acc_empty0 + (uint32_t)(a * sizeof(uint64_t)));
+      }
+    }
+  }
+  __syncthreads();
+  tc_fence_before();
+  cluster_sync();  // neither CTA touches the other's barriers or TMEM after this
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc2(tmem, 2 * BN);
 }
 
 }  // namespace tb

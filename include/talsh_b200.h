@@ -45,7 +45,8 @@ typedef struct {
   int slices;      /* INT8 slices per FP64 operand for R8/C8 fused (0 = default) */
   int tile_n;      /* tensor-core N tile: 0 (default), 128 or 256 */
   int bf16_terms;  /* split-BF16 products for R4/C4 fused: 0 (default = 3) */
-  int reserved[4];
+  int tile_m;      /* tensor-core M tile: 0 (default), 128 (one SM) or 256 (an SM pair) */
+  int reserved[3];
 } tb_plan_t;
 
 /* Last error message of the calling thread ("" if none). */

@@ -118,3 +118,26 @@ def test_long_k_splits_exact_int32_passes(xt, dev):
     assert st.method == XB.METHOD_FUSED and st.products == 21 and st.passes > 6
     want = float(Fraction(v) ** 2 * K / 2)
     assert np.allclose(got, want, rtol=1e-13, atol=0), (got[:4], want)
+
+
+@pytest.mark.parametrize("dtk", [O.R8, O.C8, O.R4, O.C4])
+def test_sm_pair_and_single_sm_tiles_agree(xt, dev, dtk):
+    """The CTA-pair kernel (256-row tiles over two SMs) and the single-SM
+    kernel (128-row tiles) compute the same sums; for the INT8 slices every
+    partial sum is exact, so R8/C8 results agree bit for bit."""
+    pattern, ext = "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)", {"a": 24, "b": 20, "c": 16, "d": 12, "i": 10, "j": 9}
+    errs, outs = [], []
+    for tm in (128, 256):
+        err, st = fused(xt, dev, pattern, ext, dtk, alpha=0.5, plan=xt.make_plan(XB.METHOD_FUSED, tile_m=tm), seed=5)
+        errs.append(err)
+    assert max(errs) <= TOL[dtk], errs
+    if dtk in (O.R8, O.C8):
+        ddims, ldims, rdims = shapes(pattern, ext)
+        vol = lambda s: int(np.prod(s))
+        d, l, r = rand_host(dtk, vol(ddims), 5), rand_host(dtk, vol(ldims), 6), rand_host(dtk, vol(rdims), 7)
+        for tm in (128, 256):
+            dd, ld, rd = dev.put(d), dev.put(l), dev.put(r)
+            xt.tensor_contract(pattern, dtk, ddims, dd.data_ptr(), ldims, ld.data_ptr(), rdims, rd.data_ptr(), 0.5,
+                               plan=xt.make_plan(XB.METHOD_FUSED, tile_m=tm), stream=dev.stream())
+            outs.append(dev.get(dd, d.dtype, d.size))
+        assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8))
