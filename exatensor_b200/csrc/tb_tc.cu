@@ -129,7 +129,7 @@ constexpr int kMaxSlicesDev = 7;
 template <typename E> constexpr int gather_rows() { return sizeof(E) == 16 ? 32 : 64; }  // 32-34 KB tiles
 constexpr int kGK = 64;
 
-enum GatherMode { G_EXP_R8, G_EXP_C8, G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A, G_SPLIT_C4B };
+enum GatherMode { G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A, G_SPLIT_C4B };
 
 struct GatherParams {
   const void* src;
@@ -167,56 +167,49 @@ __device__ __forceinline__ uint32_t slice4(long long y0, long long y1, long long
 
 template <int MODE>
 __global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant__ GatherParams P) {
-  constexpr bool CPLX = MODE == G_EXP_C8 || MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A ||
-                        MODE == G_SPLIT_C4B;
+  constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
   constexpr bool F32 = MODE == G_SPLIT_R4 || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
-  constexpr bool EXP = MODE == G_EXP_R8 || MODE == G_EXP_C8;
   using R = typename std::conditional<F32, float, double>::type;
   using E = typename std::conditional<CPLX, typename std::conditional<F32, float2, double2>::type, R>::type;
   constexpr int TM = gather_rows<E>(), TK = kGK;
   __shared__ E tile[TM][TK + 1];
   __shared__ int64_t sm_lm[TM], sm_lk[TK];
-  __shared__ unsigned sm_max[TM];
   __shared__ int sm_se[TM];  // slice modes: the row's scale exponent
   const int64_t m0 = (int64_t)blockIdx.x * TM;
   const int tid = threadIdx.x;
   if (tid < TM) {
     sm_lm[tid] = (m0 + tid < P.rows) ? P.lm[m0 + tid] : -1;
-    sm_max[tid] = 0;
-    if constexpr (!EXP && !F32) sm_se[tid] = 1021 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1021u);
+    if constexpr (!F32) sm_se[tid] = 1021 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1021u);
   }
   const E* src = (const E*)P.src;
-  const int64_t nkt = (P.K + TK - 1) / TK;                   // tiles with data
-  const int64_t ntiles = EXP ? nkt : (P.kpad / (CPLX ? 2 : 1)) / TK;  // conversion also writes the padding
+  const int64_t ntiles = (P.kpad / (CPLX ? 2 : 1)) / TK;  // conversion also writes the padding
   for (int64_t kt = blockIdx.y; kt < ntiles; kt += gridDim.y) {
     const int64_t k0 = kt * TK;
     __syncthreads();  // previous tile consumed
     if (tid < TK) sm_lk[tid] = (k0 + tid < P.K) ? P.lk[k0 + tid] : -1;
     __syncthreads();
-#pragma unroll 4
-    for (int idx = tid; idx < TM * TK; idx += kGThreads) {
-      const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-      E v;
-      if constexpr (CPLX) { v.x = 0; v.y = 0; } else { v = 0; }
-      if (sm_lm[mm] >= 0 && sm_lk[kk] >= 0) v = src[sm_lm[mm] + sm_lk[kk]];
-      tile[mm][kk] = v;
-    }
-    __syncthreads();
-    if constexpr (EXP) {
-      // row maxima of the exponent field: TPR threads per row
-      constexpr int TPR = kGThreads / TM;
-      const int mm = tid / TPR, part = tid % TPR;
-      unsigned e = 0;
-      for (int kk = part; kk < TK; kk += TPR) {
-        const E v = tile[mm][kk];
-        if constexpr (CPLX) e = max(e, max(exp_field(v.x), exp_field(v.y)));
-        else e = max(e, exp_field(v));
+    {
+      // all loads of the tile first (independent, so they overlap), then the stores
+      constexpr int IT = TM * TK / kGThreads;
+      E v[IT];
+#pragma unroll
+      for (int it = 0; it < IT; ++it) {
+        const int idx = tid + it * kGThreads;
+        const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+        const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+        if constexpr (CPLX) { v[it].x = 0; v[it].y = 0; } else { v[it] = 0; }
+        if (sm_lm[mm] >= 0 && sm_lk[kk] >= 0) v[it] = src[sm_lm[mm] + sm_lk[kk]];
       }
 #pragma unroll
-      for (int w = 1; w < TPR; w <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, w));
-      if (part == 0 && e > sm_max[mm]) sm_max[mm] = e;  // one writer per row
-    } else {
+      for (int it = 0; it < IT; ++it) {
+        const int idx = tid + it * kGThreads;
+        const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+        const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+        tile[mm][kk] = v[it];
+      }
+    }
+    __syncthreads();
+    {
       // convert: thread -> (row mm, 4 consecutive k)
       for (int idx = tid; idx < TM * (TK / 4); idx += kGThreads) {
         const int mm = idx / (TK / 4), kq = (idx % (TK / 4)) * 4;
@@ -310,10 +303,6 @@ __global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant
       }
     }
   }
-  if constexpr (EXP) {
-    __syncthreads();
-    if (tid < TM && sm_max[tid] && m0 + tid < P.rows) atomicMax(&P.rowE[m0 + tid], sm_max[tid]);
-  }
 }
 
 // exponents: rowexp[r] = rowE[r / rep] - 1021 (rep = 2 for complex B' rows)
@@ -336,6 +325,64 @@ struct Operand {
   std::vector<MGroup> ks;     // contracted groups: s1 = stride in this tensor
   bool conj;
 };
+
+// Row maxima of the FP64 exponent fields (the slice scales), streamed without
+// shared-memory staging: each thread keeps the running maximum of the rows it
+// touches in registers over all K tiles of its CTA, and the CTA merges them once
+// at the end.  Thread -> (row, k) mapping as in gather_kernel.
+template <bool CPLX>
+__global__ void __launch_bounds__(kGThreads) rowmax_kernel(const __grid_constant__ GatherParams P) {
+  using E = typename std::conditional<CPLX, double2, double>::type;
+  constexpr int TM = gather_rows<E>(), TK = kGK, IT = TM * TK / kGThreads;
+  __shared__ unsigned sm_max[TM];
+  const int tid = threadIdx.x;
+  if (tid < TM) sm_max[tid] = 0;
+  const int64_t m0 = (int64_t)blockIdx.x * TM;
+  int64_t lmv[IT];
+  unsigned emax[IT];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * kGThreads;
+    const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+    lmv[it] = m0 + mm < P.rows ? P.lm[m0 + mm] : -1;
+    emax[it] = 0;
+  }
+  const E* src = (const E*)P.src;
+  const int64_t nkt = (P.K + TK - 1) / TK;
+  for (int64_t kt = blockIdx.y; kt < nkt; kt += gridDim.y) {
+    const int64_t k0 = kt * TK;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int idx = tid + it * kGThreads;
+      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+      if (lmv[it] >= 0 && k0 + kk < P.K) {
+        const E v = src[lmv[it] + P.lk[k0 + kk]];
+        if constexpr (CPLX) emax[it] = max(emax[it], max(exp_field(v.x), exp_field(v.y)));
+        else emax[it] = max(emax[it], exp_field(v));
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * kGThreads;
+    const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+    if (emax[it]) atomicMax(&sm_max[mm], emax[it]);
+  }
+  __syncthreads();
+  if (tid < TM && sm_max[tid] && m0 + tid < P.rows) atomicMax(&P.rowE[m0 + tid], sm_max[tid]);
+}
+
+template <bool CPLX>
+int run_rowmax(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStream_t s) {
+  if (grid_rows <= 0 || grid_k <= 0) return 0;
+  if (grid_rows > INT32_MAX) { set_error("gather grid too large"); return TB_ERR_LIMIT; }
+  int64_t gy = std::max<int64_t>(1, std::min<int64_t>(grid_k, (int64_t)num_sms() * 16 / std::max<int64_t>(1, grid_rows)));
+  gy = std::min<int64_t>(gy, 65535);
+  rowmax_kernel<CPLX><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+  TB_CHECK_LAUNCH();
+  return 0;
+}
 
 template <int MODE>
 int run_gather(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStream_t s) {
@@ -556,11 +603,11 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       if (cudaMemsetAsync(rowE, 0, offRX - offRE, s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
       const int64_t eA = (M + tmr - 1) / tmr, eB = (Nc + tmr - 1) / tmr, ek = (K + kGK - 1) / kGK;
       if (!cplx) {
-        if ((err = run_gather<G_EXP_R8>(GA, eA, ek, s))) break;
-        if ((err = run_gather<G_EXP_R8>(GB, eB, ek, s))) break;
+        if ((err = run_rowmax<false>(GA, eA, ek, s))) break;
+        if ((err = run_rowmax<false>(GB, eB, ek, s))) break;
       } else {
-        if ((err = run_gather<G_EXP_C8>(GA, eA, ek, s))) break;
-        if ((err = run_gather<G_EXP_C8>(GB, eB, ek, s))) break;
+        if ((err = run_rowmax<true>(GA, eA, ek, s))) break;
+        if ((err = run_rowmax<true>(GB, eB, ek, s))) break;
       }
       exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 4096)), 256, 0, s>>>(rowE, rowx, M, 1);
       exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((Nr + 255) / 256, 4096)), 256, 0, s>>>(colE, colx, Nr,
