@@ -37,6 +37,9 @@ WORKLOADS = {
     "ccsd1_r4": dict(pattern="D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)", v=192, o=48, dtk=4),
 }
 VIRT = set("abcd")
+# dram__bytes_read.sum + dram__bytes_write.sum of tc_gemm_kernel on the v=96 case
+# (4.90 GB + 0.96 GB) times the 16x larger work of v=192 with the same tile shape
+TC_GEMM_TRAFFIC = 16 * (4.902736e9 + 0.963089e9)
 
 
 def shapes(pattern, v, o):
@@ -400,8 +403,10 @@ def run_ours(args):
         achieved = hw_ops / (per_launch_ms / 1e3) / 1e12 if gemm_n else None
         roofline = {"bound": "tensor", "kernel": kern, "achieved": round(achieved, 2) if achieved else None,
                     "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 3) if achieved else None,
-                    "traffic": None, "peak_source": peak_note, "launch_ms": round(per_launch_ms, 3),
-                    "launches_timed": gemm_n}
+                    "traffic": TC_GEMM_TRAFFIC if (chosen_method == "fused" and args.workload == "ccsd1_r8") else None,
+                    "traffic_note": "DRAM read+write bytes per launch: ncu capture of the v=96 case "
+                                    "(profiles/tc_gemm_kernel_ccsd1_v96.md) scaled by the 16x work of v=192",
+                    "peak_source": peak_note, "launch_ms": round(per_launch_ms, 3), "launches_timed": gemm_n}
         e2e = e2e_talsh(X, wl, steps=max(1, min(2, args.steps)))
         cpu = cpu_contraction_sample(steps=1) if world == 1 else None
         line = {
@@ -427,6 +432,46 @@ def run_ours(args):
         print(json.dumps(line))
 
 
+def run_profile(args):
+    """A small, single-part run for profilers: --profile contract|plain runs the
+    chosen / plain contraction of the workload (extents overridable with --v and
+    --o), --profile permute runs the 24 rank-4 permutations of an n^4 R8 tensor
+    (n = --v).  Prints one summary line; not a bench result."""
+    import itertools
+
+    import torch
+
+    import exatensor_b200 as X
+    torch.cuda.set_device(0)
+    X.device_init(0)
+    s_obj = torch.cuda.current_stream()
+    s = s_obj.cuda_stream
+    if args.profile == "permute":
+        n = args.v or 76
+        v = n ** 4
+        a = torch.empty(v * 8, dtype=torch.uint8, device="cuda")
+        b = torch.empty_like(a)
+        X.fill_uniform(8, v, a.data_ptr(), 3, stream=s)
+        perms = list(itertools.permutations([1, 2, 3, 4]))
+        ms = time_steps(lambda: [X.tensor_copy(8, [n] * 4, p, a.data_ptr(), b.data_ptr(), 0, s) for p in perms],
+                        args.steps, args.warmup, 1, s_obj)
+        print(json.dumps({"profile": "permute", "n": n, "GB/s": round(2.0 * v * 8 * len(perms) * args.steps
+                                                                       / (ms / 1e3) / 1e9, 1)}))
+        return
+    wl = dict(WORKLOADS[args.workload])
+    wl["v"] = args.v or wl["v"]
+    wl["o"] = args.o or wl["o"]
+    case = ContractionCase(X, wl, s)
+    method = X.METHOD_AUTO if args.profile == "contract" else X.METHOD_TTGT
+    ms = time_steps(lambda: case.run(method), args.steps, args.warmup, 1, s_obj)
+    X.device_check(s)
+    st = X.last_contract_stats()
+    print(json.dumps({"profile": args.profile, "workload": args.workload, "v": wl["v"], "o": wl["o"],
+                      "method": st.method, "slices": st.slices, "products": st.products,
+                      "ms_per_step": round(ms / args.steps, 3),
+                      "TFLOP/s": round(case.flops * args.steps / (ms / 1e3) / 1e12, 3)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -434,8 +479,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
+    ap.add_argument("--profile", choices=["contract", "plain", "permute"], default=None,
+                    help="run one part on a small case for a profiler (no bench line)")
+    ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n)")
+    ap.add_argument("--o", type=int, default=0, help="--profile: occupied extent")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
