@@ -405,7 +405,7 @@ def run_ours(args):
                     "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 3) if achieved else None,
                     "traffic": TC_GEMM_TRAFFIC if (chosen_method == "fused" and args.workload == "ccsd1_r8") else None,
                     "traffic_note": "DRAM read+write bytes per launch: ncu capture of the v=96 case "
-                                    "(profiles/tc_gemm_kernel_ccsd1_v96.md) scaled by the 16x work of v=192",
+                                    "scaled by the 16x work of v=192",
                     "peak_source": peak_note, "launch_ms": round(per_launch_ms, 3), "launches_timed": gemm_n}
         e2e = e2e_talsh(X, wl, steps=max(1, min(2, args.steps)))
         cpu = cpu_contraction_sample(steps=1) if world == 1 else None
