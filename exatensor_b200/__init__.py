@@ -46,6 +46,18 @@ class ContractStats(C.Structure):
                 ("products", C.c_int)]
 
 
+class BlockTask(C.Structure):
+    """tb_block_task_t: one block contraction of a block-sparse list."""
+    _fields_ = [("d", C.c_void_p), ("l", C.c_void_p), ("r", C.c_void_p), ("d_dims", C.c_int * 8),
+                ("l_dims", C.c_int * 8), ("r_dims", C.c_int * 8)]
+
+
+class BscInfo(C.Structure):
+    _fields_ = [("tasks", C.c_int), ("left_blocks", C.c_int), ("right_blocks", C.c_int), ("out_blocks", C.c_int),
+                ("work_items", C.c_int), ("slices", C.c_int), ("tile_n", C.c_int), ("flops", C.c_double),
+                ("tune_ms", C.c_float * 4)]
+
+
 def lib() -> C.CDLL:
     """Loads libtalsh_b200.so (raises if it has not been built)."""
     global _lib
@@ -75,6 +87,13 @@ def lib() -> C.CDLL:
                                          C.c_double, C.c_double, C.c_int, C.POINTER(Plan), vp]
     L.tb_tensor_contract_noalloc.argtypes = [ip, C.c_int, C.c_int, ip, vp, C.c_int, ip, vp, C.c_int, ip, vp,
                                              C.c_double, C.c_double, C.c_int, C.c_int, vp]
+    L.tb_bsc_plan_create.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(BlockTask), C.c_double, C.c_double,
+                                     C.c_int, C.POINTER(Plan), C.POINTER(C.c_void_p), vp]
+    L.tb_bsc_execute.argtypes = [vp, vp]
+    L.tb_bsc_execute_stream.argtypes = [vp, vp]
+    L.tb_bsc_autotune.argtypes = [vp, vp]
+    L.tb_bsc_plan_info.argtypes = [vp, C.POINTER(BscInfo)]
+    L.tb_bsc_plan_destroy.argtypes = [vp]
     L.tb_fill_uniform.argtypes = [C.c_int, C.c_size_t, vp, C.c_uint64, C.c_double, C.c_double, vp]
     L.tb_last_contract_stats.argtypes = [C.POINTER(ContractStats)]
     _lib = L
@@ -169,6 +188,53 @@ def tensor_contract(pattern_or_cptrn, dtk, ddims, d_ptr, ldims, l_ptr, rdims, r_
                                         len(ldims), iarr(ldims), C.c_void_p(l_ptr), len(rdims), iarr(rdims),
                                         C.c_void_p(r_ptr), a.real, a.imag, conj_bits, int(accumulative), pp,
                                         _stream(stream)))
+
+
+class BlockSparsePlan:
+    """A block-sparse contraction (list of block tasks under one pattern) run as
+    one grouped tensor-core launch; see tb_bsc_plan_create.
+
+    tasks: iterable of (d_ptr, d_dims, l_ptr, l_dims, r_ptr, r_dims)."""
+
+    def __init__(self, pattern, dtk, tasks, alpha=1.0, accumulative=True, plan: Plan | None = None, stream=None):
+        tasks = list(tasks)
+        arr = (BlockTask * len(tasks))()
+        for t, (dp, dd, lp, ld, rp, rd) in zip(arr, tasks):
+            t.d, t.l, t.r = dp, lp, rp
+            for k, v in enumerate(dd):
+                t.d_dims[k] = v
+            for k, v in enumerate(ld):
+                t.l_dims[k] = v
+            for k, v in enumerate(rd):
+                t.r_dims[k] = v
+        a = complex(alpha)
+        h = C.c_void_p()
+        _check(lib().tb_bsc_plan_create(pattern.encode(), dtk, len(tasks), arr, a.real, a.imag, int(accumulative),
+                                        C.byref(plan) if plan is not None else None, C.byref(h), _stream(stream)))
+        self._h = h
+
+    def execute(self, stream=None, graph=True):
+        f = lib().tb_bsc_execute if graph else lib().tb_bsc_execute_stream
+        _check(f(self._h, _stream(stream)))
+
+    def autotune(self, stream=None):
+        _check(lib().tb_bsc_autotune(self._h, _stream(stream)))
+
+    def info(self) -> BscInfo:
+        inf = BscInfo()
+        _check(lib().tb_bsc_plan_info(self._h, C.byref(inf)))
+        return inf
+
+    def close(self):
+        if self._h:
+            lib().tb_bsc_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 NOALLOC_ARENA_BYTES = 64 << 20  # TB_NOALLOC_ARENA_BYTES

@@ -32,284 +32,11 @@
 #include "tb_contract.h"
 #include "tb_permute.cuh"
 #include "tb_tc_gemm.cuh"
+#include "tb_tc_prep.cuh"
 
 namespace tb {
 
 namespace {
-
-// ---- TMA tensor maps (driver entry point, no libcuda link) --------------------
-PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  });
-  return fn;
-}
-
-// 3-D map over planes of [rows][kpad] K-major operands, 128-byte rows per box.
-int make_operand_map(CUtensorMap* map, const void* base, bool i8, int64_t kpad, int64_t rows, int planes,
-                     int box_rows) {
-  auto enc = get_encode();
-  if (!enc) { set_error("cuTensorMapEncodeTiled is unavailable"); return TB_ERR_CUDA; }
-  const int es = i8 ? 1 : 2;
-  cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)planes};
-  cuuint64_t strides[2] = {(cuuint64_t)(kpad * es), (cuuint64_t)(kpad * es * rows)};
-  cuuint32_t box[3] = {(cuuint32_t)(128 / es), (cuuint32_t)box_rows, 1};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = enc(map, i8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
-                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed (%d)", (int)r); return TB_ERR_CUDA; }
-  return 0;
-}
-
-// ---- offset tables: out[i] = sum_g digit_g(i) * stride_g (first group fastest) --
-struct OffsetParams {
-  int ng;
-  int64_t count;
-  int64_t ext[kMaxRank];
-  FastDiv div[kMaxRank];
-  int64_t stride[kMaxRank];
-};
-
-__global__ void offsets_kernel(const __grid_constant__ OffsetParams P, int64_t* __restrict__ out) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.count; i += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t r = (uint64_t)i;
-    int64_t o = 0;
-    for (int g = 0; g < P.ng; ++g) {
-      const uint64_t q = P.div[g].div(r);
-      o += (int64_t)(r - q * (uint64_t)P.ext[g]) * P.stride[g];
-      r = q;
-    }
-    out[i] = o;
-  }
-}
-
-int build_offsets(const std::vector<MGroup>& groups, bool use_s2, int64_t* out, cudaStream_t s) {
-  OffsetParams P;
-  std::memset(&P, 0, sizeof(P));
-  P.ng = (int)groups.size();
-  P.count = 1;
-  for (int g = 0; g < P.ng; ++g) {
-    P.ext[g] = groups[g].ext;
-    P.div[g].init((uint64_t)groups[g].ext);
-    P.stride[g] = use_s2 ? groups[g].s2 : groups[g].s1;
-    P.count *= groups[g].ext;
-  }
-  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((P.count + 255) / 256, num_sms() * 8));
-  offsets_kernel<<<(unsigned)blocks, 256, 0, s>>>(P, out);
-  TB_CHECK_LAUNCH();
-  return 0;
-}
-
-// ---- operand conversion helpers --------------------------------------------------
-__device__ __forceinline__ unsigned exp_field(double x) {
-  return (unsigned)((__double_as_longlong(x) >> 52) & 0x7FF);
-}
-
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(x);
-  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-}
-
-// ---- operand gather: 64 x 64 tiles through source offset tables ----------------
-// Element (m, k) of a matricized operand lives at src[lm[m] + lk[k]].  A tile
-// is read with lanes along whichever index is contiguous in the source, staged
-// in shared memory, and converted with lanes along k so that every thread
-// writes 4 consecutive K positions of each output plane in one store.
-// Tiles cover [0, rows_pad) x [0, kpad_src): padding is written as zeros.
-constexpr int kGThreads = 256;
-constexpr int kMaxSlicesDev = 7;
-template <typename E> constexpr int gather_rows() { return sizeof(E) == 16 ? 32 : 64; }  // 32-34 KB tiles
-constexpr int kGK = 64;
-
-enum GatherMode { G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A, G_SPLIT_C4B };
-
-struct GatherParams {
-  const void* src;
-  const int64_t* lm;   // source offset of row m (m < rows)
-  const int64_t* lk;   // source offset of contracted index k (k < K)
-  int64_t rows, K;     // valid extents
-  int64_t kpad;        // real row length of the output planes (elements)
-  int64_t pstride;     // elements per plane
-  void* planes;
-  unsigned* rowE;      // exponent fields (exp modes write, slice modes read)
-  int slices;
-  int lanes_on_k;      // 1: consecutive k are contiguous in the source
-  double isign;        // -1 conjugates the imaginary part
-};
-
-// Slices of x in (-1/2, 1/2): balanced signed base-256 digits of the fixed-point
-// value X = floor(x * 2^55) = sum_i d_i 2^(48-8i), d_i in [-128, 127] for
-// i >= 1 and |d_0| <= 64.  With Y = X + 0x808080808080 the low bytes of Y are
-// d_i + 128 and Y >> 48 = d_0, so each slice is one byte of Y (bit 7 flipped
-// for i >= 1).  Digit i has weight 2^-(8i+7); the digits are centred on zero,
-// so the parts dropped by keeping s slices or slice pairs do not accumulate a
-// bias over K.  The scaling by 2^55 is exact and the conversion rounds toward
-// minus infinity.
-__device__ __forceinline__ long long fixed55(double x) {
-  return __double2ll_rd(x * 36028797018963968.0) + 0x808080808080ll;  // 2^55; Y
-}
-// Slice i of four consecutive values, packed little-endian into one word.
-__device__ __forceinline__ uint32_t slice4(long long y0, long long y1, long long y2, long long y3, int i) {
-  const int sh = 48 - 8 * i;
-  const uint32_t flip = i == 0 ? 0u : 0x80808080u;
-  return ((uint32_t)((y0 >> sh) & 255) | ((uint32_t)((y1 >> sh) & 255) << 8) |
-          ((uint32_t)((y2 >> sh) & 255) << 16) | ((uint32_t)((y3 >> sh) & 255) << 24)) ^
-         flip;
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant__ GatherParams P) {
-  constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
-  constexpr bool F32 = MODE == G_SPLIT_R4 || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
-  using R = typename std::conditional<F32, float, double>::type;
-  using E = typename std::conditional<CPLX, typename std::conditional<F32, float2, double2>::type, R>::type;
-  constexpr int TM = gather_rows<E>(), TK = kGK;
-  __shared__ E tile[TM][TK + 1];
-  __shared__ int64_t sm_lm[TM], sm_lk[TK];
-  __shared__ int sm_se[TM];  // slice modes: the row's scale exponent
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  const int tid = threadIdx.x;
-  if (tid < TM) {
-    sm_lm[tid] = (m0 + tid < P.rows) ? P.lm[m0 + tid] : -1;
-    if constexpr (!F32) sm_se[tid] = 1021 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1021u);
-  }
-  const E* src = (const E*)P.src;
-  const int64_t ntiles = (P.kpad / (CPLX ? 2 : 1)) / TK;  // conversion also writes the padding
-  for (int64_t kt = blockIdx.y; kt < ntiles; kt += gridDim.y) {
-    const int64_t k0 = kt * TK;
-    __syncthreads();  // previous tile consumed
-    if (tid < TK) sm_lk[tid] = (k0 + tid < P.K) ? P.lk[k0 + tid] : -1;
-    __syncthreads();
-    {
-      // all loads of the tile first (independent, so they overlap), then the stores
-      constexpr int IT = TM * TK / kGThreads;
-      E v[IT];
-#pragma unroll
-      for (int it = 0; it < IT; ++it) {
-        const int idx = tid + it * kGThreads;
-        const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-        const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-        if constexpr (CPLX) { v[it].x = 0; v[it].y = 0; } else { v[it] = 0; }
-        if (sm_lm[mm] >= 0 && sm_lk[kk] >= 0) v[it] = src[sm_lm[mm] + sm_lk[kk]];
-      }
-#pragma unroll
-      for (int it = 0; it < IT; ++it) {
-        const int idx = tid + it * kGThreads;
-        const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-        const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-        tile[mm][kk] = v[it];
-      }
-    }
-    __syncthreads();
-    {
-      // convert: thread -> (row mm, 4 consecutive k)
-      for (int idx = tid; idx < TM * (TK / 4); idx += kGThreads) {
-        const int mm = idx / (TK / 4), kq = (idx % (TK / 4)) * 4;
-        const int64_t m = m0 + mm, k = k0 + kq;
-        if constexpr (MODE == G_SLICE_R8) {
-          const int se = sm_se[mm];
-          long long X[4];
-#pragma unroll
-          for (int t = 0; t < 4; ++t) X[t] = fixed55(scale2(tile[mm][kq + t], se));
-          int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
-#pragma unroll
-          for (int i = 0; i < kMaxSlicesDev; ++i)
-            if (i < P.slices) *reinterpret_cast<uint32_t*>(base + i * P.pstride) = slice4(X[0], X[1], X[2], X[3], i);
-        } else if constexpr (MODE == G_SLICE_C8A) {
-          // A' row m: (re, im) interleaved along K
-          const int se = sm_se[mm];
-          long long R[4], I[4];
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
-            R[t] = fixed55(scale2(v.x, se));
-            I[t] = fixed55(scale2(P.isign * v.y, se));
-          }
-          int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
-#pragma unroll
-          for (int i = 0; i < kMaxSlicesDev; ++i)
-            if (i < P.slices) {
-              uint2 w = make_uint2(slice4(R[0], I[0], R[1], I[1], i), slice4(R[2], I[2], R[3], I[3], i));
-              *reinterpret_cast<uint2*>(base + i * P.pstride) = w;
-            }
-        } else if constexpr (MODE == G_SLICE_C8B) {
-          // B' rows 2n = (re, -im), 2n+1 = (im, re) interleaved along K
-          const int se = sm_se[mm];
-          long long R[4], I[4], NI[4];
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
-            const double im = scale2(P.isign * v.y, se);
-            R[t] = fixed55(scale2(v.x, se));
-            I[t] = fixed55(im);
-            NI[t] = fixed55(-im);
-          }
-          int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
-          int8_t* b1 = b0 + P.kpad;
-#pragma unroll
-          for (int i = 0; i < kMaxSlicesDev; ++i)
-            if (i < P.slices) {
-              *reinterpret_cast<uint2*>(b0 + i * P.pstride) =
-                  make_uint2(slice4(R[0], NI[0], R[1], NI[1], i), slice4(R[2], NI[2], R[3], NI[3], i));
-              *reinterpret_cast<uint2*>(b1 + i * P.pstride) =
-                  make_uint2(slice4(I[0], R[0], I[1], R[1], i), slice4(I[2], R[2], I[3], R[3], i));
-            }
-        } else if constexpr (MODE == G_SPLIT_R4) {
-          __nv_bfloat16 h[4], l[4];
-#pragma unroll
-          for (int t = 0; t < 4; ++t) split_bf16(tile[mm][kq + t], h[t], l[t]);
-          __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + k;
-          __nv_bfloat162 hh[2] = {{h[0], h[1]}, {h[2], h[3]}}, ll[2] = {{l[0], l[1]}, {l[2], l[3]}};
-          *reinterpret_cast<uint2*>(base) = *reinterpret_cast<uint2*>(hh);
-          *reinterpret_cast<uint2*>(base + P.pstride) = *reinterpret_cast<uint2*>(ll);
-        } else {
-          // complex FP32: A' rows (re, im); B' rows 2n (re, -im), 2n+1 (im, re)
-          __nv_bfloat16 hr[4], lr[4], hi[4], li[4], nhi[4], nli[4];
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
-            const float im = (float)P.isign * v.y;
-            split_bf16(v.x, hr[t], lr[t]);
-            split_bf16(im, hi[t], li[t]);
-            split_bf16(-im, nhi[t], nli[t]);
-          }
-          if constexpr (MODE == G_SPLIT_C4A) {
-            __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + 2 * k;
-            __nv_bfloat162 H[4] = {{hr[0], hi[0]}, {hr[1], hi[1]}, {hr[2], hi[2]}, {hr[3], hi[3]}};
-            __nv_bfloat162 L[4] = {{lr[0], li[0]}, {lr[1], li[1]}, {lr[2], li[2]}, {lr[3], li[3]}};
-            *reinterpret_cast<uint4*>(base) = *reinterpret_cast<uint4*>(H);
-            *reinterpret_cast<uint4*>(base + P.pstride) = *reinterpret_cast<uint4*>(L);
-          } else {
-            __nv_bfloat16* b0 = (__nv_bfloat16*)P.planes + (2 * m) * P.kpad + 2 * k;
-            __nv_bfloat16* b1 = b0 + P.kpad;
-            __nv_bfloat162 H0[4] = {{hr[0], nhi[0]}, {hr[1], nhi[1]}, {hr[2], nhi[2]}, {hr[3], nhi[3]}};
-            __nv_bfloat162 L0[4] = {{lr[0], nli[0]}, {lr[1], nli[1]}, {lr[2], nli[2]}, {lr[3], nli[3]}};
-            __nv_bfloat162 H1[4] = {{hi[0], hr[0]}, {hi[1], hr[1]}, {hi[2], hr[2]}, {hi[3], hr[3]}};
-            __nv_bfloat162 L1[4] = {{li[0], lr[0]}, {li[1], lr[1]}, {li[2], lr[2]}, {li[3], lr[3]}};
-            *reinterpret_cast<uint4*>(b0) = *reinterpret_cast<uint4*>(H0);
-            *reinterpret_cast<uint4*>(b0 + P.pstride) = *reinterpret_cast<uint4*>(L0);
-            *reinterpret_cast<uint4*>(b1) = *reinterpret_cast<uint4*>(H1);
-            *reinterpret_cast<uint4*>(b1 + P.pstride) = *reinterpret_cast<uint4*>(L1);
-          }
-        }
-      }
-    }
-  }
-}
-
-// exponents: rowexp[r] = rowE[r / rep] - 1021 (rep = 2 for complex B' rows)
-__global__ void exps_kernel(const unsigned* __restrict__ rowE, int* __restrict__ out, int64_t n, int rep) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int)rowE[i / rep] - 1021;
-}
 
 // ---- driver ----------------------------------------------------------------------
 constexpr int kDefaultSlices = 6;
@@ -325,76 +52,6 @@ struct Operand {
   std::vector<MGroup> ks;     // contracted groups: s1 = stride in this tensor
   bool conj;
 };
-
-// Row maxima of the FP64 exponent fields (the slice scales), streamed without
-// shared-memory staging: each thread keeps the running maximum of the rows it
-// touches in registers over all K tiles of its CTA, and the CTA merges them once
-// at the end.  Thread -> (row, k) mapping as in gather_kernel.
-template <bool CPLX>
-__global__ void __launch_bounds__(kGThreads) rowmax_kernel(const __grid_constant__ GatherParams P) {
-  using E = typename std::conditional<CPLX, double2, double>::type;
-  constexpr int TM = gather_rows<E>(), TK = kGK, IT = TM * TK / kGThreads;
-  __shared__ unsigned sm_max[TM];
-  const int tid = threadIdx.x;
-  if (tid < TM) sm_max[tid] = 0;
-  const int64_t m0 = (int64_t)blockIdx.x * TM;
-  int64_t lmv[IT];
-  unsigned emax[IT];
-#pragma unroll
-  for (int it = 0; it < IT; ++it) {
-    const int idx = tid + it * kGThreads;
-    const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-    lmv[it] = m0 + mm < P.rows ? P.lm[m0 + mm] : -1;
-    emax[it] = 0;
-  }
-  const E* src = (const E*)P.src;
-  const int64_t nkt = (P.K + TK - 1) / TK;
-  for (int64_t kt = blockIdx.y; kt < nkt; kt += gridDim.y) {
-    const int64_t k0 = kt * TK;
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-      const int idx = tid + it * kGThreads;
-      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-      if (lmv[it] >= 0 && k0 + kk < P.K) {
-        const E v = src[lmv[it] + P.lk[k0 + kk]];
-        if constexpr (CPLX) emax[it] = max(emax[it], max(exp_field(v.x), exp_field(v.y)));
-        else emax[it] = max(emax[it], exp_field(v));
-      }
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int it = 0; it < IT; ++it) {
-    const int idx = tid + it * kGThreads;
-    const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-    if (emax[it]) atomicMax(&sm_max[mm], emax[it]);
-  }
-  __syncthreads();
-  if (tid < TM && sm_max[tid] && m0 + tid < P.rows) atomicMax(&P.rowE[m0 + tid], sm_max[tid]);
-}
-
-template <bool CPLX>
-int run_rowmax(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStream_t s) {
-  if (grid_rows <= 0 || grid_k <= 0) return 0;
-  if (grid_rows > INT32_MAX) { set_error("gather grid too large"); return TB_ERR_LIMIT; }
-  int64_t gy = std::max<int64_t>(1, std::min<int64_t>(grid_k, (int64_t)num_sms() * 16 / std::max<int64_t>(1, grid_rows)));
-  gy = std::min<int64_t>(gy, 65535);
-  rowmax_kernel<CPLX><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
-  TB_CHECK_LAUNCH();
-  return 0;
-}
-
-template <int MODE>
-int run_gather(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStream_t s) {
-  if (grid_rows <= 0 || grid_k <= 0) return 0;
-  if (grid_rows > INT32_MAX) { set_error("gather grid too large"); return TB_ERR_LIMIT; }
-  // enough CTAs to fill the GPU several times over; each walks a strided set of K tiles
-  int64_t gy = std::max<int64_t>(1, std::min<int64_t>(grid_k, (int64_t)num_sms() * 16 / std::max<int64_t>(1, grid_rows)));
-  gy = std::min<int64_t>(gy, 65535);
-  gather_kernel<MODE><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
-  TB_CHECK_LAUNCH();
-  return 0;
-}
 
 template <int BN, bool I8, int EPI>
 int launch_tc(const TcGemmParams& P, cudaStream_t s) {

@@ -47,6 +47,15 @@ struct __align__(64) TcGemmParams {
   unsigned int* err;
 };
 
+// Epilogue view of one output block: what epilogue_pass reads besides TMEM.
+struct EpiView {
+  void* D;
+  const int64_t* dn;
+  const int* colexp;
+  int N;
+  double ar, ai, br, bi;
+};
+
 struct TcSmemBarriers {
   uint64_t full[kStagesTC];
   uint64_t empty[kStagesTC];
@@ -70,16 +79,17 @@ __device__ __forceinline__ double scale2(double x, int e) {
   return e >= -1022 ? x * pow2d(e) : (x * pow2d(e + 1022)) * pow2d(-1022);
 }
 
-// One accumulator pass of the epilogue for the row held by this thread: reads
+// One accumulator pass of the epilogue for the row held by this thread (EP
+// provides D, dn, colexp, N and alpha/beta: TcGemmParams or EpiView): reads
 // the BN accumulator columns of TMEM lane `tcol` (lane and column base
 // encoded) 32 at a time, scales them and updates D through the offset tables.
 // Column metadata (D offset, scale exponent) is loaded once per 32 columns, one
 // column per lane, and broadcast with shuffles; all 32 loads of D of a chunk
 // are issued before any of them is used, so that a warp keeps 1024 loads in
 // flight instead of waiting on each one.
-template <int BN, int EPI>
-__device__ __forceinline__ void epilogue_pass(const TcGemmParams& P, uint32_t tcol, bool mval, int64_t dmo, int re,
-                                              int nb, bool first, int shift) {
+template <int BN, int EPI, class EP>
+__device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool mval, int64_t dmo, int re, int nb,
+                                              bool first, int shift) {
   using namespace sm100;
   constexpr bool OZ = EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C;
   constexpr bool CPLX = EPI == EPI_OZAKI_C || EPI == EPI_BF16_C;

@@ -157,6 +157,50 @@ int tb_tensor_contract_noalloc(const int* cptrn, int data_kind, int drank, const
                                const int* r_dims, const void* r, double alpha_real,
                                double alpha_imag, int conj_bits, int accumulative, void* stream);
 
+/* ---- block-sparse contractions -------------------------------------------
+ * A block-sparse contraction is a list of block tasks D_blk += alpha * L_blk *
+ * R_blk under one index pattern; tasks with the same d pointer add into the
+ * same output block.  ExaTENSOR's TAVP-WRK runs such lists as one
+ * talsh_tensor_contract per block (INTERVIRT/tavp_worker.F90:9420-9518, call
+ * at :9467); these calls run the whole list as one grouped tensor-core
+ * launch (R8: INT8 slices, R4: split BF16), replayed from a CUDA graph. */
+typedef struct {
+  void* d;           /* output block body (device, dlf) */
+  const void* l;     /* left operand block body */
+  const void* r;     /* right operand block body */
+  int d_dims[8];     /* extents; ranks come from the pattern (<= 8) */
+  int l_dims[8];
+  int r_dims[8];
+} tb_block_task_t;
+
+typedef struct tb_bsc_plan_s tb_bsc_plan_t;
+
+typedef struct {
+  int tasks, left_blocks, right_blocks, out_blocks, work_items;
+  int slices;        /* INT8 slices (R8) */
+  int tile_n;        /* GEMM N tile */
+  double flops;      /* sum of 2*M*N*K over the tasks */
+  float tune_ms[4];  /* autotuner timings: (tile 128, 6 slices), (128, 7), (256, 6), (256, 7) */
+} tb_bsc_info_t;
+
+/* Builds the plan: distinct operand blocks, offset tables, tensor maps and the
+ * work list (device memory owned by the plan; blocks must stay allocated).
+ * beta = accumulative ? 1 : 0 applies to every output block once per execution.
+ * plan may set slices (R8, 2..7, default 6) and tile_n (128 or 256). */
+int tb_bsc_plan_create(const char* pattern, int data_kind, int ntasks, const tb_block_task_t* tasks,
+                       double alpha_real, double alpha_imag, int accumulative, const tb_plan_t* plan,
+                       tb_bsc_plan_t** out, void* stream);
+/* Runs the contraction on stream: operand conversion + one grouped GEMM,
+ * captured into a CUDA graph on the first call and replayed afterwards. */
+int tb_bsc_execute(tb_bsc_plan_t* plan, void* stream);
+/* The same launches queued directly on the stream (no graph). */
+int tb_bsc_execute_stream(tb_bsc_plan_t* plan, void* stream);
+/* Times the tile-width and slice-count candidates on the plan's data (with
+ * alpha = 0, beta = 1, so D is unchanged) and keeps the fastest. */
+int tb_bsc_autotune(tb_bsc_plan_t* plan, void* stream);
+int tb_bsc_plan_info(const tb_bsc_plan_t* plan, tb_bsc_info_t* info);
+int tb_bsc_plan_destroy(tb_bsc_plan_t* plan);
+
 /* Seeded U[lo,hi) fill on the device (splitmix64 stream, 53-bit fractions);
  * complex kinds fill real and imaginary parts from consecutive draws. */
 int tb_fill_uniform(int data_kind, size_t volume, void* d, uint64_t seed, double lo, double hi,
