@@ -265,6 +265,84 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs):
     return out
 
 
+BSC = dict(pattern="D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)", nseg=6, lo=8, hi=96, presence=0.3, seed=1)
+
+
+def block_sparse_case(X, stream, stream_obj, dtk=8, steps=1, nseg=None, hi=None, run_loop=True):
+    """Block-sparse CCSD-like contraction: every index split into 6 seeded
+    segments of 8..96, 30% of the blocks of L and R present; all matching
+    block pairs (about 4.2k uneven block GEMMs) as one grouped launch replayed
+    from a CUDA graph, against the per-block loop of tb_tensor_contract calls.
+    Errors compare 16 sampled output blocks of the two runs."""
+    import numpy as np
+    import torch
+
+    from exatensor_b200 import blocksparse as BS
+    cfg = dict(BSC)
+    cfg["nseg"] = nseg or cfg["nseg"]
+    cfg["hi"] = hi or cfg["hi"]
+    rng = np.random.default_rng(cfg["seed"])
+    es = X.ELEM_BYTES[dtk]
+    seg = BS.random_segments(6, cfg["nseg"], cfg["lo"], cfg["hi"], rng)  # a b c d i j
+    segl, segr = seg[0:4], seg[2:6]
+    L = BS.BlockSparseTensor(segl, BS.random_keys(segl, cfg["presence"], rng), es)
+    R = BS.BlockSparseTensor(segr, BS.random_keys(segr, cfg["presence"], rng), es)
+    X.fill_uniform(dtk, L.volume, L.data.data_ptr(), 21, stream=stream)
+    X.fill_uniform(dtk, R.volume, R.data.data_ptr(), 22, stream=stream)
+    D, tasks, pairs = BS.contraction_tasks(cfg["pattern"], L, R)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan = X.BlockSparsePlan(cfg["pattern"], dtk, tasks, accumulative=False, stream=stream)
+    plan_s = time.perf_counter() - t0
+    plan.autotune(stream=stream)
+    inf = plan.info()
+    gms = time_steps(lambda: plan.execute(stream=stream), steps, 1, 1, stream_obj) / steps
+    keys = list(D.blocks)
+    pick = [keys[int(i)] for i in rng.choice(len(keys), size=min(16, len(keys)), replace=False)]
+    dt = {8: np.float64, 4: np.float32}[dtk]
+
+    def sample():
+        torch.cuda.synchronize()
+        out = []
+        for k in pick:
+            off, dims = D.blocks[k]
+            n = int(np.prod(dims))
+            out.append(D.data[off * es:(off + n) * es].cpu().numpy().view(dt).copy())
+        return np.concatenate(out)
+
+    got = sample()
+    plan.close()
+    base = D.data.data_ptr()
+
+    def loop():
+        D.data.zero_()
+        for dp, dd, lp, ld, rp, rd in tasks:
+            X.tensor_contract(cfg["pattern"], dtk, dd, dp, ld, lp, rd, rp, 1.0, 0, True, None, stream)
+
+    if not run_loop:
+        return {"pairs": len(tasks), "flops": inf.flops, "grouped_ms": round(gms, 2),
+                "grouped_tflops": round(inf.flops / (gms / 1e3) / 1e12, 3)}
+    lms = time_steps(loop, 1, 0, 1, stream_obj)
+    want = sample()
+    del base
+    rel = float(np.linalg.norm(got.astype(np.float64) - want) / np.linalg.norm(want))
+    res = {"workload": f"bsc_{'r8' if dtk == 8 else 'r4'}: {cfg['pattern']}, {cfg['nseg']} segments of "
+                       f"{cfg['lo']}..{cfg['hi']} per index, {int(cfg['presence'] * 100)}% blocks, seed {cfg['seed']}",
+           "pairs": len(tasks), "out_blocks": len(D.blocks), "flops": inf.flops,
+           "grouped": {"value": round(inf.flops / (gms / 1e3) / 1e12, 3), "unit": "TFLOP/s", "ms": round(gms, 2),
+                       "launch": "CUDA graph: grouped conversion + one persistent grouped GEMM"},
+           "per_block_loop": {"value": round(inf.flops / (lms / 1e3) / 1e12, 3), "unit": "TFLOP/s",
+                              "ms": round(lms, 2), "launch": f"{len(tasks)} tb_tensor_contract calls"},
+           "grouped_over_loop": round(lms / gms, 2),
+           "rel_frobenius_grouped_vs_loop": rel,
+           "autotune": {"tile_n": inf.tile_n, "slices": inf.slices, "tune_ms": [round(x, 2) for x in inf.tune_ms]},
+           "plan_seconds": round(plan_s, 2)}
+    del L, R, D, tasks
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return res
+
+
 def e2e_talsh(X, wl, steps):
     """Same contraction through talshTensorContract with Host-resident tensors:
     each step copies V, T, D to the GPU and D back (copy control TTT)."""
@@ -355,6 +433,14 @@ def run_ours(args):
     s_obj = torch.cuda.current_stream()
     s = s_obj.cuda_stream
     wl = WORKLOADS[args.workload]
+    bsc = None
+    if rank == 0 and not args.no_block_sparse:
+        try:
+            bsc = block_sparse_case(X, s, s_obj, 8, steps=1)
+        except Exception as exc:  # reported, not fatal: the headline contraction still runs
+            bsc = {"error": str(exc)[:300]}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
     case = ContractionCase(X, wl, s)
     torch.cuda.synchronize()
     # chosen form (plan selector)
@@ -421,7 +507,7 @@ def run_ours(args):
                       "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),
                       "chosen_over_plain": round(value / world / plain, 3)},
             "error": {"chosen": err_chosen, "plain": err_plain, "oracle": "double-double dot products"},
-            "permute": perm, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "permute": perm, "block_sparse": bsc, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk,
         }
     if world > 1:
@@ -446,6 +532,11 @@ def run_profile(args):
     X.device_init(0)
     s_obj = torch.cuda.current_stream()
     s = s_obj.cuda_stream
+    if args.profile == "bsc":
+        print(json.dumps({"profile": "bsc", **block_sparse_case(X, s, s_obj, 8, steps=max(1, args.steps),
+                                                                nseg=args.v or None, hi=args.o or None,
+                                                                run_loop=not (args.v or args.o))}))
+        return
     if args.profile == "permute":
         n = args.v or 76
         v = n ** 4
@@ -479,10 +570,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
-    ap.add_argument("--profile", choices=["contract", "plain", "permute"], default=None,
+    ap.add_argument("--no-block-sparse", action="store_true", help="skip the block-sparse measurement")
+    ap.add_argument("--profile", choices=["contract", "plain", "permute", "bsc"], default=None,
                     help="run one part on a small case for a profiler (no bench line)")
-    ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n)")
-    ap.add_argument("--o", type=int, default=0, help="--profile: occupied extent")
+    ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n; bsc: segments per index)")
+    ap.add_argument("--o", type=int, default=0, help="--profile: occupied extent (bsc: largest segment)")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

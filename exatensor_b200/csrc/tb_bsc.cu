@@ -13,6 +13,7 @@
 // fastest.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <numeric>
 #include <unordered_map>
@@ -93,6 +94,12 @@ struct tb_bsc_plan_s {
   tb::BscDBlk* dblks = nullptr;
   tb::BscPair* pairs = nullptr;
   tb::BscItem* items[2] = {nullptr, nullptr};  // items for BN = 128 / 256
+  tb::BscPass* passes = nullptr;   // per output block, for the current slice count
+  tb::BscChunk* chunks = nullptr;
+  size_t passes_cap = 0, chunks_cap = 0;
+  std::vector<tb::BscDBlk> dblk_host;            // output blocks (pass ranges rewritten per slice count)
+  std::vector<std::vector<int>> dpair_kb;       // K blocks of every pair of every output block
+  std::vector<int> dpair0;                      // first global pair index of every output block
   unsigned* queue = nullptr;
   // graph of the current configuration
   cudaGraph_t graph = nullptr;
@@ -102,38 +109,6 @@ struct tb_bsc_plan_s {
 
 namespace tb {
 namespace {
-
-// Passes of the grouped GEMM for s slices: slice pairs of equal i + j share an
-// INT32 accumulator while entries x K blocks x 2^21 stays below 2^31 for the
-// longest block K (no K split: block K is at most 1023 blocks of 128).
-int bsc_passes(int S, int max_kblocks, BscParams* P) {
-  const int64_t per_entry = (int64_t)max_kblocks << 21;
-  const int64_t cap = per_entry > 0 ? (int64_t)INT32_MAX / per_entry : 0;
-  if (cap < 1) return TB_ERR_NOT_IMPLEMENTED;
-  int np = 0, q = 0;
-  for (int dsum = 2; dsum <= S + 1; ++dsum) {
-    int in_pass = 0;
-    for (int i = 1; i < dsum; ++i) {
-      const int j = dsum - i;
-      if (i > S || j > S) continue;
-      if (in_pass == 0 || in_pass >= cap) {
-        if (np >= kMaxProducts) return TB_ERR_NOT_IMPLEMENTED;
-        P->pass_first[np] = q;
-        P->pass_shift[np] = 8 * dsum - 2;
-        ++np;
-        in_pass = 0;
-      }
-      if (q >= kMaxProducts) return TB_ERR_NOT_IMPLEMENTED;
-      P->prod_a[q] = i - 1;
-      P->prod_b[q] = j - 1;
-      ++q;
-      ++in_pass;
-    }
-  }
-  P->npass = np;
-  P->pass_first[np] = q;
-  return 0;
-}
 
 template <int BN, bool I8, int EPI>
 int launch_bsc(const BscParams& P, int grid, cudaStream_t s) {
@@ -183,15 +158,7 @@ int bsc_enqueue(tb_bsc_plan_s* pl, cudaStream_t s) {
   std::memset(&P, 0, sizeof(P));
   P.lops = pl->lops; P.rops = pl->rops[bi]; P.dblks = pl->dblks; P.pairs = pl->pairs; P.items = pl->items[bi];
   P.queue = pl->queue; P.nitems = pl->n_items[bi];
-  if (pl->i8) {
-    if (int e = bsc_passes(pl->slices, pl->max_kblocks, &P)) {
-      set_error("block-sparse plan: %d slices need too many passes for K blocks of %d", pl->slices, pl->max_kblocks);
-      return e;
-    }
-  } else {
-    P.npass = 1; P.pass_first[0] = 0; P.pass_first[1] = 3;
-    P.prod_a[0] = 0; P.prod_b[0] = 0; P.prod_a[1] = 0; P.prod_b[1] = 1; P.prod_a[2] = 1; P.prod_b[2] = 0;
-  }
+  P.passes = pl->passes; P.chunks = pl->chunks;
   P.ar = pl->ar; P.ai = pl->ai; P.br = pl->br; P.bi = pl->bi;
   P.err = device_error_word();
   const int grid = std::max(1, std::min(P.nitems, num_sms()));
@@ -208,6 +175,75 @@ void drop_graph(tb_bsc_plan_s* pl) {
   pl->graph = nullptr;
 }
 
+// Accumulator passes of every output block for the current slice count.
+// INT8: slice pairs (i, j) of equal i + j share a pass while the K blocks
+// summed into it stay within 1023 (each adds at most 128^3 = 2^21, so the
+// INT32 sum is exact); a product over many pairs is split at pair boundaries.
+// BF16: one pass with the three products over all pairs.
+void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, std::vector<BscChunk>& chunks,
+                 std::vector<BscDBlk>* dbl) {
+  passes.clear();
+  chunks.clear();
+  for (size_t d = 0; d < pl->dpair_kb.size(); ++d) {
+    const std::vector<int>& kb = pl->dpair_kb[d];
+    const int p0 = pl->dpair0[d], np = (int)kb.size();
+    const int pass0 = (int)passes.size();
+    if (!pl->i8) {
+      passes.push_back(BscPass{(int)chunks.size(), 3, 0, 0});
+      chunks.push_back(BscChunk{0, 0, p0, p0 + np});
+      chunks.push_back(BscChunk{0, 1, p0, p0 + np});
+      chunks.push_back(BscChunk{1, 0, p0, p0 + np});
+    } else {
+      for (int dsum = 2; dsum <= S + 1; ++dsum) {
+        int load = 1 << 30;  // forces a new pass for every diagonal
+        for (int i = 1; i < dsum; ++i) {
+          const int j = dsum - i;
+          if (i > S || j > S) continue;
+          int q = 0;
+          while (q < np) {
+            if (load + kb[q] > 1023) {
+              passes.push_back(BscPass{(int)chunks.size(), 0, 8 * dsum - 2, 0});
+              load = 0;
+            }
+            int e = q, l = load;
+            while (e < np && l + kb[e] <= 1023) l += kb[e++];
+            chunks.push_back(BscChunk{i - 1, j - 1, p0 + q, p0 + e});
+            passes.back().nchunk++;
+            load = l;
+            q = e;
+          }
+        }
+      }
+    }
+    if (dbl) {
+      (*dbl)[d].pass0 = pass0;
+      (*dbl)[d].npass = (int)passes.size() - pass0;
+    }
+  }
+}
+
+int build_passes(tb_bsc_plan_s* pl, cudaStream_t s) {
+  std::vector<BscPass> passes;
+  std::vector<BscChunk> chunks;
+  plan_passes(pl, pl->slices, passes, chunks, &pl->dblk_host);
+  if (passes.size() > pl->passes_cap || chunks.size() > pl->chunks_cap) {
+    set_error("block-sparse plan: pass table larger than allocated");
+    return TB_ERR_LIMIT;
+  }
+  if (cudaMemcpyAsync(pl->passes, passes.data(), passes.size() * sizeof(BscPass), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(pl->chunks, chunks.data(), chunks.size() * sizeof(BscChunk), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(pl->dblks, pl->dblk_host.data(), pl->dblk_host.size() * sizeof(BscDBlk), cudaMemcpyHostToDevice,
+                      s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("block-sparse plan: pass table upload failed");
+    return TB_ERR_CUDA;
+  }
+  return 0;
+}
+
 // Sets the slice count used by the gathers (stored in the job table).
 int set_slices(tb_bsc_plan_s* pl, int S, cudaStream_t s) {
   const int n = pl->n_a + pl->n_b;
@@ -220,7 +256,7 @@ int set_slices(tb_bsc_plan_s* pl, int S, cudaStream_t s) {
       cudaStreamSynchronize(s) != cudaSuccess)
     return TB_ERR_CUDA;
   pl->slices = S;
-  return 0;
+  return build_passes(pl, s);
 }
 
 }  // namespace
@@ -268,8 +304,8 @@ int plan_create(const char* pattern, int dtk, int ntasks, const tb_block_task_t*
   auto* pl = new tb_bsc_plan_s();
   pl->dtk = dtk;
   pl->i8 = dtk == kR8;
-  pl->max_slices = pl->i8 ? 7 : 2;
   pl->slices = pl->i8 ? ((plan && plan->slices >= 2 && plan->slices <= 7) ? plan->slices : 6) : 2;
+  pl->max_slices = pl->i8 ? std::max(pl->slices, 6) : 2;  // planes allocated (the autotuner stays within them)
   pl->bn = (plan && plan->tile_n == 128) ? 128 : 256;
   pl->ar = std::abs(ai) > 0 ? (ar != 0.0 ? std::hypot(ar, ai) * (ar > 0 ? 1.0 : -1.0) : ai) : ar;
   pl->br = accumulative ? 1.0 : 0.0;
@@ -348,6 +384,20 @@ int plan_create(const char* pattern, int dtk, int ntasks, const tb_block_task_t*
     pl->flops += 2.0 * (double)A[ia].R * (double)B[ib].R * (double)A[ia].K;
   }
   pl->n_a = (int)A.size(); pl->n_b = (int)B.size(); pl->n_d = (int)Ds.size(); pl->n_pairs = ntasks;
+  // Operand blocks that meet in an output block must share row (column)
+  // scales: union the A blocks (B blocks) of every output block.
+  std::vector<int> ua(A.size()), ub(B.size());
+  std::iota(ua.begin(), ua.end(), 0);
+  std::iota(ub.begin(), ub.end(), 0);
+  auto find = [](std::vector<int>& u, int x) {
+    while (u[x] != x) x = u[x] = u[u[x]];
+    return x;
+  };
+  for (auto& d : Ds)
+    for (auto& pr : d.pairs) {
+      ua[find(ua, pr.first)] = find(ua, d.pairs[0].first);
+      ub[find(ub, pr.second)] = find(ub, d.pairs[0].second);
+    }
   // sizes, tables, planes
   const int oes = pl->i8 ? 1 : 2;
   const int np = pl->i8 ? pl->max_slices : 2;
@@ -356,13 +406,18 @@ int plan_create(const char* pattern, int dtk, int ntasks, const tb_block_task_t*
   int max_kb = 0;
   for (auto* V : {&A, &B}) {
     const bool isb = V == &B;
-    for (auto& o : *V) {
+    std::vector<int>& u = isb ? ub : ua;
+    std::vector<size_t> comp_off(V->size(), SIZE_MAX);
+    for (size_t i = 0; i < V->size(); ++i) {
+      OpBlock& o = (*V)[i];
       o.Rpad = rup(o.R, isb ? 256 : 128);
       o.Kpad = rup(o.K, 128);
       max_kb = std::max<int>(max_kb, (int)(o.Kpad * oes / 128));
       o.lm_off = tab.size(); host_offsets(o.rows, false, tab);
       o.lk_off = tab.size(); host_offsets(o.ks, false, tab);
-      o.e_off = erows; erows += (size_t)o.R;
+      const int c = find(u, (int)i);  // exponent rows are per component (same row count by construction)
+      if (comp_off[c] == SIZE_MAX) { comp_off[c] = erows; erows += (size_t)o.R; }
+      o.e_off = comp_off[c];
       o.plane_off = plane_bytes;
       plane_bytes += (size_t)np * o.Rpad * o.Kpad * oes;
       plane_bytes = (plane_bytes + 255) & ~size_t(255);
@@ -443,18 +498,36 @@ int plan_create(const char* pattern, int dtk, int ntasks, const tb_block_task_t*
   pl->rops[0] = upload(pl, r128, &err, s);
   pl->rops[1] = upload(pl, r256, &err, s);
   // output blocks, pairs and work items (largest first)
-  std::vector<BscDBlk> dbl(Ds.size());
+  std::vector<BscDBlk>& dbl = pl->dblk_host;
+  dbl.assign(Ds.size(), BscDBlk{});
   std::vector<BscPair> prs;
+  pl->dpair_kb.assign(Ds.size(), {});
+  pl->dpair0.assign(Ds.size(), 0);
   for (size_t d = 0; d < Ds.size(); ++d) {
     dbl[d].D = Ds[d].ptr;
     dbl[d].dm = pl->tables + dm_off[d];
     dbl[d].dn = pl->tables + dn_off[d];
     dbl[d].M = (int)Ds[d].M; dbl[d].N = (int)Ds[d].N;
-    dbl[d].pair0 = (int)prs.size(); dbl[d].npair = (int)Ds[d].pairs.size();
-    for (auto& p : Ds[d].pairs) prs.push_back(BscPair{p.first, p.second});
+    pl->dpair0[d] = (int)prs.size();
+    for (auto& p : Ds[d].pairs) {
+      prs.push_back(BscPair{p.first, p.second});
+      pl->dpair_kb[d].push_back((int)(A[p.first].Kpad * oes / 128));
+    }
+  }
+  {
+    std::vector<BscPass> ps;
+    std::vector<BscChunk> cs;
+    plan_passes(pl, pl->i8 ? pl->max_slices : 2, ps, cs, nullptr);  // the largest tables any slice count needs
+    pl->passes_cap = ps.size();
+    pl->chunks_cap = cs.size();
+    pl->passes = (BscPass*)dalloc(ps.size() * sizeof(BscPass), &err);
+    if (pl->passes) pl->allocs.push_back(pl->passes);
+    pl->chunks = (BscChunk*)dalloc(cs.size() * sizeof(BscChunk), &err);
+    if (pl->chunks) pl->allocs.push_back(pl->chunks);
   }
   pl->dblks = upload(pl, dbl, &err, s);
   pl->pairs = upload(pl, prs, &err, s);
+  if (!err) err = build_passes(pl, s);
   for (int bi = 0; bi < 2; ++bi) {
     const int BN = bi ? 256 : 128;
     std::vector<std::pair<int64_t, BscItem>> its;
@@ -565,7 +638,7 @@ extern "C" int tb_bsc_autotune(tb_bsc_plan_t* pl, void* stream) {
   const int s0 = pl->slices, bn0 = pl->bn;
   pl->ar = 0.0; pl->ai = 0.0; pl->br = 1.0; pl->bi = 0.0;
   const int cand_s[2] = {6, 7};
-  const int ns = pl->i8 ? 2 : 1;
+  const int ns = pl->i8 ? (pl->max_slices >= 7 ? 2 : 1) : 1;
   float best = 1e30f;
   int bs = s0, bbn = bn0, err = 0;
   cudaEvent_t e0, e1;

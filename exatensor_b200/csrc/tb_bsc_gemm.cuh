@@ -7,10 +7,11 @@
 //
 // Work items are (output block, 128-row tile, BN-column tile), ordered by
 // decreasing cost; CTAs take them from a device-side queue (one atomic counter)
-// so that the uneven blocks balance across the SMs.  A work item runs all its
-// pairs back to back in the same TMEM accumulators: each (pair, pass) hands one
-// accumulator to the epilogue, which adds it into the output tile, so pairs
-// that share an output block never race.  Roles as in tc_gemm_kernel:
+// so that the uneven blocks balance across the SMs.  A work item sums all its
+// pairs inside each TMEM accumulator pass (the operand blocks of an output
+// block share row and column scales, so that INT32 sums over several pairs
+// stay exact) and hands each pass to the epilogue, which adds it into the
+// output tile; pairs that share an output block therefore never race.  Roles as in tc_gemm_kernel:
 //   warp 0   queue + TMA producer (one lane); it publishes every item it takes
 //            in a small shared-memory ring read by the other roles
 //   warp 1   TMEM allocation and the single MMA-issuing thread
@@ -38,10 +39,17 @@ struct __align__(16) BscDBlk {  // output block
   const int64_t* dm;            // D offset of row m
   const int64_t* dn;            // D offset of column n
   int M, N;
-  int pair0, npair;             // its (L, R) pairs: pairs[pair0 .. pair0 + npair)
+  int pass0, npass;             // its accumulator passes: passes[pass0 .. pass0 + npass)
 };
 struct BscPair { int l, r; };
 struct BscItem { int d, mt, nt, pad_; };
+// A pass is one exact TMEM accumulator: chunks[chunk0 .. chunk0 + nchunk),
+// each the product of plane a of A and plane b of B summed over the pairs
+// pairs[p0 .. p1) of the output block (all their K blocks).  INT8 slices: the
+// pass's weight is 2^-shift; the operand blocks of one output block share
+// their row (column) scales, so their products add up exactly in INT32.
+struct BscPass { int chunk0, nchunk, shift, pad_; };
+struct BscChunk { int a, b, p0, p1; };
 
 constexpr int kBscRing = 4;
 
@@ -51,13 +59,11 @@ struct __align__(64) BscParams {
   const BscDBlk* dblks;
   const BscPair* pairs;
   const BscItem* items;
+  const BscPass* passes;
+  const BscChunk* chunks;
   unsigned int* queue;          // next item (zeroed before every launch)
   int nitems;
-  int npass;
-  int pass_first[kMaxProducts + 1];
-  int prod_a[kMaxProducts], prod_b[kMaxProducts];
-  int pass_shift[kMaxProducts];
-  double ar, ai, br, bi;        // beta applies to the first (pair, pass) of each tile
+  double ar, ai, br, bi;        // beta applies to the first pass of each tile
   unsigned int* err;
 };
 
@@ -117,20 +123,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
         if (cur < 0) break;
         const BscItem I = P.items[cur];
         const BscDBlk Dd = P.dblks[I.d];
-        for (int pp = 0; pp < Dd.npair && ok; ++pp) {
-          const BscPair pr = P.pairs[Dd.pair0 + pp];
-          const BscLOp lo = P.lops[pr.l];
-          const BscROp ro = P.rops[pr.r];
-          for (int q = 0; q < P.pass_first[P.npass] && ok; ++q) {
-            for (int kb = 0; kb < lo.kblocks; ++kb, ++it) {
-              const int s = (int)(it % kStagesTC);
-              const uint32_t ph = (it / kStagesTC) & 1;
-              if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err))) break;
-              mbar_expect_tx(&bars->full[s], 128 * 128 + BN * 128);
-              tma_load_3d(smA + (size_t)s * 128 * 128, lo.map, kb * (I8 ? 128 : 64), I.mt * 128, P.prod_a[q],
-                          &bars->full[s]);
-              tma_load_3d(smB + (size_t)s * BN * 128, ro.map, kb * (I8 ? 128 : 64), I.nt * BN, P.prod_b[q],
-                          &bars->full[s]);
+        for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p) {
+          const BscPass ps = P.passes[p];
+          for (int c = ps.chunk0; c < ps.chunk0 + ps.nchunk && ok; ++c) {
+            const BscChunk ch = P.chunks[c];
+            for (int pp = ch.p0; pp < ch.p1 && ok; ++pp) {
+              const BscPair pr = P.pairs[pp];
+              const BscLOp lo = P.lops[pr.l];
+              const CUtensorMap* rmap = P.rops[pr.r].map;
+              for (int kb = 0; kb < lo.kblocks; ++kb, ++it) {
+                const int s = (int)(it % kStagesTC);
+                const uint32_t ph = (it / kStagesTC) & 1;
+                if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err))) break;
+                mbar_expect_tx(&bars->full[s], 128 * 128 + BN * 128);
+                tma_load_3d(smA + (size_t)s * 128 * 128, lo.map, kb * (I8 ? 128 : 64), I.mt * 128, ch.a,
+                            &bars->full[s]);
+                tma_load_3d(smB + (size_t)s * BN * 128, rmap, kb * (I8 ? 128 : 64), I.nt * BN, ch.b,
+                            &bars->full[s]);
+              }
             }
           }
         }
@@ -148,17 +158,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
         if (cur < 0) break;
         const BscItem I = P.items[cur];
         const BscDBlk Dd = P.dblks[I.d];
-        for (int pp = 0; pp < Dd.npair && ok; ++pp) {
-          const BscPair pr = P.pairs[Dd.pair0 + pp];
-          const int kblocks = P.lops[pr.l].kblocks;
-          for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
-            const int a = acc_it & 1;
-            const uint32_t aph = (acc_it >> 1) & 1;
-            if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err))) break;
-            tc_fence_after();
-            const uint32_t dcol = tmem + (uint32_t)(a * BN);
-            bool first = true;
-            for (int q = P.pass_first[p]; q < P.pass_first[p + 1] && ok; ++q) {
+        for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p, ++acc_it) {
+          const BscPass ps = P.passes[p];
+          const int a = acc_it & 1;
+          const uint32_t aph = (acc_it >> 1) & 1;
+          if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err))) break;
+          tc_fence_after();
+          const uint32_t dcol = tmem + (uint32_t)(a * BN);
+          bool first = true;
+          for (int c = ps.chunk0; c < ps.chunk0 + ps.nchunk && ok; ++c) {
+            const BscChunk ch = P.chunks[c];
+            for (int pp = ch.p0; pp < ch.p1 && ok; ++pp) {
+              const int kblocks = P.lops[P.pairs[pp].l].kblocks;
               for (int kb = 0; kb < kblocks; ++kb, ++it) {
                 const int s = (int)(it % kStagesTC);
                 const uint32_t ph = (it / kStagesTC) & 1;
@@ -174,8 +185,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
                 mma_commit(&bars->empty[s]);
               }
             }
-            mma_commit(&bars->acc_full[a]);
           }
+          mma_commit(&bars->acc_full[a]);
         }
         mbar_arrive(&bars->item_empty[slot]);
       }
@@ -194,22 +205,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
       const int m = I.mt * 128 + quad * 32 + lane;
       const bool mval = m < Dd.M;
       const int64_t dmo = mval ? Dd.dm[m] : 0;
-      for (int pp = 0; pp < Dd.npair && ok; ++pp) {
-        const BscPair pr = P.pairs[Dd.pair0 + pp];
-        const int re = (EPI == EPI_OZAKI_R) && mval ? P.lops[pr.l].rowexp[m] : 0;
-        const EpiView V{Dd.D, Dd.dn, P.rops[pr.r].colexp, Dd.N, P.ar, P.ai, P.br, P.bi};
-        for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
-          const int a = acc_it & 1;
-          const uint32_t aph = (acc_it >> 1) & 1;
-          if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err))) break;
-          tc_fence_after();
-          const int shift = (EPI == EPI_OZAKI_R) ? P.pass_shift[p] : 0;
-          epilogue_pass<BN, EPI>(V, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, I.nt,
-                                 pp == 0 && p == 0, shift);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bars->acc_empty[a]);
-        }
+      // all pairs of an output block share its row and column scales
+      const BscPair pr0 = P.pairs[P.chunks[P.passes[Dd.pass0].chunk0].p0];
+      const int re = (EPI == EPI_OZAKI_R) && mval ? P.lops[pr0.l].rowexp[m] : 0;
+      const EpiView V{Dd.D, Dd.dn, P.rops[pr0.r].colexp, Dd.N, P.ar, P.ai, P.br, P.bi};
+      for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p, ++acc_it) {
+        const int a = acc_it & 1;
+        const uint32_t aph = (acc_it >> 1) & 1;
+        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err))) break;
+        tc_fence_after();
+        const int shift = (EPI == EPI_OZAKI_R) ? P.passes[p].shift : 0;
+        epilogue_pass<BN, EPI>(V, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, I.nt,
+                               p == Dd.pass0, shift);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars->acc_empty[a]);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&bars->item_empty[slot]);
