@@ -343,6 +343,61 @@ def block_sparse_case(X, stream, stream_obj, dtk=8, steps=1, nseg=None, hi=None,
     return res
 
 
+SELECTOR_CORPUS = os.path.join(ROOT, "tests", "golden", "selector_corpus.npz")
+
+
+def selector_case(X):
+    """Learned plan selector on the recorded corpus: trained with the
+    library's CUDA kernels on the first 80% of the corpus, judged on the rest
+    by runtime regret against the best measured plan, beside the size rule;
+    plus the selection latency of the host inference used by METHOD_AUTO and
+    the GPU batch inference kernel's throughput."""
+    import numpy as np
+    import torch
+
+    from exatensor_b200 import selector as S
+    if not os.path.exists(SELECTOR_CORPUS):
+        return None
+    d = np.load(SELECTOR_CORPUS)
+    F, T = d["features"], d["log_ms"]
+    ok = np.isfinite(T).all(axis=1)
+    F, T = F[ok], T[ok]
+    n_train = int(0.8 * len(F))
+    t0 = time.perf_counter()
+    params, mean, scale, hist = S.train(F[:n_train], T[:n_train], hidden=128, epochs=150, seed=0, log_every=149)
+    train_s = time.perf_counter() - t0
+    pred = S.predict(params, mean, scale, F[n_train:], hidden=128)
+    learned = S.evaluate(T[n_train:], pred.argmin(axis=1))
+    rule = S.evaluate(T[n_train:], [S.rule_choice(f) for f in F[n_train:]])
+    always = {name: S.evaluate(T[n_train:], [i] * (len(F) - n_train))["total_time_regret"]
+              for i, name in enumerate(S.PLAN_NAMES)}
+    X.selector_install(128, params, mean, scale)
+    t0 = time.perf_counter()
+    for f in F[n_train:n_train + 2000]:
+        X.selector_choose(f)
+    host_us = (time.perf_counter() - t0) / min(2000, len(F) - n_train) * 1e6
+    X.selector_install(0, None, None, None)
+    net = X.MLP(F.shape[1], 128, len(S.PLANS), max_batch=1024)
+    net.set_params(params)
+    xn = torch.from_numpy(((F[n_train:] - mean) / scale).astype(np.float32)).cuda()
+    y = torch.empty((len(xn), len(S.PLANS)), dtype=torch.float32, device="cuda")
+    net.forward(xn.data_ptr(), len(xn), y.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        net.forward(xn.data_ptr(), len(xn), y.data_ptr())
+    e1.record()
+    torch.cuda.synchronize()
+    gpu_us = e0.elapsed_time(e1) / 10 * 1e3 / len(xn)
+    net.close()
+    return {"corpus": f"{int(ok.sum())} labelled random contractions (seed 0), {n_train} train / "
+                      f"{len(F) - n_train} held out", "plans": S.PLAN_NAMES,
+            "learned": learned, "size_rule": rule, "always_one_plan_total_regret": always,
+            "train_seconds": round(train_s, 1), "final_train_loss": round(hist[-1][1], 4) if hist else None,
+            "selection_us_host": round(host_us, 2), "selection_us_gpu_batched": round(gpu_us, 4)}
+
+
 def e2e_talsh(X, wl, steps):
     """Same contraction through talshTensorContract with Host-resident tensors:
     each step copies V, T, D to the GPU and D back (copy control TTT)."""
@@ -415,7 +470,9 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": "TFLOP/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v)",
-            "config": {"workload": "ccsd1_r8 CPU sample v=96 o=48", "parallelism": "host threads"},
+            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['pattern']} "
+                                   f"v={WORKLOADS[args.workload]['v']} o={WORKLOADS[args.workload]['o']}",
+                       "parallelism": "host threads", "sample": res["sample"]},
             "cpu_baseline": res,
             "e2e": {"value": res["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -473,6 +530,10 @@ def run_ours(args):
         err_chosen = sample_error(X, case, X.METHOD_AUTO)
         err_plain = sample_error(X, case, X.METHOD_TTGT)
         perm = permute_sweep(X, s, s_obj, hbm_gbs)
+        try:
+            sel = selector_case(X)
+        except Exception as exc:  # reported, not fatal
+            sel = {"error": str(exc)[:300]}
         # dominant kernel of the chosen step
         per_launch_ms = gemm_ms / max(1, gemm_n)
         if chosen_method == "fused":
@@ -507,7 +568,8 @@ def run_ours(args):
                       "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),
                       "chosen_over_plain": round(value / world / plain, 3)},
             "error": {"chosen": err_chosen, "plain": err_plain, "oracle": "double-double dot products"},
-            "permute": perm, "block_sparse": bsc, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "permute": perm, "block_sparse": bsc, "selector": sel, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e,
             "gpu_launches": launches, "clocks": clk,
         }
     if world > 1:
@@ -532,6 +594,9 @@ def run_profile(args):
     X.device_init(0)
     s_obj = torch.cuda.current_stream()
     s = s_obj.cuda_stream
+    if args.profile == "selector":
+        print(json.dumps({"profile": "selector", **(selector_case(X) or {"error": "no corpus"})}))
+        return
     if args.profile == "bsc":
         print(json.dumps({"profile": "bsc", **block_sparse_case(X, s, s_obj, 8, steps=max(1, args.steps),
                                                                 nseg=args.v or None, hi=args.o or None,
@@ -571,7 +636,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
     ap.add_argument("--no-block-sparse", action="store_true", help="skip the block-sparse measurement")
-    ap.add_argument("--profile", choices=["contract", "plain", "permute", "bsc"], default=None,
+    ap.add_argument("--profile", choices=["contract", "plain", "permute", "bsc", "selector"], default=None,
                     help="run one part on a small case for a profiler (no bench line)")
     ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n; bsc: segments per index)")
     ap.add_argument("--o", type=int, default=0, help="--profile: occupied extent (bsc: largest segment)")

@@ -94,6 +94,19 @@ def lib() -> C.CDLL:
     L.tb_bsc_autotune.argtypes = [vp, vp]
     L.tb_bsc_plan_info.argtypes = [vp, C.POINTER(BscInfo)]
     L.tb_bsc_plan_destroy.argtypes = [vp]
+    fp = C.POINTER(C.c_float)
+    L.tb_contract_descriptor.argtypes = [ip, C.c_int, C.c_int, ip, C.c_int, ip, C.c_int, ip, fp]
+    L.tb_mlp_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]
+    L.tb_mlp_destroy.argtypes = [vp]
+    L.tb_mlp_num_params.argtypes = [vp]
+    L.tb_mlp_num_params.restype = C.c_longlong
+    L.tb_mlp_get_params.argtypes = [vp, fp, C.c_int]
+    L.tb_mlp_set_params.argtypes = [vp, fp]
+    L.tb_mlp_forward.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.tb_mlp_backward.argtypes = [vp, vp, vp, C.c_int, fp, vp]
+    L.tb_mlp_adam_step.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, vp]
+    L.tb_selector_install.argtypes = [C.c_int, fp, fp, fp, C.c_float, C.c_int]
+    L.tb_selector_choose.argtypes = [fp, fp]
     L.tb_fill_uniform.argtypes = [C.c_int, C.c_size_t, vp, C.c_uint64, C.c_double, C.c_double, vp]
     L.tb_last_contract_stats.argtypes = [C.POINTER(ContractStats)]
     _lib = L
@@ -235,6 +248,88 @@ class BlockSparsePlan:
             self.close()
         except Exception:
             pass
+
+
+DESC_FEATURES, SELECT_PLANS = 16, 3
+
+
+def contract_descriptor(pattern, dtk, ddims, ldims, rdims):
+    """Feature vector of a contraction (host only; see tb_contract_descriptor)."""
+    import numpy as np
+    cptrn, dr, lr, rr, _ = parse_pattern(pattern)
+    f = (C.c_float * DESC_FEATURES)()
+    _check(lib().tb_contract_descriptor(iarr(cptrn), dtk, len(ddims), iarr(ddims), len(ldims), iarr(ldims),
+                                        len(rdims), iarr(rdims), f))
+    return np.array(f[:], dtype=np.float32)
+
+
+def _fptr(a):
+    import numpy as np
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class MLP:
+    """The selector network on the GPU (tb_mlp_*): in -> hidden -> hidden -> out."""
+
+    def __init__(self, n_in, n_hidden, n_out, max_batch=256, seed=1):
+        h = C.c_void_p()
+        _check(lib().tb_mlp_create(n_in, n_hidden, n_out, max_batch, seed, C.byref(h)))
+        self._h, self.n_in, self.n_hidden, self.n_out, self.max_batch = h, n_in, n_hidden, n_out, max_batch
+        self.n_params = int(lib().tb_mlp_num_params(h))
+
+    def params(self, grads=False):
+        import numpy as np
+        out = np.empty(self.n_params, dtype=np.float32)
+        _check(lib().tb_mlp_get_params(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), int(grads)))
+        return out
+
+    def set_params(self, p):
+        a, ptr = _fptr(p)
+        _check(lib().tb_mlp_set_params(self._h, ptr))
+
+    def forward(self, x_dev_ptr, batch, y_dev_ptr, stream=None):
+        _check(lib().tb_mlp_forward(self._h, C.c_void_p(x_dev_ptr), batch, C.c_void_p(y_dev_ptr), _stream(stream)))
+
+    def backward(self, x_dev_ptr, t_dev_ptr, batch, stream=None, want_loss=True):
+        loss = C.c_float()
+        _check(lib().tb_mlp_backward(self._h, C.c_void_p(x_dev_ptr), C.c_void_p(t_dev_ptr), batch,
+                                     C.byref(loss) if want_loss else None, _stream(stream)))
+        return loss.value
+
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
+        _check(lib().tb_mlp_adam_step(self._h, lr, beta1, beta2, eps, _stream(stream)))
+
+    def close(self):
+        if self._h:
+            lib().tb_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def selector_install(n_hidden, params, mean, scale, margin=0.0, autotune=False):
+    """Installs a trained selector for METHOD_AUTO (params None removes it)."""
+    if params is None:
+        _check(lib().tb_selector_install(0, None, None, None, 0.0, 0))
+        return
+    _p, pp = _fptr(params)
+    _m, mp = _fptr(mean)
+    _s, sp = _fptr(scale)
+    _check(lib().tb_selector_install(n_hidden, pp, mp, sp, float(margin), int(autotune)))
+
+
+def selector_choose(features):
+    """(plan index, predicted log-runtimes) for a descriptor, or (-1, None)."""
+    import numpy as np
+    _f, fp = _fptr(features)
+    y = (C.c_float * SELECT_PLANS)()
+    idx = lib().tb_selector_choose(fp, y)
+    return idx, (np.array(y[:]) if idx >= 0 else None)
 
 
 NOALLOC_ARENA_BYTES = 64 << 20  # TB_NOALLOC_ARENA_BYTES

@@ -272,6 +272,28 @@ done:
 
 }  // namespace
 
+// Runs a non-scalar contraction with plan->method (TTGT or FUSED).  With
+// fallback, a fused request outside the tensor-core path's scope runs as TTGT.
+int run_method(const Matricization& Z, int dtk, const int* ddims, void* d, const int* ldims, const void* l,
+               const int* rdims, const void* r, double ar, double ai, int accumulative, int lconj, int rconj,
+               const tb_plan_t* plan, cudaStream_t s, bool fallback = true) {
+  if (plan->method == TB_METHOD_FUSED) {
+    const int e = contract_fused(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, lconj, rconj, plan, s,
+                                 &g_stats);
+    if (e != TB_ERR_NOT_IMPLEMENTED) { if (!e) g_stats.method = TB_METHOD_FUSED; return e; }
+    if (!fallback) return e;  // explicitly requested: no silent substitution
+  }
+  g_stats.method = TB_METHOD_TTGT;
+  g_stats.gemm_launches = 1;
+  switch (dtk) {
+    case kR4: return ttgt<float>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, 0, 0, s);
+    case kR8: return ttgt<double>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, 0, 0, s);
+    case kC4: return ttgt<float2>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, lconj, rconj, s);
+    case kC8: return ttgt<double2>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, lconj, rconj, s);
+  }
+  return TB_ERR_INVALID_ARGS;
+}
+
 int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* d, int lrank, const int* ldims,
                   const void* l, int rrank, const int* rdims, const void* r, double ar, double ai, int conj_bits,
                   int accumulative, const tb_plan_t* plan, cudaStream_t s) {
@@ -301,22 +323,57 @@ int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* 
     }
   }
   int method = plan ? plan->method : TB_METHOD_AUTO;
-  if (method == TB_METHOD_AUTO) method = select_method(dtk, Z, plan);
-  if (method == TB_METHOD_FUSED) {
-    e = contract_fused(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, lconj, rconj, plan, s,
-                       &g_stats);
-    if (e != TB_ERR_NOT_IMPLEMENTED) { if (!e) g_stats.method = TB_METHOD_FUSED; return e; }
-    if (plan && plan->method == TB_METHOD_FUSED) return e;  // explicitly requested: no silent substitution
+  tb_plan_t learned;
+  if (method == TB_METHOD_AUTO) {
+    // learned selector when installed, else the size rule
+    float f[TB_DESC_FEATURES];
+    int idx = -1;
+    bool ambiguous = false;
+    uint64_t key = 0;
+    descriptor_of(Z, dtk, f);
+    if (selector_pick(f, &idx, &ambiguous, &key) == 0) {
+      if (ambiguous) {
+        // too close to call: time every candidate once with alpha = 0, beta = 1 (D unchanged)
+        float best = 1e30f;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        for (int c = 0; c < TB_SELECT_PLANS; ++c) {
+          tb_plan_t cp = plan ? *plan : tb_plan_t{};
+          cp.method = c == 0 ? TB_METHOD_TTGT : TB_METHOD_FUSED;
+          cp.tile_n = c == 1 ? 128 : (c == 2 ? 256 : 0);
+          cudaEventRecord(e0, s);
+          const int ce = run_method(Z, dtk, ddims, d, ldims, l, rdims, r, 0.0, 0.0, 1, lconj, rconj, &cp, s);
+          cudaEventRecord(e1, s);
+          float ms = 0.f;
+          if (!ce && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
+              ms < best) {
+            best = ms;
+            idx = c;
+          }
+          cudaGetLastError();
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        selector_remember(key, idx);
+        std::memset(&g_stats, 0, sizeof(g_stats));
+        g_stats.m = Z.M; g_stats.n = Z.N; g_stats.k = Z.K;
+        g_stats.flops = (cplx ? 8.0 : 2.0) * (double)Z.M * (double)Z.N * (double)Z.K;
+      }
+      learned = plan ? *plan : tb_plan_t{};
+      learned.method = idx == 0 ? TB_METHOD_TTGT : TB_METHOD_FUSED;
+      learned.tile_n = idx == 1 ? 128 : (idx == 2 ? 256 : 0);
+      return run_method(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative, lconj, rconj, &learned, s,
+                        /*fallback=*/true);
+    }
+    method = select_method(dtk, Z, plan);
   }
-  g_stats.method = TB_METHOD_TTGT;
-  g_stats.gemm_launches = 1;
-  switch (dtk) {
-    case kR4: return ttgt<float>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, 0, 0, s);
-    case kR8: return ttgt<double>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, 0, 0, s);
-    case kC4: return ttgt<float2>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, lconj, rconj, s);
-    case kC8: return ttgt<double2>(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative != 0, lconj, rconj, s);
-  }
-  return TB_ERR_INVALID_ARGS;
+  if (method == TB_METHOD_AUTO) method = TB_METHOD_TTGT;
+  learned = plan ? *plan : tb_plan_t{};
+  const bool requested = plan && plan->method == TB_METHOD_FUSED;
+  learned.method = method;
+  return run_method(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative, lconj, rconj, &learned, s,
+                    /*fallback=*/!requested);
 }
 
 }  // namespace tb

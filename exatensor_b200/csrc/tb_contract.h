@@ -20,4 +20,12 @@ int contract_fused(const Matricization& Z, int dtk, const int* ddims, void* d, c
                    const int* rdims, const void* r, double ar, double ai, bool accumulate, int lconj, int rconj,
                    const tb_plan_t* plan, cudaStream_t s, tb_contract_stats_t* stats);
 
+// Learned plan selection (tb_select.cu).
+int descriptor_of(const Matricization& Z, int dtk, float* features);
+// -1 when no selector is installed; else 0 with the chosen plan index, whether
+// the two best predictions are too close to call (and autotuning is on), and a
+// cache key of the descriptor.
+int selector_pick(const float* features, int* idx, bool* ambiguous, uint64_t* key);
+void selector_remember(uint64_t key, int idx);
+
 }  // namespace tb

@@ -81,6 +81,21 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   }
   if (blast < 0) return TB_ERR_NOT_IMPLEMENTED;
   auto vol_of = [&]() { int64_t v = 1; for (int i = 0; i < r; ++i) v *= t[i]; return v; };
+  // 4a. the fastest dimension stays fastest (the load and store blocks end on
+  // the same dim): the permutation moves whole runs of it, so make those runs
+  // long -- that dim up to Vmax, then the next input dim as the row direction.
+  if (a == blast) {
+    const int64_t others = vol_of() / t[a];
+    t[a] = std::max(t[a], even(D[a], std::max<int64_t>(1, Vmax / others)));
+    if (vol_of() < Vmin && a + 1 < r && t[a + 1] == 1) {
+      // a divisor of the extent, so that this dim is never partial (only the
+      // load and store blocks' last dims may be: pa, pb)
+      int64_t want = std::max<int64_t>(1, Vmax / vol_of()), best = 1;
+      for (int64_t x = std::min(want, D[a + 1]); x >= 1; --x)
+        if (D[a + 1] % x == 0) { best = x; break; }
+      t[a + 1] = best;
+    }
+  }
   // 4. extend the tile to Vmin elements: whole small dims first, then the partial dims
   for (int guard = 0; guard < 4 * r + 8; ++guard) {
     int64_t V = vol_of();
@@ -200,6 +215,12 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     }
     P.st_base[c] = off; P.st_ebase[c] = (int32_t)eb; P.st_dpa[c] = (int16_t)dpa;
   }
+  P.lin2d = (restA.size() <= 1 && restB.size() <= 1 && prodB == 1) ? 1 : 0;
+  P.row_is_pb = (!restA.empty() && restA[0] == pb) ? 1 : 0;
+  P.chunk_is_pa = (!restB.empty() && restB[0] == pa) ? 1 : 0;
+  P.row_sin = restA.empty() ? 0 : SI[restA[0]];
+  P.chunk_sout = restB.empty() ? 0 : SO[restB[0]];
+  P.chunk_eb = restB.empty() ? 0 : (int32_t)est[restB[0]];
   // positions inside a store chunk: store-block dims before blast
   for (int64_t j = 0; j < prodB; ++j) {
     int64_t x = j, e = 0;

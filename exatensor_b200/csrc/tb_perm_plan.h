@@ -50,6 +50,15 @@ struct PermParams {
   int32_t st_ebase[kMaxChunks]; // shared-memory position base of store chunk c'
   int16_t st_dpa[kMaxChunks];   // digit of pa in store chunk c' (-1: pa inside the chunk or none)
   int32_t ejf[kMaxEjf];         // shared-memory position of j' % prodB inside a store chunk
+  // Two-dimensional tiles (at most one dim outside the load block, at most one
+  // outside the store block, single-dim store block): load row c starts at
+  // c * row_sin in the input, store chunk c at c * chunk_sout in the output and
+  // at c * chunk_eb in shared memory, and position j of a store chunk sits at
+  // j * ej_pb_stride after it.  Lets the kernel skip the chunk tables.
+  int lin2d;
+  int row_is_pb, chunk_is_pa;   // the row (chunk) dim is the partial dim pb (pa)
+  int64_t row_sin, chunk_sout;
+  int32_t chunk_eb;
 };
 
 // Host-side plan builder.  dims/sin/sout describe the input dims (input

@@ -15,6 +15,7 @@
 #include "tb_common.cuh"
 #include "tb_perm_plan.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
@@ -248,18 +249,97 @@ perm_pipe_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ 
   if (!BULK) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Two-dimensional tiles (PermParams::lin2d): every load row and every store
+// chunk is one step of a single dimension, so their offsets are c * stride and
+// the kernel needs no chunk tables.  Warps take whole rows (loads: 16-byte or
+// element cp.async, lanes along the row) and whole chunks (stores: lanes along
+// the output run), which keeps the instruction count per element low; the
+// 3-stage cp.async pipeline is the same as perm_pipe_kernel's !BULK path.
+template <typename Elem>
+__device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in, Elem* stage, int64_t tile) {
+  const TileOrigin o = tile_origin(P, tile);
+  int len = P.LA;
+  if (!o.full && P.pa >= 0) len = P.prodA * (P.pb == P.pa ? min(o.rem_a, o.rem_b) : o.rem_a);
+  int rows = P.nA;
+  if (!o.full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = min(rows, o.rem_b);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kW = kPermThreads / 32;
+  const bool vec = P.tma_ok && sizeof(Elem) < 16;
+  constexpr int VW = sizeof(Elem) < 16 ? 16 / sizeof(Elem) : 1;
+  const int w = vec ? VW : 1;
+  const int nvec = (len + w - 1) / w;
+  for (int r = warp; r < rows; r += kW) {
+    const Elem* src = in + o.in_base + (int64_t)r * P.row_sin;
+    Elem* dst = stage + (size_t)r * P.lap;
+    for (int v = lane; v < nvec; v += 32) {
+      const int j = v * w;
+      if (vec || sizeof(Elem) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst + j)), "l"(src + j) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst + j)), "l"(src + j),
+                     "n"(sizeof(Elem))
+                     : "memory");
+    }
+  }
+}
+
+template <typename Elem, typename Store>
+__device__ __forceinline__ void perm2d_store(const PermParams& P, const Elem* stage, int64_t tile, const Store& st) {
+  const TileOrigin o = tile_origin(P, tile);
+  const int qlim = (!o.full && P.pb >= 0) ? (P.pa == P.pb ? min(o.rem_a, o.rem_b) : o.rem_b) : (1 << 30);
+  int chunks = P.nB;
+  if (!o.full && P.pa >= 0 && P.pa != P.pb && P.chunk_is_pa) chunks = min(chunks, o.rem_a);
+  const int jlim = min(P.LB, qlim);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kW = kPermThreads / 32;
+  const int pstride = P.ej_pb_stride;
+  for (int c = warp; c < chunks; c += kW) {
+    const int64_t ob = o.out_base + (int64_t)c * P.chunk_sout;
+    const Elem* sb = stage + (size_t)c * P.chunk_eb;
+#pragma unroll 2
+    for (int j = lane; j < jlim; j += 32) st(ob + j, sb[j * pstride]);
+  }
+}
+
+template <typename Elem, typename Store>
+__global__ void __launch_bounds__(kPermThreads)
+perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Elem* bufs = reinterpret_cast<Elem*>(smem_raw);
+  const size_t stage_elems = (size_t)P.nA * P.lap;
+  const int64_t first = blockIdx.x, step = gridDim.x;
+  const int64_t mine = first < P.ntiles ? (P.ntiles - 1 - first) / step + 1 : 0;
+  for (int k = 0; k < kStages - 1; ++k) {
+    if (k < mine) perm2d_issue<Elem>(P, in, bufs + (size_t)k * stage_elems, first + k * step);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int64_t k = 0; k < mine; ++k) {
+    const int stg = (int)(k % kStages);
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+    __syncthreads();
+    const int64_t nk = k + kStages - 1;
+    if (nk < mine) perm2d_issue<Elem>(P, in, bufs + (size_t)(nk % kStages) * stage_elems, first + nk * step);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    perm2d_store<Elem, Store>(P, bufs + (size_t)stg * stage_elems, first + k * step, st);
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Launches the pipelined kernel with a grid sized to the SM count.
 template <typename Elem, typename Store>
 int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream_t s) {
   if (P.ntiles <= 0) return 0;
   const size_t smem = perm_smem_bytes(P);
-  // TB_PERM_LOADS=async|bulk|auto selects the load mechanism (tuning knob;
-  // both produce identical results).  auto: bulk copies only for long rows.
+  // TB_PERM_LOADS=async|bulk|tables|auto selects the load mechanism (tuning
+  // knob; all produce identical results).  auto: bulk copies for long rows,
+  // the 2-D kernel for other 2-D tiles.
   static int mode = [] {
     const char* e = getenv("TB_PERM_LOADS");
     if (!e) return 0;
     if (!strcmp(e, "bulk")) return 1;
     if (!strcmp(e, "async")) return 2;
+    if (!strcmp(e, "tables")) return 3;  // the table-driven kernel even for 2-D tiles
     return 0;
   }();
   const bool eligible = P.tma_ok && ((uintptr_t)in % 16 == 0);
@@ -276,7 +356,19 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
   if (per_sm > 2048 / kPermThreads) per_sm = 2048 / kPermThreads;
   int64_t grid = (int64_t)num_sms() * per_sm;
   if (grid > P.ntiles) grid = P.ntiles;
-  if (bulk)
+  if (!bulk && P.lin2d && mode != 3) {
+    // two-dimensional tiles: no chunk tables in shared memory, so more CTAs fit
+    const size_t smem2 = (size_t)kStages * (size_t)perm_stage_bytes(P) + 128;
+    static bool attr2 = false;
+    if (!attr2) {
+      cudaFuncSetAttribute(perm2d_kernel<Elem, Store>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      attr2 = true;
+    }
+    int per2 = (int)((224 * 1024) / (smem2 + 1024));
+    per2 = std::max(1, std::min(per2, 2048 / kPermThreads));
+    int64_t grid2 = std::min<int64_t>((int64_t)num_sms() * per2, P.ntiles);
+    perm2d_kernel<Elem, Store><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
+  } else if (bulk)
     perm_pipe_kernel<Elem, Store, true><<<(unsigned)grid, kPermThreads, smem, s>>>(P, in, st, device_error_word());
   else
     perm_pipe_kernel<Elem, Store, false><<<(unsigned)grid, kPermThreads, smem, s>>>(P, in, st, device_error_word());

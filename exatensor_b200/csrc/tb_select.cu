@@ -1,0 +1,198 @@
+// tb_select.cpp -- contraction descriptors and the learned plan selector.
+//
+// The descriptor summarises what decides the speed of a contraction plan: the
+// matricized sizes M, N, K (log2), work and footprint, ranks, the smallest
+// extents of the row, column and contracted groups, whether L, R and D are
+// already in the TTGT matrix orders (no permutation pass needed), and the data
+// type.  The selector is a 3-layer MLP (trained by tb_mlp.cu's kernels on
+// autotuner timings) evaluated here on the host for each TB_METHOD_AUTO call:
+// a few tens of thousands of multiply-adds, far cheaper than a GPU round trip.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "tb_common.cuh"
+#include "tb_contract.h"
+#include "tb_pattern.h"
+
+namespace tb {
+namespace {
+
+float lg2(double v) { return (float)std::log2(v < 1.0 ? 1.0 : v); }
+
+// True when the tensor with these dims is already laid out as the TTGT matrix
+// whose fastest index groups are `first` then `second` (each in group order;
+// s1 of `first` and of `second` give the tensor's strides).
+bool in_matrix_order(const std::vector<MGroup>& first, const std::vector<MGroup>& second, bool first_s2,
+                     bool second_s2) {
+  int64_t expect = 1;
+  for (auto& g : first) {
+    if ((first_s2 ? g.s2 : g.s1) != expect) return false;
+    expect *= g.ext;
+  }
+  for (auto& g : second) {
+    if ((second_s2 ? g.s2 : g.s1) != expect) return false;
+    expect *= g.ext;
+  }
+  return true;
+}
+
+struct Selector {
+  std::mutex mu;
+  bool on = false;
+  int nh = 0;
+  std::vector<float> p, mean, scale;
+  float margin = 0.f;
+  int autotune = 0;
+  std::unordered_map<uint64_t, int> cache;
+};
+Selector& sel() {
+  static Selector S;
+  return S;
+}
+
+void mlp_host(const Selector& S, const float* x, float* y) {
+  const int F = TB_DESC_FEATURES, H = S.nh, O = TB_SELECT_PLANS;
+  const float* W1 = S.p.data();
+  const float* b1 = W1 + (size_t)F * H;
+  const float* W2 = b1 + H;
+  const float* b2 = W2 + (size_t)H * H;
+  const float* W3 = b2 + H;
+  const float* b3 = W3 + (size_t)H * O;
+  std::vector<float> xn(F), h1(H), h2(H);
+  for (int i = 0; i < F; ++i) xn[i] = (x[i] - S.mean[i]) / S.scale[i];
+  for (int o = 0; o < H; ++o) {
+    float a = b1[o];
+    for (int i = 0; i < F; ++i) a = std::fma(xn[i], W1[(size_t)i * H + o], a);
+    h1[o] = a > 0.f ? a : 0.f;
+  }
+  for (int o = 0; o < H; ++o) {
+    float a = b2[o];
+    for (int i = 0; i < H; ++i) a = std::fma(h1[i], W2[(size_t)i * H + o], a);
+    h2[o] = a > 0.f ? a : 0.f;
+  }
+  for (int o = 0; o < O; ++o) {
+    float a = b3[o];
+    for (int i = 0; i < H; ++i) a = std::fma(h2[i], W3[(size_t)i * O + o], a);
+    y[o] = a;
+  }
+}
+
+}  // namespace
+
+int descriptor_of(const Matricization& Z0, int dtk, float* f) {
+  Matricization Z = Z0;
+  const double M = (double)Z.M, N = (double)Z.N, K = (double)Z.K;
+  const double es = elem_bytes(dtk);
+  const bool cplx = is_complex(dtk);
+  auto minext = [](const std::vector<MGroup>& g) {
+    int64_t m = 0;
+    for (auto& x : g) m = m == 0 ? x.ext : std::min<int64_t>(m, x.ext);
+    return (double)(m ? m : 1);
+  };
+  // L as [M][K] with K fastest (contracted groups first), R as [N][K], D as [M][N]
+  std::vector<MGroup> kl = Z.k, kr = Z.k;
+  for (auto& g : kr) g.s1 = g.s2;  // R strides of the contracted groups
+  f[0] = lg2(M);
+  f[1] = lg2(N);
+  f[2] = lg2(K);
+  f[3] = lg2((cplx ? 8.0 : 2.0) * M * N * K);
+  f[4] = lg2((M * K + N * K + M * N) * es);
+  f[5] = (float)Z.drank;
+  f[6] = (float)Z.lrank;
+  f[7] = (float)Z.rrank;
+  f[8] = (float)Z.k.size();
+  f[9] = lg2(minext(Z.k));
+  f[10] = lg2(minext(Z.m));
+  f[11] = lg2(minext(Z.n));
+  f[12] = in_matrix_order(kl, Z.m, false, false) ? 1.f : 0.f;
+  f[13] = in_matrix_order(kr, Z.n, false, false) ? 1.f : 0.f;
+  f[14] = in_matrix_order(Z.m, Z.n, true, true) ? 1.f : 0.f;
+  f[15] = is_double(dtk) ? 1.f : 0.f;
+  return 0;
+}
+
+int selector_pick(const float* f, int* idx, bool* ambiguous, uint64_t* key) {
+  Selector& S = sel();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.on) return -1;
+  float y[TB_SELECT_PLANS];
+  mlp_host(S, f, y);
+  int best = 0, second = -1;
+  for (int i = 1; i < TB_SELECT_PLANS; ++i)
+    if (y[i] < y[best]) best = i;
+  for (int i = 0; i < TB_SELECT_PLANS; ++i)
+    if (i != best && (second < 0 || y[i] < y[second])) second = i;
+  *idx = best;
+  // key: the descriptor quantised to 1/64 (log2 units)
+  uint64_t h = 1469598103934665603ull;
+  for (int i = 0; i < TB_DESC_FEATURES; ++i) {
+    h ^= (uint64_t)(int64_t)std::lround(f[i] * 64.f);
+    h *= 1099511628211ull;
+  }
+  *key = h;
+  *ambiguous = S.autotune && second >= 0 && (y[second] - y[best]) < S.margin;
+  if (*ambiguous) {
+    auto it = S.cache.find(h);
+    if (it != S.cache.end()) { *idx = it->second; *ambiguous = false; }
+  }
+  return 0;
+}
+
+void selector_remember(uint64_t key, int idx) {
+  Selector& S = sel();
+  std::lock_guard<std::mutex> lk(S.mu);
+  S.cache[key] = idx;
+}
+
+}  // namespace tb
+
+using namespace tb;
+
+extern "C" int tb_contract_descriptor(const int* cptrn, int data_kind, int drank, const int* d_dims, int lrank,
+                                      const int* l_dims, int rrank, const int* r_dims, float* features) {
+  if (!cptrn || !features || !elem_bytes(data_kind)) { set_error("tb_contract_descriptor: bad arguments"); return TB_ERR_INVALID_ARGS; }
+  Matricization Z;
+  if (int e = matricize(cptrn, drank, d_dims, lrank, l_dims, rrank, r_dims, &Z)) {
+    set_error("tb_contract_descriptor: pattern does not match the shapes (code %d)", e);
+    return e;
+  }
+  return descriptor_of(Z, data_kind, features);
+}
+
+extern "C" int tb_selector_install(int n_hidden, const float* params, const float* mean, const float* scale,
+                                   float margin, int autotune) {
+  Selector& S = sel();
+  std::lock_guard<std::mutex> lk(S.mu);
+  S.cache.clear();
+  if (!params) { S.on = false; return 0; }
+  if (n_hidden < 1 || !mean || !scale) { set_error("tb_selector_install: bad arguments"); return TB_ERR_INVALID_ARGS; }
+  const int F = TB_DESC_FEATURES, O = TB_SELECT_PLANS;
+  const size_t n = (size_t)F * n_hidden + n_hidden + (size_t)n_hidden * n_hidden + n_hidden + (size_t)n_hidden * O + O;
+  S.p.assign(params, params + n);
+  S.mean.assign(mean, mean + F);
+  S.scale.assign(scale, scale + F);
+  for (auto& v : S.scale)
+    if (!(v > 0.f)) v = 1.f;
+  S.nh = n_hidden;
+  S.margin = margin;
+  S.autotune = autotune;
+  S.on = true;
+  return 0;
+}
+
+extern "C" int tb_selector_choose(const float* features, float* predicted) {
+  Selector& S = sel();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.on || !features) return -1;
+  float y[TB_SELECT_PLANS];
+  mlp_host(S, features, y);
+  int best = 0;
+  for (int i = 1; i < TB_SELECT_PLANS; ++i)
+    if (y[i] < y[best]) best = i;
+  if (predicted) std::memcpy(predicted, y, sizeof(y));
+  return best;
+}

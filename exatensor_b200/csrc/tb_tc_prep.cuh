@@ -289,13 +289,13 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kGThreads) gather_kernel(const __grid_constant__ GatherParams P) {
+__global__ void __launch_bounds__(kGThreads, 4) gather_kernel(const __grid_constant__ GatherParams P) {
   gather_body<MODE>(P, blockIdx.x, blockIdx.y, gridDim.y);
 }
 
 // Grouped form: CTA x works on row tile map[x].y of job map[x].x.
 template <int MODE>
-__global__ void __launch_bounds__(kGThreads) gather_grouped_kernel(const GatherParams* __restrict__ jobs,
+__global__ void __launch_bounds__(kGThreads, 4) gather_grouped_kernel(const GatherParams* __restrict__ jobs,
                                                                    const int2* __restrict__ map) {
   const int2 jm = map[blockIdx.x];
   const GatherParams P = jobs[jm.x];
@@ -321,23 +321,50 @@ __device__ __forceinline__ void rowmax_body(const GatherParams& P, int64_t rowti
   const int tid = threadIdx.x;
   if (tid < TM) sm_max[tid] = 0;
   const int64_t m0 = rowtile * TM;
+  const E* src = (const E*)P.src;
+  const int64_t nkt = (P.K + TK - 1) / TK;
+  if (!P.lanes_on_k) {
+    // rows contiguous in the source: each thread keeps one row (tid % TM) and
+    // walks k = tid / TM + j * (threads / TM) -- one offset, one maximum
+    constexpr int KS = kGThreads / TM;
+    const int mm = tid % TM;
+    const int64_t lm = m0 + mm < P.rows ? P.lm[m0 + mm] : -1;
+    unsigned e = 0;
+    if (lm >= 0) {
+      for (int64_t kt = ky; kt < nkt; kt += kstep) {
+        const int64_t k0 = kt * TK + tid / TM;
+#pragma unroll
+        for (int it = 0; it < TK / KS; ++it) {
+          const int64_t k = k0 + it * KS;
+          if (k < P.K) {
+            const E v = src[lm + P.lk[k]];
+            if constexpr (CPLX) e = max(e, max(exp_field(v.x), exp_field(v.y)));
+            else e = max(e, exp_field(v));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (e) atomicMax(&sm_max[mm], e);
+    __syncthreads();
+    if (tid < TM && sm_max[tid] && m0 + tid < P.rows) atomicMax(&P.rowE[m0 + tid], sm_max[tid]);
+    return;
+  }
   int64_t lmv[IT];
   unsigned emax[IT];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
     const int idx = tid + it * kGThreads;
-    const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+    const int mm = idx / TK;
     lmv[it] = m0 + mm < P.rows ? P.lm[m0 + mm] : -1;
     emax[it] = 0;
   }
-  const E* src = (const E*)P.src;
-  const int64_t nkt = (P.K + TK - 1) / TK;
   for (int64_t kt = ky; kt < nkt; kt += kstep) {
     const int64_t k0 = kt * TK;
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
       const int idx = tid + it * kGThreads;
-      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+      const int kk = idx % TK;
       if (lmv[it] >= 0 && k0 + kk < P.K) {
         const E v = src[lmv[it] + P.lk[k0 + kk]];
         if constexpr (CPLX) emax[it] = max(emax[it], max(exp_field(v.x), exp_field(v.y)));
@@ -349,7 +376,7 @@ __device__ __forceinline__ void rowmax_body(const GatherParams& P, int64_t rowti
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
     const int idx = tid + it * kGThreads;
-    const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+    const int mm = idx / TK;
     if (emax[it]) atomicMax(&sm_max[mm], emax[it]);
   }
   __syncthreads();

@@ -186,7 +186,8 @@ typedef struct {
 /* Builds the plan: distinct operand blocks, offset tables, tensor maps and the
  * work list (device memory owned by the plan; blocks must stay allocated).
  * beta = accumulative ? 1 : 0 applies to every output block once per execution.
- * plan may set slices (R8, 2..7, default 6) and tile_n (128 or 256). */
+ * plan may set slices (R8, 2..7, default 6; planes are allocated for
+ * max(slices, 6)) and tile_n (128 or 256). */
 int tb_bsc_plan_create(const char* pattern, int data_kind, int ntasks, const tb_block_task_t* tasks,
                        double alpha_real, double alpha_imag, int accumulative, const tb_plan_t* plan,
                        tb_bsc_plan_t** out, void* stream);
@@ -195,11 +196,54 @@ int tb_bsc_plan_create(const char* pattern, int data_kind, int ntasks, const tb_
 int tb_bsc_execute(tb_bsc_plan_t* plan, void* stream);
 /* The same launches queued directly on the stream (no graph). */
 int tb_bsc_execute_stream(tb_bsc_plan_t* plan, void* stream);
-/* Times the tile-width and slice-count candidates on the plan's data (with
- * alpha = 0, beta = 1, so D is unchanged) and keeps the fastest. */
+/* Times the tile-width candidates (and 6 vs 7 slices when the planes hold 7)
+ * on the plan's data, with alpha = 0 and beta = 1 so that D is unchanged, and
+ * keeps the fastest. */
 int tb_bsc_autotune(tb_bsc_plan_t* plan, void* stream);
 int tb_bsc_plan_info(const tb_bsc_plan_t* plan, tb_bsc_info_t* info);
 int tb_bsc_plan_destroy(tb_bsc_plan_t* plan);
+
+/* ---- learned plan selection ---------------------------------------------
+ * No counterpart in the reference, which always runs TTGT through cuBLAS.
+ * A contraction descriptor (TB_DESC_FEATURES floats) feeds a 3-layer MLP that
+ * predicts the log-runtime of each candidate plan (TTGT; tensor cores with
+ * N tiles 128 and 256); TB_METHOD_AUTO then takes the fastest predicted plan.
+ * Every candidate meets the accuracy bounds, so the choice changes speed, not
+ * what is computed beyond those bounds. */
+#define TB_DESC_FEATURES 16
+#define TB_SELECT_PLANS 3
+
+/* Descriptor of a contraction (host only, no GPU work). */
+int tb_contract_descriptor(const int* cptrn, int data_kind, int drank, const int* d_dims, int lrank,
+                           const int* l_dims, int rrank, const int* r_dims, float* features);
+
+/* The network: hand-written CUDA forward, backward (deterministic) and Adam
+ * kernels.  Parameters are W1 b1 W2 b2 W3 b3 with W_l stored [in][out]. */
+typedef struct tb_mlp_s tb_mlp_t;
+int tb_mlp_create(int n_in, int n_hidden, int n_out, int max_batch, uint64_t seed, tb_mlp_t** out);
+int tb_mlp_destroy(tb_mlp_t* net);
+long long tb_mlp_num_params(const tb_mlp_t* net);
+int tb_mlp_get_params(const tb_mlp_t* net, float* host, int grads);  /* grads != 0: last gradients */
+int tb_mlp_set_params(tb_mlp_t* net, const float* host);
+/* y[batch][n_out] = net(x[batch][n_in]); device pointers, asynchronous. */
+int tb_mlp_forward(tb_mlp_t* net, const float* x, int batch, float* y, void* stream);
+/* Mean squared error over the labelled targets (NaN = unlabelled) and its
+ * gradients for one batch (<= max_batch); *loss (host) if non-NULL syncs. */
+int tb_mlp_backward(tb_mlp_t* net, const float* x, const float* targets, int batch, float* loss, void* stream);
+int tb_mlp_adam_step(tb_mlp_t* net, float lr, float beta1, float beta2, float eps, void* stream);
+
+/* Installs a trained selector for TB_METHOD_AUTO: the parameters of a
+ * (TB_DESC_FEATURES -> hidden -> hidden -> TB_SELECT_PLANS) network and the
+ * feature normalisation (x - mean) / scale.  params = NULL removes it (the
+ * rule-based choice returns).  margin: when the two best predictions differ
+ * by less than this (in natural-log units) and autotune != 0, the library
+ * times both plans once (alpha = 0, beta = 1 runs, D unchanged) and caches
+ * the winner per descriptor. */
+int tb_selector_install(int n_hidden, const float* params, const float* mean, const float* scale, float margin,
+                        int autotune);
+/* The selector's choice for a descriptor: plan index (0 TTGT, 1 tensor cores
+ * N tile 128, 2 N tile 256) and the predicted log-runtimes (may be NULL). */
+int tb_selector_choose(const float* features, float* predicted);
 
 /* Seeded U[lo,hi) fill on the device (splitmix64 stream, 53-bit fractions);
  * complex kinds fill real and imaginary parts from consecutive draws. */

@@ -38,7 +38,7 @@ int main(int argc, char** argv) {
     for (int d = 0; d < rank; ++d) { long long x = r % dims[d]; r /= dims[d]; o += x * sout[d]; }
     ref[o] = i;
   }
-  std::vector<long long> out(vol, -1);
+  std::vector<long long> out(vol, -1), out2(P.lin2d ? vol : 0, -1);
   const int V = P.V, LA = P.LA, LB = P.LB;
   const long long bufn = (long long)P.nA * P.lap;
   std::vector<long long> buf(bufn, -1);
@@ -131,10 +131,41 @@ int main(int argc, char** argv) {
           }
         }
     }
+    // two-dimensional kernel replay (perm2d_kernel): rows, chunks and
+    // positions by formula instead of the chunk tables
+    if (P.lin2d) {
+      int rows = P.nA;
+      if (!full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = std::min(rows, rem_b);
+      for (int c = 0; c < P.nA; ++c) {
+        const bool tab_ok = !(!full && P.pb >= 0 && P.pb != P.pa) || P.ld_dpb[c] < rem_b;
+        if ((c < rows) != tab_ok) fail("2d row count", c, rows);
+        if (P.ld_base[c] != (long long)c * P.row_sin) fail("2d row stride", c, P.row_sin);
+      }
+      int chunks = P.nB;
+      if (!full && P.pa >= 0 && P.pa != P.pb && P.chunk_is_pa) chunks = std::min(chunks, rem_a);
+      const int qlim = (!full && P.pb >= 0) ? (P.pa == P.pb ? std::min(rem_a, rem_b) : rem_b) : (1 << 30);
+      const int jlim = std::min(LB, qlim);
+      for (int c = 0; c < P.nB; ++c) {
+        const bool tab_ok = !(!full && P.pa >= 0 && P.pa != P.pb) || P.st_dpa[c] < rem_a;
+        if ((c < chunks) != tab_ok) fail("2d chunk count", c, chunks);
+        if (c >= chunks) continue;
+        if (P.st_base[c] != (long long)c * P.chunk_sout || P.st_ebase[c] != c * P.chunk_eb) fail("2d chunk stride", c, 0);
+        for (int j = 0; j < jlim; ++j) {
+          const long long ee = (long long)c * P.chunk_eb + (long long)j * P.ej_pb_stride;
+          if (ee < 0 || ee >= bufn) fail("2d smem oob", ee, bufn);
+          const long long dst = out_base + (long long)c * P.chunk_sout + j;
+          if (dst < 0 || dst >= vol) fail("2d store oob", dst, tile);
+          if (buf[ee] < 0) fail("2d store reads unloaded smem", ee, tile);
+          if (out2[dst] != -1) fail("2d double write", dst, tile);
+          out2[dst] = buf[ee];
+        }
+      }
+    }
   }
   for (long long o = 0; o < vol; ++o) {
     if (out[o] != ref[o]) fail("wrong value at", o, out[o]);
+    if (P.lin2d && out2[o] != ref[o]) fail("2d wrong value at", o, out2[o]);
   }
-  printf("OK %lld %d %d %d tma=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok);
+  printf("OK %lld %d %d %d tma=%d lin2d=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok, P.lin2d);
   return 0;
 }
