@@ -27,5 +27,6 @@ int descriptor_of(const Matricization& Z, int dtk, float* features);
 // cache key of the descriptor.
 int selector_pick(const float* features, int* idx, bool* ambiguous, uint64_t* key);
 void selector_remember(uint64_t key, int idx);
+void selector_autoload();
 
 }  // namespace tb

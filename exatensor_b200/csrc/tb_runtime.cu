@@ -1,6 +1,7 @@
 // tb_runtime.cu -- device selection, error reporting, scratch memory, and the
 // elementwise kernels (init, scale, norms, seeded fill).
 #include "tb_common.cuh"
+#include "tb_contract.h"
 
 #include <cmath>
 #include <cstdarg>
@@ -247,6 +248,8 @@ extern "C" int tb_device_init(int gpu) {
     set_error("device %d is sm_%d%d; this library is built for sm_100a only", gpu, prop.major, prop.minor);
     return TB_ERR_NOT_IMPLEMENTED;
   }
+  // The learned plan selector shipped next to the library (if any).
+  selector_autoload();
   // Keep freed scratch in the pool between calls.
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, gpu) == cudaSuccess) {

@@ -7,9 +7,14 @@
 // type.  The selector is a 3-layer MLP (trained by tb_mlp.cu's kernels on
 // autotuner timings) evaluated here on the host for each TB_METHOD_AUTO call:
 // a few tens of thousands of multiply-adds, far cheaper than a GPU round trip.
+#include <dlfcn.h>
+
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -196,3 +201,61 @@ extern "C" int tb_selector_choose(const float* features, float* predicted) {
   if (predicted) std::memcpy(predicted, y, sizeof(y));
   return best;
 }
+
+// Weights file: "TBSEL001", int32 features, hidden, outputs, float32 margin,
+// int32 autotune, float32 mean[features], scale[features], then the network's
+// parameters (W1 b1 W2 b2 W3 b3).
+extern "C" int tb_selector_load(const char* path) {
+  if (!path) return TB_ERR_INVALID_ARGS;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { set_error("tb_selector_load: cannot open %s", path); return TB_ERR_INVALID_ARGS; }
+  char magic[8];
+  int32_t nf = 0, nh = 0, no = 0, at = 0;
+  float margin = 0.f;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "TBSEL001", 8) == 0 &&
+            std::fread(&nf, 4, 1, f) == 1 && std::fread(&nh, 4, 1, f) == 1 && std::fread(&no, 4, 1, f) == 1 &&
+            std::fread(&margin, 4, 1, f) == 1 && std::fread(&at, 4, 1, f) == 1 && nf == TB_DESC_FEATURES &&
+            no == TB_SELECT_PLANS && nh > 0 && nh <= 4096;
+  std::vector<float> mean(nf > 0 ? nf : 0), scale(nf > 0 ? nf : 0), p;
+  if (ok) {
+    const size_t n = (size_t)nf * nh + nh + (size_t)nh * nh + nh + (size_t)nh * no + no;
+    p.resize(n);
+    ok = std::fread(mean.data(), 4, nf, f) == (size_t)nf && std::fread(scale.data(), 4, nf, f) == (size_t)nf &&
+         std::fread(p.data(), 4, n, f) == n;
+  }
+  std::fclose(f);
+  if (!ok) { set_error("tb_selector_load: %s is not a selector weights file", path); return TB_ERR_INVALID_ARGS; }
+  return tb_selector_install(nh, p.data(), mean.data(), scale.data(), margin, at);
+}
+
+namespace tb {
+// Installs the weights shipped next to the library (selector_weights.bin)
+// unless a selector is already installed; TB_SELECTOR=0 disables this and
+// TB_SELECTOR=<path> names another file.  Called by tb_device_init.
+void selector_autoload() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const char* env = std::getenv("TB_SELECTOR");
+    if (env && std::strcmp(env, "0") == 0) return;
+    {
+      Selector& S = sel();
+      std::lock_guard<std::mutex> lk(S.mu);
+      if (S.on) return;
+    }
+    std::string path;
+    if (env && *env) {
+      path = env;
+    } else {
+      Dl_info info;
+      if (!dladdr((void*)&tb_selector_load, &info) || !info.dli_fname) return;
+      path = info.dli_fname;
+      const size_t slash = path.rfind('/');
+      path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/selector_weights.bin";
+    }
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return;
+    std::fclose(f);
+    if (tb_selector_load(path.c_str())) set_error("");  // a bad file leaves the size rule in place
+  });
+}
+}  // namespace tb

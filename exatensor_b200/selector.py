@@ -205,17 +205,39 @@ def evaluate(log_ms, choice):
             "picked_best": float(np.mean(c == t.argmin(axis=1)))}
 
 
+def save_weights(path, params, mean, scale, hidden=128, margin=0.0, autotune=0):
+    """Writes a weights file for tb_selector_load / automatic loading."""
+    import struct
+    with open(path, "wb") as f:
+        f.write(b"TBSEL001")
+        f.write(struct.pack("<iiifi", NFEAT, hidden, len(PLANS), float(margin), int(autotune)))
+        f.write(np.asarray(mean, "<f4").tobytes())
+        f.write(np.asarray(scale, "<f4").tobytes())
+        f.write(np.asarray(params, "<f4").tobytes())
+
+
 def main(argv=None):
     import argparse
     import sys
     ap = argparse.ArgumentParser(description="selector corpus labelling and training")
-    ap.add_argument("cmd", choices=["label"])
+    ap.add_argument("cmd", choices=["label", "train"])
+    ap.add_argument("--corpus", default=None, help="train: labelled corpus (.npz)")
+    ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--n", type=int, default=20000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--start", type=int, default=0)
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--out", required=True, help="label: corpus .npz; train: weights file")
     a = ap.parse_args(argv)
-    label_corpus(a.n, a.seed, a.out, log=sys.stdout, start=a.start)
+    if a.cmd == "label":
+        label_corpus(a.n, a.seed, a.out, reps=a.reps, log=sys.stdout, start=a.start)
+        return
+    d = np.load(a.corpus)
+    params, mean, scale, hist = train(d["features"], d["log_ms"], hidden=128, epochs=a.epochs, seed=a.seed,
+                                      log_every=max(1, a.epochs // 10))
+    save_weights(a.out, params, mean, scale)
+    for ep, loss in hist:
+        print(f"epoch {ep} loss {loss:.4f}")
 
 
 if __name__ == "__main__":

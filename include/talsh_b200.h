@@ -244,6 +244,11 @@ int tb_selector_install(int n_hidden, const float* params, const float* mean, co
 /* The selector's choice for a descriptor: plan index (0 TTGT, 1 tensor cores
  * N tile 128, 2 N tile 256) and the predicted log-runtimes (may be NULL). */
 int tb_selector_choose(const float* features, float* predicted);
+/* Installs a selector from a weights file ("TBSEL001" header, features,
+ * hidden, outputs, margin, autotune, mean, scale, parameters).  tb_device_init
+ * loads selector_weights.bin from the library's directory when present
+ * (TB_SELECTOR=0 disables this, TB_SELECTOR=<path> names another file). */
+int tb_selector_load(const char* path);
 
 /* Seeded U[lo,hi) fill on the device (splitmix64 stream, 53-bit fractions);
  * complex kinds fill real and imaginary parts from consecutive draws. */
