@@ -2,6 +2,7 @@
 #include "tb_perm_plan.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -34,7 +35,15 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   std::stable_sort(Q.begin(), Q.end(), [&](int x, int y) { return SO[x] < SO[y]; });
   if (SO[Q[0]] != 1) return TB_ERR_NOT_IMPLEMENTED;
   const int64_t T = std::max<int64_t>(1, 256 / es);
-  const int64_t Vmin = 16384 / es, Vmax = 32768 / es;
+  // tile volume bounds (bytes; 16 KB .. 32 KB unless TB_PERM_VMIN_KB /
+  // TB_PERM_VMAX_KB say otherwise -- tuning knobs that leave results unchanged)
+  auto knob = [](const char* name, long dflt) {
+    const char* e = std::getenv(name);
+    const long v = e ? std::atol(e) : 0;
+    return (int64_t)(v >= 4 && v <= 96 ? v : dflt) * 1024;
+  };
+  static const int64_t vmin_bytes = knob("TB_PERM_VMIN_KB", 16), vmax_bytes = knob("TB_PERM_VMAX_KB", 32);
+  const int64_t Vmax = std::max<int64_t>(1, vmax_bytes / es), Vmin = std::min(Vmax, std::max<int64_t>(1, vmin_bytes / es));
   std::vector<int64_t> t(r, 1);
   auto cdiv = [](int64_t x, int64_t y) { return (x + y - 1) / y; };
   // Even split: the smallest extent >= want that tiles D in the same number

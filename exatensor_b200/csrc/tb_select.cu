@@ -139,7 +139,9 @@ int selector_pick(const float* f, int* idx, bool* ambiguous, uint64_t* key) {
     h *= 1099511628211ull;
   }
   *key = h;
-  *ambiguous = S.autotune && second >= 0 && (y[second] - y[best]) < S.margin;
+  // timing the candidates costs a few contractions: only worth it for large ones
+  constexpr float kTuneMinLog2Flops = 34.0f;  // about 1.7e10 FLOP
+  *ambiguous = S.autotune && second >= 0 && (y[second] - y[best]) < S.margin && f[3] >= kTuneMinLog2Flops;
   if (*ambiguous) {
     auto it = S.cache.find(h);
     if (it != S.cache.end()) { *idx = it->second; *ambiguous = false; }

@@ -223,6 +223,8 @@ def main(argv=None):
     ap.add_argument("cmd", choices=["label", "train"])
     ap.add_argument("--corpus", default=None, help="train: labelled corpus (.npz)")
     ap.add_argument("--epochs", type=int, default=150)
+    ap.add_argument("--margin", type=float, default=0.25, help="train: ln-time margin below which AUTO times plans")
+    ap.add_argument("--autotune", type=int, default=1)
     ap.add_argument("--n", type=int, default=20000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--start", type=int, default=0)
@@ -235,7 +237,7 @@ def main(argv=None):
     d = np.load(a.corpus)
     params, mean, scale, hist = train(d["features"], d["log_ms"], hidden=128, epochs=a.epochs, seed=a.seed,
                                       log_every=max(1, a.epochs // 10))
-    save_weights(a.out, params, mean, scale)
+    save_weights(a.out, params, mean, scale, margin=a.margin, autotune=a.autotune)
     for ep, loss in hist:
         print(f"epoch {ep} loss {loss:.4f}")
 

@@ -112,15 +112,25 @@ def test_auto_uses_the_installed_selector(xt, dev):
             assert O.rel_frobenius(got, exact) <= 1e-12
         finally:
             XB.selector_install(0, None, None, None)
-    # autotune fallback: equal predictions are ambiguous for any margin > 0
+    # autotune fallback (large contractions only): equal predictions are
+    # ambiguous for any margin > 0, so every candidate is timed once with
+    # alpha = 0, beta = 1; D must come out as one plain contraction would make it
+    pattern2, m = "D(i,j)+=L(k,i)*R(k,j)", 2048
+    d2, l2, r2 = rand_host(O.R8, m * m, 4), rand_host(O.R8, m * m, 5), rand_host(O.R8, m * m, 6)
+    dd, ld, rd = dev.put(d2), dev.put(l2), dev.put(r2)
+    xt.tensor_contract(pattern2, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(), 1.0,
+                       plan=xt.make_plan(XB.METHOD_TTGT), stream=dev.stream())
+    want = dev.get(dd, np.float64, d2.size)
     XB.selector_install(nh, np.zeros(n, np.float32), np.zeros(16, np.float32), np.ones(16, np.float32),
                         margin=0.5, autotune=True)
     try:
-        dd, ld, rd = dev.put(d), dev.put(l), dev.put(r)
-        xt.tensor_contract(pattern, O.R8, ddims, dd.data_ptr(), ldims, ld.data_ptr(), rdims, rd.data_ptr(), 1.0,
-                           stream=dev.stream())
-        got = dev.get(dd, np.float64, d.size)
-        assert O.rel_frobenius(got, exact) <= 1e-12
+        for _ in range(2):  # the second call takes the cached decision
+            dd = dev.put(d2)
+            xt.tensor_contract(pattern2, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(),
+                               1.0, stream=dev.stream())
+            got = dev.get(dd, np.float64, d2.size)
+            assert xt.last_contract_stats().method in (XB.METHOD_TTGT, XB.METHOD_FUSED)
+            assert O.rel_frobenius(got, want) <= 1e-12
     finally:
         XB.selector_install(0, None, None, None)
     xt.device_check(dev.stream())
