@@ -123,6 +123,19 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     }
     if (!grown) break;
   }
+  // 5a. a partial load-block dimension gets rows of whole 16-byte units where
+  // the extent allows (so that rows can move as 16-byte copies)
+  if (t[a] < D[a]) {
+    int64_t pA = 1;
+    for (int i = 0; i < a; ++i) pA *= D[i];
+    int64_t m = 16, x = pA * es;
+    while (x % 2 == 0 && m > 1) { x /= 2; m /= 2; }  // m = 16 / gcd(pA*es, 16)
+    const int64_t up = cdiv(t[a], m) * m;
+    if (up <= D[a] && up != t[a]) {
+      const int64_t Vn = vol_of() / t[a] * up;
+      if (Vn <= Vmax) t[a] = up;
+    }
+  }
   // 5. bulk-copy alignment: when the load block ends on a whole dimension and
   // its rows are not a multiple of 16 bytes, extend it into the next input
   // dimension by the smallest extent that makes them so (shrinking the store
@@ -156,12 +169,19 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   // row stride is padded so that transposed reads (consecutive output
   // elements one row apart) spread over the banks: an odd number of 4-byte
   // words per row, or for bulk-copy rows an odd number of 16-byte units.
+  // Rows of whole 8-byte units (4-byte elements) use an odd number of
+  // 8-byte units per row instead, so that 8-byte copies stay aligned.
   const bool bulk_rows = (LA * es) % 16 == 0;
+  const bool rows8 = !bulk_rows && es < 8 && (LA * es) % 8 == 0;
   int64_t lap;
   if (bulk_rows) {
     const int64_t u = 16 / es;  // elements per 16 bytes (>= 1)
     lap = LA;
     if (((lap * es) / 16) % 2 == 0) lap += u;
+  } else if (rows8) {
+    const int64_t u = 8 / es;
+    lap = LA;
+    if (((lap * es) / 8) % 2 == 0) lap += u;
   } else {
     lap = (LA % 2 == 1) ? LA : LA + 1;
   }
@@ -199,6 +219,10 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     bool ok = bulk_rows && (tot * es) % 16 == 0 && (prodA * t[a] * es) % 16 == 0;
     for (int i = a + 1; i < r; ++i) if ((SI[i] * es) % 16 != 0) ok = false;
     P.tma_ok = ok ? 1 : 0;
+    // the same for 8-byte copies of 4-byte elements
+    bool ok8 = rows8 && (tot * es) % 8 == 0 && (prodA * t[a] * es) % 8 == 0;
+    for (int i = a + 1; i < r; ++i) if ((SI[i] * es) % 8 != 0) ok8 = false;
+    P.vec8 = ok8 ? 1 : 0;
   }
   for (int i = 0; i < r; ++i) { P.dims[i] = D[i]; P.tile[i] = t[i]; P.sin[i] = SI[i]; P.sout[i] = SO[i]; }
   magic32((uint32_t)LA, &P.la_magic, &P.la_shift);
@@ -230,15 +254,29 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   P.row_sin = restA.empty() ? 0 : SI[restA[0]];
   P.chunk_sout = restB.empty() ? 0 : SO[restB[0]];
   P.chunk_eb = restB.empty() ? 0 : (int32_t)est[restB[0]];
+  P.vbytes = P.tma_ok ? 16 : (P.vec8 ? 8 : 0);
+  P.vec2d = (P.lin2d && P.vbytes && es <= P.vbytes && P.chunk_eb == 1 &&
+             (P.ej_pb_stride * (int64_t)es) % P.vbytes == 0 && nB <= LA && (LA * es) % P.vbytes == 0) ? 1 : 0;
+  P.nvec = P.vbytes ? (int)((LA * es + P.vbytes - 1) / P.vbytes) : 0;
+  magic32((uint32_t)std::max(1, P.nvec), &P.nv_magic, &P.nv_shift);
   // positions inside a store chunk: store-block dims before blast
   for (int64_t j = 0; j < prodB; ++j) {
     int64_t x = j, e = 0;
     for (int d : Bdims) { if (d == blast) continue; int64_t dg = x % t[d]; x /= t[d]; e += dg * est[d]; }
     P.ejf[j] = (int32_t)e;
   }
-  // 6. tile grid
+  // 6. tile grid: consecutive tiles step along the dims in output order, so
+  // that the CTAs running at one time write neighbouring output runs (the
+  // write side of a permutation is the less forgiving one; measured +15% on
+  // rank-4 R8 permutations over input order).  TB_PERM_GRID=in selects input
+  // order (a tuning knob; results are identical).
+  static const bool grid_out = [] {
+    const char* e = std::getenv("TB_PERM_GRID");
+    return !(e && std::strcmp(e, "in") == 0);
+  }();
   int g = 0; int64_t nt = 1;
-  for (int i = 0; i < r; ++i) {
+  for (int jj = 0; jj < r; ++jj) {
+    const int i = grid_out ? Q[jj] : jj;
     const int64_t ext = cdiv(D[i], t[i]);
     if (ext > 1) { P.gdim[g] = i; P.gext[g] = ext; P.gdiv[g].init((uint64_t)ext); ++g; nt *= ext; }
   }

@@ -59,6 +59,14 @@ struct PermParams {
   int row_is_pb, chunk_is_pa;   // the row (chunk) dim is the partial dim pb (pa)
   int64_t row_sin, chunk_sout;
   int32_t chunk_eb;
+  // 2-D tiles whose store chunks are adjacent columns of vector-aligned rows
+  // (chunk_eb == 1): the store phase reads vbytes (vbytes / es columns) per
+  // lane and the load phase walks (row, vector) pairs.
+  int vec2d;
+  int vec8;                     // 4-byte elements: rows move as 8-byte copies (tma_ok: 16-byte)
+  int vbytes;                   // vector bytes of the 2-D path: 16, 8 or 0
+  int nvec;                     // vectors per full load row
+  uint32_t nv_magic; int nv_shift;  // fast division by nvec
 };
 
 // Host-side plan builder.  dims/sin/sout describe the input dims (input

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 namespace tb {
 
@@ -109,8 +110,10 @@ __device__ __forceinline__ void perm_issue(const PermParams& P, const PermSmem& 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kW = kPermThreads / 32, kU = 4;  // copies per lane per unit
     const bool vec = P.tma_ok && sizeof(Elem) < 16;
+    const bool vec8 = !vec && P.vec8 && sizeof(Elem) < 8;
     constexpr int VW = sizeof(Elem) < 16 ? 16 / sizeof(Elem) : 1;
-    const int w = vec ? VW : 1;                        // elements per copy
+    constexpr int VW8 = sizeof(Elem) < 8 ? 8 / sizeof(Elem) : 1;
+    const int w = vec ? VW : (vec8 ? VW8 : 1);         // elements per copy
     const int nvec = (len + w - 1) / w;                // copies per row (vector rows round up)
     const int nseg = (nvec + 32 * kU - 1) / (32 * kU);
     const int units = P.nA * nseg;
@@ -126,6 +129,9 @@ __device__ __forceinline__ void perm_issue(const PermParams& P, const PermSmem& 
         const int j = v * w;
         if (vec || sizeof(Elem) == 16)
           asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst + j)), "l"(src + j)
+                       : "memory");
+        else if (vec8)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst + j)), "l"(src + j)
                        : "memory");
         else
           asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst + j)), "l"(src + j),
@@ -266,8 +272,10 @@ __device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int kW = kPermThreads / 32;
   const bool vec = P.tma_ok && sizeof(Elem) < 16;
+  const bool vec8 = !vec && P.vec8 && sizeof(Elem) < 8;
   constexpr int VW = sizeof(Elem) < 16 ? 16 / sizeof(Elem) : 1;
-  const int w = vec ? VW : 1;
+  constexpr int VW8 = sizeof(Elem) < 8 ? 8 / sizeof(Elem) : 1;
+  const int w = vec ? VW : (vec8 ? VW8 : 1);
   const int nvec = (len + w - 1) / w;
   for (int r = warp; r < rows; r += kW) {
     const Elem* src = in + o.in_base + (int64_t)r * P.row_sin;
@@ -276,6 +284,8 @@ __device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in
       const int j = v * w;
       if (vec || sizeof(Elem) == 16)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst + j)), "l"(src + j) : "memory");
+      else if (vec8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst + j)), "l"(src + j) : "memory");
       else
         asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst + j)), "l"(src + j),
                      "n"(sizeof(Elem))
@@ -302,16 +312,89 @@ __device__ __forceinline__ void perm2d_store(const PermParams& P, const Elem* st
   }
 }
 
-template <typename Elem, typename Store>
+// Vectorised 2-D tiles (PermParams::vec2d): the load phase walks (row,
+// 16-byte vector) pairs over the whole CTA, and the store phase gives each
+// lane 16 / es adjacent columns (= store chunks) of one row: one 16-byte
+// shared-memory read feeds 16 / es output runs, and consecutive lanes take
+// consecutive rows, i.e. consecutive positions of those runs.  Rows are an
+// odd number of 16-byte units long, so a warp's 16-byte reads of one column
+// group spread over all banks.  The tile's store bounds are computed by
+// thread 0 when the tile is issued and kept in shared memory until its store.
+struct Perm2dHdr {
+  int64_t out_base;
+  int chunks, jlim;
+};
+
+template <typename Elem, int VB>
+__device__ __forceinline__ void perm2dv_issue(const PermParams& P, const Elem* in, Elem* stage, int64_t tile,
+                                              Perm2dHdr* hdr) {
+  const TileOrigin o = tile_origin(P, tile);
+  int len = P.LA;
+  if (!o.full && P.pa >= 0) len = P.prodA * (P.pb == P.pa ? min(o.rem_a, o.rem_b) : o.rem_a);
+  int rows = P.nA;
+  if (!o.full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = min(rows, o.rem_b);
+  if (threadIdx.x == 0) {
+    const int qlim = (!o.full && P.pb >= 0) ? (P.pa == P.pb ? min(o.rem_a, o.rem_b) : o.rem_b) : (1 << 30);
+    int chunks = P.nB;
+    if (!o.full && P.pa >= 0 && P.pa != P.pb && P.chunk_is_pa) chunks = min(chunks, o.rem_a);
+    hdr->out_base = o.out_base;
+    hdr->chunks = chunks;
+    hdr->jlim = min(P.LB, qlim);
+  }
+  constexpr int VW = VB / (int)sizeof(Elem);
+  const int nv = (len + VW - 1) / VW;  // valid vectors of a row in this tile
+  const int total = rows * P.nvec;
+  const Elem* src0 = in + o.in_base;
+  for (int v = threadIdx.x; v < total; v += kPermThreads) {
+    const int r = (int)fdiv32((uint32_t)v, P.nv_magic, P.nv_shift);
+    const int x = v - r * P.nvec;
+    if (x >= nv) continue;
+    const Elem* src = src0 + (int64_t)r * P.row_sin + x * VW;
+    Elem* dst = stage + (size_t)r * P.lap + x * VW;
+    if (VB == 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+  }
+}
+
+template <typename Elem, typename Store, int VB>
+__device__ __forceinline__ void perm2dv_store(const PermParams& P, const Elem* stage, const Perm2dHdr& h,
+                                              const Store& st) {
+  constexpr int VW = VB / (int)sizeof(Elem);
+  using V = typename std::conditional<VB == 16, uint4, uint2>::type;
+  const int groups = (h.chunks + VW - 1) / VW;
+  const int total = groups * P.LB;
+  const int pstride = P.ej_pb_stride;
+  for (int e = threadIdx.x; e < total; e += kPermThreads) {
+    const int g = (int)fdiv32((uint32_t)e, P.lb_magic, P.lb_shift);
+    const int j = e - g * P.LB;
+    if (j >= h.jlim) continue;
+    const int c0 = g * VW;
+    union { V q; Elem v[VW]; } u;
+    u.q = *reinterpret_cast<const V*>(stage + (size_t)j * pstride + c0);
+    const int64_t ob = h.out_base + j;
+#pragma unroll
+    for (int t = 0; t < VW; ++t)
+      if (c0 + t < h.chunks) st(ob + (int64_t)(c0 + t) * P.chunk_sout, u.v[t]);
+  }
+}
+
+template <typename Elem, typename Store, int VB>  // VB: vector bytes of the vectorised path, 0 = scalar
 __global__ void __launch_bounds__(kPermThreads)
 perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st) {
+  constexpr bool VEC = VB > 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ Perm2dHdr hdr[kStages];
   Elem* bufs = reinterpret_cast<Elem*>(smem_raw);
   const size_t stage_elems = (size_t)P.nA * P.lap;
   const int64_t first = blockIdx.x, step = gridDim.x;
   const int64_t mine = first < P.ntiles ? (P.ntiles - 1 - first) / step + 1 : 0;
   for (int k = 0; k < kStages - 1; ++k) {
-    if (k < mine) perm2d_issue<Elem>(P, in, bufs + (size_t)k * stage_elems, first + k * step);
+    if (k < mine) {
+      if (VEC) perm2dv_issue<Elem, VB ? VB : 16>(P, in, bufs + (size_t)k * stage_elems, first + k * step, &hdr[k]);
+      else perm2d_issue<Elem>(P, in, bufs + (size_t)k * stage_elems, first + k * step);
+    }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
   for (int64_t k = 0; k < mine; ++k) {
@@ -319,9 +402,14 @@ perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in,
     asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
     __syncthreads();
     const int64_t nk = k + kStages - 1;
-    if (nk < mine) perm2d_issue<Elem>(P, in, bufs + (size_t)(nk % kStages) * stage_elems, first + nk * step);
+    const int nstg = (int)(nk % kStages);
+    if (nk < mine) {
+      if (VEC) perm2dv_issue<Elem, VB ? VB : 16>(P, in, bufs + (size_t)nstg * stage_elems, first + nk * step, &hdr[nstg]);
+      else perm2d_issue<Elem>(P, in, bufs + (size_t)nstg * stage_elems, first + nk * step);
+    }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    perm2d_store<Elem, Store>(P, bufs + (size_t)stg * stage_elems, first + k * step, st);
+    if (VEC) perm2dv_store<Elem, Store, VB ? VB : 16>(P, bufs + (size_t)stg * stage_elems, hdr[stg], st);
+    else perm2d_store<Elem, Store>(P, bufs + (size_t)stg * stage_elems, first + k * step, st);
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
@@ -340,6 +428,7 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
     if (!strcmp(e, "bulk")) return 1;
     if (!strcmp(e, "async")) return 2;
     if (!strcmp(e, "tables")) return 3;  // the table-driven kernel even for 2-D tiles
+    if (!strcmp(e, "scalar2d")) return 4;  // the 2-D kernel without 16-byte column groups
     return 0;
   }();
   const bool eligible = P.tma_ok && ((uintptr_t)in % 16 == 0);
@@ -361,13 +450,22 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
     const size_t smem2 = (size_t)kStages * (size_t)perm_stage_bytes(P) + 128;
     static bool attr2 = false;
     if (!attr2) {
-      cudaFuncSetAttribute(perm2d_kernel<Elem, Store>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      cudaFuncSetAttribute(perm2d_kernel<Elem, Store, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      cudaFuncSetAttribute(perm2d_kernel<Elem, Store, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      if (sizeof(Elem) <= 8)
+        cudaFuncSetAttribute(perm2d_kernel<Elem, Store, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
       attr2 = true;
     }
     int per2 = (int)((224 * 1024) / (smem2 + 1024));
     per2 = std::max(1, std::min(per2, 2048 / kPermThreads));
     int64_t grid2 = std::min<int64_t>((int64_t)num_sms() * per2, P.ntiles);
-    perm2d_kernel<Elem, Store><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
+    const bool vec = P.vec2d && (uintptr_t)in % (uintptr_t)P.vbytes == 0 && mode != 4;
+    if (vec && P.vbytes == 16)
+      perm2d_kernel<Elem, Store, 16><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
+    else if (vec && P.vbytes == 8 && sizeof(Elem) <= 8)
+      perm2d_kernel<Elem, Store, (sizeof(Elem) <= 8 ? 8 : 16)><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
+    else
+      perm2d_kernel<Elem, Store, 0><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
   } else if (bulk)
     perm_pipe_kernel<Elem, Store, true><<<(unsigned)grid, kPermThreads, smem, s>>>(P, in, st, device_error_word());
   else

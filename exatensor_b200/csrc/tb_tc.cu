@@ -319,6 +319,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       stats->slices = S;
       stats->passes = (int)passes.size();
       stats->products = nplane_products;
+      stats->tile_n = BN;
       stats->gemm_launches = 1;
       stats->m = M; stats->n = Nr; stats->k = Kr;
     }

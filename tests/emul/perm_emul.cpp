@@ -82,21 +82,24 @@ int main(int argc, char** argv) {
         buf[p] = src;
       }
     }
-    if (P.tma_ok) {
-      // bulk-copy replay: each valid row is copied with its byte length rounded
-      // up to 16; the copy must stay inside the tensor and inside its smem row
+    if (P.tma_ok || P.vec8) {
+      // vector-copy replay: each valid row is copied with its byte length
+      // rounded up to the vector (16 bytes, or 8 for vec8); the copy must stay
+      // inside the tensor and inside its smem row, both ends aligned
+      const long long vb = P.tma_ok ? 16 : 8;
+      if (P.vec8 && (es >= 8 || P.tma_ok)) fail("vec8 with wide elements or tma", es, P.tma_ok);
       for (int c = 0; c < P.nA; ++c) {
         bool ok = true;
         if (!full && P.pb >= 0 && P.pb != P.pa) ok = P.ld_dpb[c] < rem_b;
         if (!ok) continue;
         long long len = (!full && P.pa >= 0) ? (long long)P.prodA * std::min(rem_a, P.pb == P.pa ? rem_b : rem_a)
                                               : (long long)LA;
-        long long bytes = (len * es + 15) / 16 * 16;
+        long long bytes = (len * es + vb - 1) / vb * vb;
         long long src = in_base + P.ld_base[c];
-        if ((src * es) % 16 != 0) fail("bulk source misaligned", src, c);
-        if (src * es + bytes > vol * es) fail("bulk copy leaves the tensor", src, bytes);
-        if (bytes > (long long)P.lap * es) fail("bulk copy overflows its row", bytes, P.lap);
-        if (((long long)c * P.lap * es) % 16 != 0) fail("bulk destination misaligned", c, P.lap);
+        if ((src * es) % vb != 0) fail("vector source misaligned", src, c);
+        if (src * es + bytes > vol * es) fail("vector copy leaves the tensor", src, bytes);
+        if (bytes > (long long)P.lap * es) fail("vector copy overflows its row", bytes, P.lap);
+        if (((long long)c * P.lap * es) % vb != 0) fail("vector destination misaligned", c, P.lap);
       }
     }
     // store phase as perm_store: 8 warps, (chunk, block) units, strided positions
@@ -133,6 +136,21 @@ int main(int argc, char** argv) {
     }
     // two-dimensional kernel replay (perm2d_kernel): rows, chunks and
     // positions by formula instead of the chunk tables
+    if (P.vec2d) {
+      // 16-byte column groups: the widest group read stays inside a row, rows
+      // and groups are 16-byte aligned, and full-row vectors fit the row
+      const int VB = P.vbytes, VW = VB / es;
+      if (VB != 16 && VB != 8) fail("vec2d vector bytes", VB, 0);
+      if (VW < 1) fail("vec2d element wider than the vector", es, VB);
+      if (!P.lin2d || P.chunk_eb != 1) fail("vec2d without unit chunk step", P.chunk_eb, 0);
+      if ((long long)((P.nB + VW - 1) / VW) * VW > P.lap) fail("vec2d group beyond row", P.nB, P.lap);
+      if (((long long)P.ej_pb_stride * es) % VB || ((long long)P.lap * es) % VB) fail("vec2d row alignment", P.lap, 0);
+      if ((long long)P.nvec * VB > (long long)P.lap * es) fail("vec2d vectors beyond row", P.nvec, P.lap);
+      if (P.nvec != (P.LA * es + VB - 1) / VB) fail("vec2d nvec", P.nvec, P.LA);
+      if (!(VB == 16 ? P.tma_ok : P.vec8)) fail("vec2d without aligned copies", VB, 0);
+      for (int v = 0; v < P.nA * P.nvec; v += 7)
+        if ((int)fdiv32((uint32_t)v, P.nv_magic, P.nv_shift) != v / P.nvec) fail("fdiv32 nvec", v, P.nvec);
+    }
     if (P.lin2d) {
       int rows = P.nA;
       if (!full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = std::min(rows, rem_b);
@@ -166,6 +184,6 @@ int main(int argc, char** argv) {
     if (out[o] != ref[o]) fail("wrong value at", o, out[o]);
     if (P.lin2d && out2[o] != ref[o]) fail("2d wrong value at", o, out2[o]);
   }
-  printf("OK %lld %d %d %d tma=%d lin2d=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok, P.lin2d);
+  printf("OK %lld %d %d %d tma=%d lin2d=%d vec2d=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok, P.lin2d, P.vec2d);
   return 0;
 }
