@@ -143,19 +143,24 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   {
     int64_t pA = 1;
     for (int i = 0; i < a; ++i) pA *= D[i];
-    if ((pA * t[a] * es) % 16 != 0 && t[a] == D[a] && a + 1 < r) {
+    // rows of whole 8-byte units of 4-byte elements move as 8-byte copies:
+    // no need to grow the load block for them
+    const bool rows8_ok = es < 8 && (pA * t[a] * es) % 8 == 0;
+    if ((pA * t[a] * es) % 16 != 0 && !rows8_ok && t[a] == D[a] && a + 1 < r) {
       const int64_t pA2 = pA * D[a];
       int64_t g = 16, x = pA2 * es;
       while (x % 2 == 0 && g > 1) { x /= 2; g /= 2; }  // g = 16 / gcd(pA2*es, 16)
       int64_t nt = t[a + 1] > 1 ? cdiv(t[a + 1], g) * g : g;
       if (nt <= D[a + 1]) {
         int64_t Vn = vol_of() / t[a + 1] * nt;
+        const int64_t tblast0 = blast >= 0 ? t[blast] : 0;
         if (Vn > Vmax && blast > a + 1 && t[blast] > 1) {  // only a store dim outside the load block
           const int64_t pBfull = [&]() { int64_t p = 1; for (int j = 0; j < r; ++j) if (inB[j] && j != blast) p *= t[j]; return p; }();
           const int64_t tb = std::max<int64_t>(cdiv(T, pBfull), t[blast] * Vmax / Vn);
           if (tb < t[blast]) { t[blast] = tb; Vn = vol_of() / t[a + 1] * nt; }
         }
         if (Vn <= Vmax) { t[a + 1] = nt; a = a + 1; }
+        else if (blast >= 0) t[blast] = tblast0;  // extension rejected: keep the store block as it was
       }
     }
   }
