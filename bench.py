@@ -562,7 +562,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if wl["dtk"] == 8 else "f32",
             "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v, D=0)",
             "config": {"workload": f"{args.workload}: {wl['pattern']} v={wl['v']} o={wl['o']}",
-                       "method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products,
+                       "method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products, "tile_n": st.tile_n,
                        "l2": "inputs larger than L2 (V alone is 10.9 GB)", "parallelism": f"replicas x{world}"},
             "plain": {"value": round(plain, 3), "unit": "TFLOP/s", "method": "ttgt (permute + FP64 DMMA GEMM)",
                       "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),
@@ -623,7 +623,7 @@ def run_profile(args):
     X.device_check(s)
     st = X.last_contract_stats()
     print(json.dumps({"profile": args.profile, "workload": args.workload, "v": wl["v"], "o": wl["o"],
-                      "method": st.method, "slices": st.slices, "products": st.products,
+                      "method": st.method, "slices": st.slices, "products": st.products, "tile_n": st.tile_n,
                       "ms_per_step": round(ms / args.steps, 3),
                       "TFLOP/s": round(case.flops * args.steps / (ms / 1e3) / 1e12, 3)}))
 

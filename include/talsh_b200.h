@@ -265,6 +265,7 @@ typedef struct {
   double flops;      /* 2*M*N*K (real) or 8*M*N*K (complex), the reference's accounting */
   int products;      /* plane products the tensor-core GEMM ran (INT8 slice pairs or BF16
                         terms); its tensor-core work is products * flops */
+  int tile_n;        /* tensor-core N tile of the executed plan */
 } tb_contract_stats_t;
 int tb_last_contract_stats(tb_contract_stats_t* stats);
 
