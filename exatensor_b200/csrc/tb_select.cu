@@ -17,6 +17,7 @@
 #include <string>
 #include <mutex>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "tb_common.cuh"
@@ -53,6 +54,7 @@ struct Selector {
   float margin = 0.f;
   int autotune = 0;
   std::unordered_map<uint64_t, int> cache;
+  std::unordered_set<uint64_t> seen;  // close calls met once, not yet timed
 };
 Selector& sel() {
   static Selector S;
@@ -144,7 +146,14 @@ int selector_pick(const float* f, int* idx, bool* ambiguous, uint64_t* key) {
   *ambiguous = S.autotune && second >= 0 && (y[second] - y[best]) < S.margin && f[3] >= kTuneMinLog2Flops;
   if (*ambiguous) {
     auto it = S.cache.find(h);
-    if (it != S.cache.end()) { *idx = it->second; *ambiguous = false; }
+    if (it != S.cache.end()) {
+      *idx = it->second;
+      *ambiguous = false;
+    } else if (S.seen.insert(h).second) {
+      // first time this shape is seen: take the prediction; time the
+      // candidates only if the same shape comes back (one-off shapes never pay)
+      *ambiguous = false;
+    }
   }
   return 0;
 }
@@ -175,6 +184,7 @@ extern "C" int tb_selector_install(int n_hidden, const float* params, const floa
   Selector& S = sel();
   std::lock_guard<std::mutex> lk(S.mu);
   S.cache.clear();
+  S.seen.clear();
   if (!params) { S.on = false; return 0; }
   if (n_hidden < 1 || !mean || !scale) { set_error("tb_selector_install: bad arguments"); return TB_ERR_INVALID_ARGS; }
   const int F = TB_DESC_FEATURES, O = TB_SELECT_PLANS;

@@ -236,9 +236,10 @@ int tb_mlp_adam_step(tb_mlp_t* net, float lr, float beta1, float beta2, float ep
  * (TB_DESC_FEATURES -> hidden -> hidden -> TB_SELECT_PLANS) network and the
  * feature normalisation (x - mean) / scale.  params = NULL removes it (the
  * rule-based choice returns).  margin: when the two best predictions differ
- * by less than this (in natural-log units) and autotune != 0, the library
- * times both plans once (alpha = 0, beta = 1 runs, D unchanged) and caches
- * the winner per descriptor. */
+ * by less than this (in natural-log units), autotune != 0 and the contraction
+ * is large (about 1.7e10 FLOP or more), the second call with the same
+ * descriptor times every plan once (alpha = 0, beta = 1 runs, D unchanged)
+ * and caches the winner; one-off shapes keep the prediction. */
 int tb_selector_install(int n_hidden, const float* params, const float* mean, const float* scale, float margin,
                         int autotune);
 /* The selector's choice for a descriptor: plan index (0 TTGT, 1 tensor cores

@@ -124,7 +124,7 @@ def test_auto_uses_the_installed_selector(xt, dev):
     XB.selector_install(nh, np.zeros(n, np.float32), np.zeros(16, np.float32), np.ones(16, np.float32),
                         margin=0.5, autotune=True)
     try:
-        for _ in range(2):  # the second call takes the cached decision
+        for _ in range(3):  # first: prediction; second: timed candidates; third: cached decision
             dd = dev.put(d2)
             xt.tensor_contract(pattern2, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(),
                                1.0, stream=dev.stream())
