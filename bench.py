@@ -169,11 +169,16 @@ class ContractionCase:
                           self.rd, self.R.data_ptr(), 1.0, 0, accumulative, X.make_plan(method), self.s)
 
 
-def time_steps(fn, steps, warmup, world, stream_obj):
+def time_steps(fn, steps, warmup, world, stream_obj, on_timed=None):
+    """Device time (ms) of `steps` calls of fn after `warmup` untimed calls;
+    on_timed() runs between the two (after a synchronize), e.g. to reset
+    per-kernel counters so that they cover the timed calls only."""
     import torch
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
+    if on_timed is not None:
+        on_timed()
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -504,24 +509,28 @@ def run_ours(args):
     case.run(X.METHOD_AUTO)
     torch.cuda.synchronize()
     clocks = Clocks(local)
-    n0 = X.launch_count()
-    X.timing_enable(True)
-    X.timing_read()
-    clocks.start()
-    ms = time_steps(lambda: case.run(X.METHOD_AUTO), args.steps, args.warmup, world, s_obj)
+    n0 = [0]
+
+    def start_counters():
+        # the warm-up calls include the selector's one-time timing of close
+        # candidates; launches and GEMM events count the timed calls only
+        n0[0] = X.launch_count()
+        X.timing_enable(True)
+        X.timing_read()
+        clocks.start()
+    ms = time_steps(lambda: case.run(X.METHOD_AUTO), args.steps, args.warmup, world, s_obj, on_timed=start_counters)
     clk = clocks.stop()
     gemm_ms, gemm_n = X.timing_read()
     X.timing_enable(False)
-    launches = X.launch_count() - n0
+    launches = X.launch_count() - n0[0]
     st = X.last_contract_stats()
     chosen_method = {1: "ttgt", 2: "fused"}.get(st.method, str(st.method))
     ms_max = max_over_ranks(ms, world)
     value = world * args.steps * case.flops / (ms_max / 1e3) / 1e12
     # plain form
     psteps = max(1, args.steps // 2)
-    X.timing_enable(True)
-    X.timing_read()
-    pms = time_steps(lambda: case.run(X.METHOD_TTGT), psteps, 1, world, s_obj)
+    pms = time_steps(lambda: case.run(X.METHOD_TTGT), psteps, 1, world, s_obj,
+                     on_timed=lambda: (X.timing_enable(True), X.timing_read()))
     pgemm_ms, pgemm_n = X.timing_read()
     X.timing_enable(False)
     plain = case.flops / (max_over_ranks(pms, world) / psteps / 1e3) / 1e12

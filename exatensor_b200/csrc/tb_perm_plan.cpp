@@ -164,6 +164,36 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
       }
     }
   }
+  // 5b. partial dims that a nearby divisor tiles exactly: tiles at a
+  // dimension's end are partial and take the kernel's general (slower) code,
+  // so a partial extent moves to a divisor of its dimension within a factor
+  // two when the tile stays within Vmax and keeps its vector-aligned rows
+  // (76 with 26: 38, no partial tile).  The largest such tile is taken.
+  {
+    int64_t pA = 1;
+    for (int i = 0; i < a; ++i) pA *= D[i];
+    auto row_class = [&](int64_t ta) {  // 16: rows of 16-byte units, 8: of 8-byte units (4-byte elements)
+      const int64_t bytes = pA * ta * es;
+      return bytes % 16 == 0 ? 16 : (es < 8 && bytes % 8 == 0 ? 8 : 0);
+    };
+    int dims_to_fix[2] = {blast, a};
+    for (int k = 0; k < 2; ++k) {
+      const int d = dims_to_fix[k];
+      if (d < 0 || t[d] >= D[d] || D[d] % t[d] == 0) continue;
+      if (k == 1 && d == blast) continue;  // same dim as the store block's last: already done
+      const int64_t V = vol_of(), cur = t[d];
+      int64_t best = 0, bestV = 0;
+      for (int64_t x = std::max<int64_t>(1, cur / 2); x <= std::min(D[d], 2 * cur); ++x) {
+        if (D[d] % x != 0) continue;
+        const int64_t Vn = V / cur * x;
+        if (Vn > Vmax || Vn < Vmin / 2) continue;
+        if (d == a && row_class(x) < row_class(cur)) continue;
+        if (d == blast && x * (V / cur) < 1) continue;
+        if (Vn > bestV) { best = x; bestV = Vn; }
+      }
+      if (best) t[d] = best;
+    }
+  }
   // 6. chunk structure
   const int pa = (t[a] < D[a]) ? a : -1;
   const int pb = (t[blast] < D[blast]) ? blast : -1;
@@ -264,6 +294,16 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
              (P.ej_pb_stride * (int64_t)es) % P.vbytes == 0 && nB <= LA && (LA * es) % P.vbytes == 0) ? 1 : 0;
   P.nvec = P.vbytes ? (int)((LA * es + P.vbytes - 1) / P.vbytes) : 0;
   magic32((uint32_t)std::max(1, P.nvec), &P.nv_magic, &P.nv_shift);
+  // row copies: store chunk c is load row c (same dim, same run), rows of
+  // whole vectors
+  P.rows2d = (P.lin2d && P.vbytes && es <= P.vbytes && nA == nB && LA == LB && P.ej_pb_stride == 1 &&
+              P.chunk_eb == lap && (LA * es) % P.vbytes == 0) ? 1 : 0;
+  {
+    bool ov = P.rows2d && (P.chunk_sout * es) % P.vbytes == 0;
+    for (int i = 0; ov && i < r; ++i)
+      if (t[i] < D[i] && (t[i] * SO[i] * es) % P.vbytes != 0) ov = false;  // tile steps along grid dims
+    P.out_vec = ov ? 1 : 0;
+  }
   // positions inside a store chunk: store-block dims before blast
   for (int64_t j = 0; j < prodB; ++j) {
     int64_t x = j, e = 0;
@@ -306,6 +346,29 @@ int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, Per
   for (int q = 0; q < rank; ++q) { pos[q] = s; s *= oe[q]; }
   for (int i = 0; i < rank; ++i) SO[i] = pos[cptrn[i] - 1];
   return build_perm_plan(es, rank, D, SI, SO, p);
+}
+
+int perm2d_list_entries(const PermParams& P, bool rows, int nthr) {
+  if (!P.lin2d || P.vbytes <= 0 || P.es > P.vbytes || P.nvec <= 0) return 0;
+  const int64_t VW = P.vbytes / P.es;
+  int64_t nld = (int64_t)P.nA * P.nvec, nst, maxb_ld, maxb_st;
+  maxb_ld = (int64_t)(P.nA - 1) * P.row_sin + (int64_t)P.nvec * VW;
+  if (rows) {
+    if (!P.rows2d) return 0;
+    nst = (int64_t)P.nB * P.nvec;
+    maxb_st = (int64_t)(P.nB - 1) * P.chunk_sout + (int64_t)P.nvec * VW;
+  } else {
+    if (!P.vec2d || P.nB % VW != 0) return 0;
+    nst = (int64_t)P.LB * (P.nB / VW);
+    maxb_st = (int64_t)P.LB + (int64_t)P.nB * P.chunk_sout;
+  }
+  const int64_t lim = (int64_t)1 << 31;
+  // shared-memory offsets are below the stage size; global ones must fit int32
+  if (maxb_ld >= lim || maxb_st >= lim || P.row_sin < 0 || P.chunk_sout < 0) return 0;
+  const int64_t need = std::max(nld, nst);
+  if (need <= 8 * (int64_t)nthr) return 8;
+  if (need <= 16 * (int64_t)nthr) return 16;
+  return 0;
 }
 
 }  // namespace tb

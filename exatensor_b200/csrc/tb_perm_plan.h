@@ -67,13 +67,37 @@ struct PermParams {
   int vbytes;                   // vector bytes of the 2-D path: 16, 8 or 0
   int nvec;                     // vectors per full load row
   uint32_t nv_magic; int nv_shift;  // fast division by nvec
+  // 2-D tiles whose store chunks are the load rows themselves (row copies:
+  // the fastest dim stays fastest, one other dim moves): the store phase
+  // moves whole vectors as well.  out_vec: every store run starts on a
+  // vbytes boundary of the output (relative to an aligned output pointer).
+  int rows2d;
+  int out_vec;
 };
+
+// Full-tile offset lists of the 2-D kernel.  A thread's i-th copy in a full
+// tile is the linear position lin = tid + i * nthr of the tile's (outer p,
+// inner q) grid in q-fastest order; it sits at shared-memory byte offset
+// p*Ap + q*Aq and at global element offset p*Bp + q*Bq from the tile origin.
+// The offsets are the same in every full tile, so the kernel computes them
+// once.  The same function drives the CPU emulation of the kernel.
+TB_HD void perm_list_entry(int lin, int nq, uint32_t Aq, uint32_t Ap, int32_t Bq, int32_t Bp, uint32_t* a,
+                           int32_t* b) {
+  const int p = lin / nq, q = lin - p * nq;
+  *a = (uint32_t)p * Ap + (uint32_t)q * Aq;
+  *b = (int32_t)((uint32_t)p * (uint32_t)Bp + (uint32_t)q * (uint32_t)Bq);
+}
 
 // Host-side plan builder.  dims/sin/sout describe the input dims (input
 // strides, output strides), first dim fastest in the input.  Returns 0 or a
 // TB_ERR code.  Dims of extent 1 are dropped and mergeable neighbours fused.
 int build_perm_plan(int es, int rank, const int64_t* dims, const int64_t* sin, const int64_t* sout,
                     PermParams* p);
+// Entries per thread of the 2-D kernel's full-tile offset lists for a plan
+// whose vector path is rows (row copies) or column groups (transposes): 8 or
+// 16, or 0 when the lists would not cover a tile, an offset would not fit in
+// 32 bits, or the last column group is ragged (the general code runs then).
+int perm2d_list_entries(const PermParams& P, bool rows, int nthr);
 // Bytes of one pipeline stage (a tile in shared memory).
 inline int64_t perm_stage_bytes(const PermParams& P) { return (int64_t)P.nA * P.lap * P.es; }
 // Convenience: plain O2N permutation of a dense tensor (cptrn 1-based).

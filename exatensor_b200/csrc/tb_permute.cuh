@@ -258,13 +258,26 @@ perm_pipe_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ 
 // ---------------------------------------------------------------------------
 // Two-dimensional tiles (PermParams::lin2d): every load row and every store
 // chunk is one step of a single dimension, so their offsets are c * stride and
-// the kernel needs no chunk tables.  Warps take whole rows (loads: 16-byte or
-// element cp.async, lanes along the row) and whole chunks (stores: lanes along
-// the output run), which keeps the instruction count per element low; the
-// 3-stage cp.async pipeline is the same as perm_pipe_kernel's !BULK path.
+// the kernel needs no chunk tables.
+//
+// Full tiles (all but those at the tensor's edges) run on per-thread offset
+// lists (perm_list_entry): a thread's copies sit at the same tile-relative
+// offsets in every full tile, so the kernel computes them once, keeps them in
+// registers and its loops are unrolled loads and stores at base + offset.
+// One thread computes each tile's origin, one tile ahead, into a ring of
+// headers in shared memory.  Partial tiles, and plans whose lists do not fit
+// (perm2d_list_entries == 0), take the general code:
+//   perm2d_issue / perm2d_store    warps take whole rows (lanes along the row)
+//                                  and whole chunks (lanes along the run);
+//   perm2dv_issue                  the CTA walks (row, vector) pairs;
+//   perm2dv_store                  each lane reads VB bytes = VB / es adjacent
+//                                  columns (store chunks) of one row and writes
+//                                  that many output runs.
+// Rows in shared memory are an odd number of 16-byte units long where the
+// plan allows it, so a warp's vector reads down a column spread over the banks.
+// ---------------------------------------------------------------------------
 template <typename Elem>
-__device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in, Elem* stage, int64_t tile) {
-  const TileOrigin o = tile_origin(P, tile);
+__device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in, Elem* stage, const TileOrigin& o) {
   int len = P.LA;
   if (!o.full && P.pa >= 0) len = P.prodA * (P.pb == P.pa ? min(o.rem_a, o.rem_b) : o.rem_a);
   int rows = P.nA;
@@ -295,8 +308,8 @@ __device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in
 }
 
 template <typename Elem, typename Store>
-__device__ __forceinline__ void perm2d_store(const PermParams& P, const Elem* stage, int64_t tile, const Store& st) {
-  const TileOrigin o = tile_origin(P, tile);
+__device__ __forceinline__ void perm2d_store(const PermParams& P, const Elem* stage, const TileOrigin& o,
+                                             const Store& st) {
   const int qlim = (!o.full && P.pb >= 0) ? (P.pa == P.pb ? min(o.rem_a, o.rem_b) : o.rem_b) : (1 << 30);
   int chunks = P.nB;
   if (!o.full && P.pa >= 0 && P.pa != P.pb && P.chunk_is_pa) chunks = min(chunks, o.rem_a);
@@ -312,35 +325,12 @@ __device__ __forceinline__ void perm2d_store(const PermParams& P, const Elem* st
   }
 }
 
-// Vectorised 2-D tiles (PermParams::vec2d): the load phase walks (row,
-// 16-byte vector) pairs over the whole CTA, and the store phase gives each
-// lane 16 / es adjacent columns (= store chunks) of one row: one 16-byte
-// shared-memory read feeds 16 / es output runs, and consecutive lanes take
-// consecutive rows, i.e. consecutive positions of those runs.  Rows are an
-// odd number of 16-byte units long, so a warp's 16-byte reads of one column
-// group spread over all banks.  The tile's store bounds are computed by
-// thread 0 when the tile is issued and kept in shared memory until its store.
-struct Perm2dHdr {
-  int64_t out_base;
-  int chunks, jlim;
-};
-
 template <typename Elem, int VB>
-__device__ __forceinline__ void perm2dv_issue(const PermParams& P, const Elem* in, Elem* stage, int64_t tile,
-                                              Perm2dHdr* hdr) {
-  const TileOrigin o = tile_origin(P, tile);
+__device__ __forceinline__ void perm2dv_issue(const PermParams& P, const Elem* in, Elem* stage, const TileOrigin& o) {
   int len = P.LA;
   if (!o.full && P.pa >= 0) len = P.prodA * (P.pb == P.pa ? min(o.rem_a, o.rem_b) : o.rem_a);
   int rows = P.nA;
   if (!o.full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = min(rows, o.rem_b);
-  if (threadIdx.x == 0) {
-    const int qlim = (!o.full && P.pb >= 0) ? (P.pa == P.pb ? min(o.rem_a, o.rem_b) : o.rem_b) : (1 << 30);
-    int chunks = P.nB;
-    if (!o.full && P.pa >= 0 && P.pa != P.pb && P.chunk_is_pa) chunks = min(chunks, o.rem_a);
-    hdr->out_base = o.out_base;
-    hdr->chunks = chunks;
-    hdr->jlim = min(P.LB, qlim);
-  }
   constexpr int VW = VB / (int)sizeof(Elem);
   const int nv = (len + VW - 1) / VW;  // valid vectors of a row in this tile
   const int total = rows * P.nvec;
@@ -359,59 +349,194 @@ __device__ __forceinline__ void perm2dv_issue(const PermParams& P, const Elem* i
 }
 
 template <typename Elem, typename Store, int VB>
-__device__ __forceinline__ void perm2dv_store(const PermParams& P, const Elem* stage, const Perm2dHdr& h,
+__device__ __forceinline__ void perm2dv_store(const PermParams& P, const Elem* stage, const TileOrigin& o,
                                               const Store& st) {
   constexpr int VW = VB / (int)sizeof(Elem);
   using V = typename std::conditional<VB == 16, uint4, uint2>::type;
-  const int groups = (h.chunks + VW - 1) / VW;
+  const int qlim = (!o.full && P.pb >= 0) ? (P.pa == P.pb ? min(o.rem_a, o.rem_b) : o.rem_b) : (1 << 30);
+  int chunks = P.nB;
+  if (!o.full && P.pa >= 0 && P.pa != P.pb && P.chunk_is_pa) chunks = min(chunks, o.rem_a);
+  const int jlim = min(P.LB, qlim);
+  const int groups = (chunks + VW - 1) / VW;
   const int total = groups * P.LB;
   const int pstride = P.ej_pb_stride;
   for (int e = threadIdx.x; e < total; e += kPermThreads) {
     const int g = (int)fdiv32((uint32_t)e, P.lb_magic, P.lb_shift);
     const int j = e - g * P.LB;
-    if (j >= h.jlim) continue;
+    if (j >= jlim) continue;
     const int c0 = g * VW;
     union { V q; Elem v[VW]; } u;
     u.q = *reinterpret_cast<const V*>(stage + (size_t)j * pstride + c0);
-    const int64_t ob = h.out_base + j;
+    const int64_t ob = o.out_base + j;
 #pragma unroll
     for (int t = 0; t < VW; ++t)
-      if (c0 + t < h.chunks) st(ob + (int64_t)(c0 + t) * P.chunk_sout, u.v[t]);
+      if (c0 + t < chunks) st(ob + (int64_t)(c0 + t) * P.chunk_sout, u.v[t]);
   }
 }
 
-template <typename Elem, typename Store, int VB>  // VB: vector bytes of the vectorised path, 0 = scalar
-__global__ void __launch_bounds__(kPermThreads)
-perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st) {
+// A thread's full-tile offset list (N entries, n of them valid).
+template <int N>
+struct PermList {
+  uint32_t a[N];  // shared-memory byte offset
+  int32_t b[N];   // global element offset from the tile origin
+  int n;
+  __device__ __forceinline__ void build(int nq, int np, uint32_t Aq, uint32_t Ap, int32_t Bq, int32_t Bp) {
+    const int total = nq * np, tid = threadIdx.x;
+    n = tid < total ? min(N, (total - 1 - tid) / kPermThreads + 1) : 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) perm_list_entry(tid + i * kPermThreads, nq, Aq, Ap, Bq, Bp, &a[i], &b[i]);
+  }
+};
+
+// Store functors that can write a whole vector of adjacent elements.
+template <class S, class = void>
+struct has_vec_store : std::false_type {};
+template <class S>
+struct has_vec_store<S, std::void_t<decltype(S::kVecStore)>> : std::true_type {};
+
+constexpr int kHdrRing = kStages + 1;  // tile headers: issued, in flight, stored, being written
+
+// VB: vector bytes of the vector paths (0: scalar general code only).
+// ROWS: row copies (PermParams::rows2d), else column-group transposes.
+// N: entries of the full-tile offset lists (0: general code only).
+template <typename Elem, typename Store, int VB, bool ROWS, int N>
+__global__ void __launch_bounds__(kPermThreads, N >= 16 ? 2 : (N > 0 ? 3 : 1))
+perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st, int flags) {
   constexpr bool VEC = VB > 0;
+  constexpr bool LISTS = VEC && N > 0;
+  constexpr int VBv = VB ? VB : 16;
+  constexpr int es = (int)sizeof(Elem);
+  constexpr int VW = VBv / es > 0 ? VBv / es : 1;
+  constexpr int NL = N > 0 ? N : 1;
+  using V = typename std::conditional<VBv == 16, uint4, uint2>::type;
+  // flags: bit 0 = the functor's vector stores (row copies), bit 1 = full
+  // tiles through the general code as well (a tuning/diagnostic switch)
+  const bool vstore = (flags & 1) != 0;
+  const bool lists = LISTS && (flags & 2) == 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ Perm2dHdr hdr[kStages];
+  __shared__ TileOrigin org[kHdrRing];
   Elem* bufs = reinterpret_cast<Elem*>(smem_raw);
   const size_t stage_elems = (size_t)P.nA * P.lap;
   const int64_t first = blockIdx.x, step = gridDim.x;
-  const int64_t mine = first < P.ntiles ? (P.ntiles - 1 - first) / step + 1 : 0;
-  for (int k = 0; k < kStages - 1; ++k) {
-    if (k < mine) {
-      if (VEC) perm2dv_issue<Elem, VB ? VB : 16>(P, in, bufs + (size_t)k * stage_elems, first + k * step, &hdr[k]);
-      else perm2d_issue<Elem>(P, in, bufs + (size_t)k * stage_elems, first + k * step);
+  const int mine = first < P.ntiles ? (int)((P.ntiles - 1 - first) / step + 1) : 0;
+  PermList<NL> ldl, stl;
+  if (LISTS) {
+    ldl.build(P.nvec, P.nA, VBv, (uint32_t)(P.lap * es), VW, (int32_t)P.row_sin);
+    if (ROWS)
+      stl.build(P.nvec, P.nB, VBv, (uint32_t)(P.chunk_eb * es), VW, (int32_t)P.chunk_sout);
+    else
+      stl.build(P.LB, P.nB / VW, (uint32_t)(P.ej_pb_stride * es), VBv, 1, (int32_t)(VW * P.chunk_sout));
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kStages && k < mine; ++k) org[k] = tile_origin(P, first + k * step);
+  __syncthreads();
+
+  auto issue = [&](int k) {
+    const TileOrigin o = org[k % kHdrRing];
+    Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
+    if (lists && o.full) {
+      const Elem* src = in + o.in_base;
+      const uint32_t sb = smem_addr(stage);
+#pragma unroll
+      for (int i = 0; i < NL; ++i) {
+        if (i < ldl.n) {
+          if (VBv == 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sb + ldl.a[i]), "l"(src + ldl.b[i])
+                         : "memory");
+          else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sb + ldl.a[i]), "l"(src + ldl.b[i])
+                         : "memory");
+        }
+      }
+    } else if (VEC) {
+      perm2dv_issue<Elem, VBv>(P, in, stage, o);
+    } else {
+      perm2d_issue<Elem>(P, in, stage, o);
     }
+  };
+  auto store = [&](int k) {
+    const TileOrigin o = org[k % kHdrRing];
+    const Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
+    if (lists && o.full) {
+      Store s2 = st;
+      s2.out += o.out_base;
+      const unsigned char* sb = reinterpret_cast<const unsigned char*>(stage);
+      const int32_t cs = (int32_t)P.chunk_sout;
+#pragma unroll
+      for (int i = 0; i < NL; ++i) {
+        if (i < stl.n) {
+          union { V q; Elem v[VW]; } u;
+          u.q = *reinterpret_cast<const V*>(sb + stl.a[i]);
+          if (ROWS) {
+            bool done = false;
+            if constexpr (has_vec_store<Store>::value) {
+              if (vstore) { s2.template vec<V>(stl.b[i], u.q); done = true; }
+            }
+            if (!done) {
+#pragma unroll
+              for (int t = 0; t < VW; ++t) s2(stl.b[i] + t, u.v[t]);
+            }
+          } else {
+#pragma unroll
+            for (int t = 0; t < VW; ++t) s2(stl.b[i] + t * cs, u.v[t]);
+          }
+        }
+      }
+    } else if (VEC && !ROWS) {
+      perm2dv_store<Elem, Store, VBv>(P, stage, o, st);
+    } else {
+      perm2d_store<Elem, Store>(P, stage, o, st);
+    }
+  };
+
+  for (int k = 0; k < kStages - 1; ++k) {
+    if (k < mine) issue(k);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
-  for (int64_t k = 0; k < mine; ++k) {
-    const int stg = (int)(k % kStages);
+  for (int k = 0; k < mine; ++k) {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
     __syncthreads();
-    const int64_t nk = k + kStages - 1;
-    const int nstg = (int)(nk % kStages);
-    if (nk < mine) {
-      if (VEC) perm2dv_issue<Elem, VB ? VB : 16>(P, in, bufs + (size_t)nstg * stage_elems, first + nk * step, &hdr[nstg]);
-      else perm2d_issue<Elem>(P, in, bufs + (size_t)nstg * stage_elems, first + nk * step);
-    }
+    const int nk = k + kStages - 1;
+    if (nk < mine) issue(nk);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    if (VEC) perm2dv_store<Elem, Store, VB ? VB : 16>(P, bufs + (size_t)stg * stage_elems, hdr[stg], st);
-    else perm2d_store<Elem, Store>(P, bufs + (size_t)stg * stage_elems, first + k * step, st);
+    // the header slot of tile k + kStages last held tile k - 1, whose store
+    // finished before the barrier above; it is read after the next barrier
+    if (threadIdx.x == 0 && k + kStages < mine) org[(k + kStages) % kHdrRing] = tile_origin(P, first + (int64_t)(k + kStages) * step);
+    store(k);
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Whether a store functor writes vectors of vbytes to an aligned output
+// (functors without vector stores: no; StoreCopy overloads this below).
+template <typename S>
+inline bool store_vec_ok(const S&, int) { return false; }
+
+// One 2-D kernel variant; N = list entries (0, 8 or 16).  The grid is the
+// number of CTAs resident at once (tiles are dealt to CTAs round robin).
+template <typename Elem, typename Store, int VB, bool ROWS>
+void launch_2d(int N, int64_t ntiles, size_t smem, cudaStream_t s, const PermParams& P, const Elem* in,
+               const Store& st, int flags) {
+  using Kern = void (*)(PermParams, const Elem*, Store, int);
+  const int idx = VB > 0 ? (N == 16 ? 2 : (N == 8 ? 1 : 0)) : 0;
+  const Kern kern = idx == 2 ? (Kern)perm2d_kernel<Elem, Store, VB, ROWS, (VB > 0 ? 16 : 0)>
+                  : idx == 1 ? (Kern)perm2d_kernel<Elem, Store, VB, ROWS, (VB > 0 ? 8 : 0)>
+                             : (Kern)perm2d_kernel<Elem, Store, VB, ROWS, 0>;
+  static bool attr[3] = {false, false, false};
+  static size_t occ_smem[3] = {0, 0, 0};
+  static int occ_blocks[3] = {0, 0, 0};
+  if (!attr[idx]) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    attr[idx] = true;
+  }
+  if (occ_smem[idx] != smem) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kPermThreads, smem) != cudaSuccess || b < 1) b = 1;
+    occ_smem[idx] = smem;
+    occ_blocks[idx] = b;
+  }
+  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)num_sms() * occ_blocks[idx], ntiles);
+  kern<<<grid, kPermThreads, smem, s>>>(P, in, st, flags);
 }
 
 // Launches the pipelined kernel with a grid sized to the SM count.
@@ -429,6 +554,7 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
     if (!strcmp(e, "async")) return 2;
     if (!strcmp(e, "tables")) return 3;  // the table-driven kernel even for 2-D tiles
     if (!strcmp(e, "scalar2d")) return 4;  // the 2-D kernel without 16-byte column groups
+    if (!strcmp(e, "norows")) return 5;    // row copies through the scalar 2-D store
     return 0;
   }();
   const bool eligible = P.tma_ok && ((uintptr_t)in % 16 == 0);
@@ -448,24 +574,22 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
   if (!bulk && P.lin2d && mode != 3) {
     // two-dimensional tiles: no chunk tables in shared memory, so more CTAs fit
     const size_t smem2 = (size_t)kStages * (size_t)perm_stage_bytes(P) + 128;
-    static bool attr2 = false;
-    if (!attr2) {
-      cudaFuncSetAttribute(perm2d_kernel<Elem, Store, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-      cudaFuncSetAttribute(perm2d_kernel<Elem, Store, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-      if (sizeof(Elem) <= 8)
-        cudaFuncSetAttribute(perm2d_kernel<Elem, Store, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-      attr2 = true;
+    const bool in_ok = P.vbytes && (uintptr_t)in % (uintptr_t)P.vbytes == 0 && mode != 4;
+    const bool vec = P.vec2d && in_ok;
+    const bool rows = P.rows2d && in_ok && mode != 5;  // TB_PERM_LOADS=norows: row copies as scalar stores
+    // TB_PERM_FAST=0: full tiles through the general code too (diagnostic)
+    static const int nowalk = [] { const char* e = getenv("TB_PERM_FAST"); return e && e[0] == '0' ? 2 : 0; }();
+    constexpr int V8 = sizeof(Elem) <= 8 ? 8 : 16;
+    if (rows || vec) {
+      const int N = perm2d_list_entries(P, rows, kPermThreads);
+      const int flags = (rows && P.out_vec && store_vec_ok(st, P.vbytes) ? 1 : 0) | nowalk;
+      if (rows && P.vbytes == 16) launch_2d<Elem, Store, 16, true>(N, P.ntiles, smem2, s, P, in, st, flags);
+      else if (rows) launch_2d<Elem, Store, V8, true>(N, P.ntiles, smem2, s, P, in, st, flags);
+      else if (P.vbytes == 16) launch_2d<Elem, Store, 16, false>(N, P.ntiles, smem2, s, P, in, st, flags);
+      else launch_2d<Elem, Store, V8, false>(N, P.ntiles, smem2, s, P, in, st, flags);
+    } else {
+      launch_2d<Elem, Store, 0, false>(0, P.ntiles, smem2, s, P, in, st, 0);
     }
-    int per2 = (int)((224 * 1024) / (smem2 + 1024));
-    per2 = std::max(1, std::min(per2, 2048 / kPermThreads));
-    int64_t grid2 = std::min<int64_t>((int64_t)num_sms() * per2, P.ntiles);
-    const bool vec = P.vec2d && (uintptr_t)in % (uintptr_t)P.vbytes == 0 && mode != 4;
-    if (vec && P.vbytes == 16)
-      perm2d_kernel<Elem, Store, 16><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
-    else if (vec && P.vbytes == 8 && sizeof(Elem) <= 8)
-      perm2d_kernel<Elem, Store, (sizeof(Elem) <= 8 ? 8 : 16)><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
-    else
-      perm2d_kernel<Elem, Store, 0><<<(unsigned)grid2, kPermThreads, smem2, s>>>(P, in, st);
   } else if (bulk)
     perm_pipe_kernel<Elem, Store, true><<<(unsigned)grid, kPermThreads, smem, s>>>(P, in, st, device_error_word());
   else
@@ -480,8 +604,16 @@ struct alignas(16) u128 { uint64_t lo, hi; };
 template <typename E>
 struct StoreCopy {
   E* out;
+  static constexpr bool kVecStore = true;
   __device__ __forceinline__ void operator()(int64_t o, const E& v) const { out[o] = v; }
+  // adjacent elements o, o+1, ... as one vector (o * sizeof(E) aligned to V)
+  template <typename V>
+  __device__ __forceinline__ void vec(int64_t o, const V& v) const { *reinterpret_cast<V*>(out + o) = v; }
 };
+template <typename E>
+inline bool store_vec_ok(const StoreCopy<E>& st, int vbytes) {
+  return vbytes > 0 && (uintptr_t)st.out % (uintptr_t)vbytes == 0;
+}
 // Conjugating copies: flip the sign bit of the imaginary part.
 struct StoreConjC4 {  // complex float as one 64-bit word (re low, im high)
   uint64_t* out;

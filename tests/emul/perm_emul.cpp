@@ -39,6 +39,46 @@ int main(int argc, char** argv) {
     ref[o] = i;
   }
   std::vector<long long> out(vol, -1), out2(P.lin2d ? vol : 0, -1);
+  const bool vecpath = P.lin2d && (P.vec2d || P.rows2d);
+  std::vector<long long> out3(vecpath ? vol : 0, -1);
+  // Full-tile offset lists of perm2d_kernel (perm_list_entry), replayed for
+  // every thread: the N entries of each thread together must cover the
+  // tile's (outer, inner) grid exactly once, with the offsets the formulas
+  // give, and the global ones must fit in 32 bits.
+  const int NLIST = vecpath ? perm2d_list_entries(P, P.rows2d != 0, 256) : 0;
+  struct Grid { int nq, np; long long Aq, Ap, Bq, Bp; };
+  Grid gl{}, gs{};
+  if (vecpath) {
+    const int VB = P.vbytes, VW = VB / es;
+    if (P.vec2d && P.rows2d) { printf("FAIL vec2d and rows2d both set\n"); return 1; }
+    if (P.rows2d && (P.nA != P.nB || P.LA != P.LB || P.ej_pb_stride != 1 || P.chunk_eb != P.lap ||
+                     P.chunk_sout == 0 || (P.LA * es) % VB != 0)) {
+      printf("FAIL rows2d shape\n"); return 1;
+    }
+    gl = {P.nvec, P.nA, VB, (long long)P.lap * es, VW, P.row_sin};
+    if (P.rows2d) gs = {P.nvec, P.nB, VB, (long long)P.chunk_eb * es, VW, P.chunk_sout};
+    else gs = {P.LB, P.nB / VW, (long long)P.ej_pb_stride * es, VB, 1, (long long)VW * P.chunk_sout};
+    if (NLIST != 0 && NLIST != 8 && NLIST != 16) { printf("FAIL list entries %d\n", NLIST); return 1; }
+    if (NLIST && !P.rows2d && P.nB % VW != 0) { printf("FAIL lists with a ragged column group\n"); return 1; }
+    auto check_list = [&](const Grid& g, const char* what) {
+      std::vector<int> seen((size_t)g.nq * g.np, 0);
+      for (int tid = 0; tid < 256; ++tid)
+        for (int i = 0; i < NLIST; ++i) {
+          const long long lin = (long long)tid + (long long)i * 256;
+          if (lin >= (long long)g.nq * g.np) break;
+          uint32_t a; int32_t b;
+          perm_list_entry((int)lin, g.nq, (uint32_t)g.Aq, (uint32_t)g.Ap, (int32_t)g.Bq, (int32_t)g.Bp, &a, &b);
+          const long long q = lin % g.nq, pp = lin / g.nq;
+          if ((long long)a != pp * g.Ap + q * g.Aq || (long long)b != pp * g.Bp + q * g.Bq) {
+            printf("FAIL %s list offsets %d %d\n", what, tid, i); exit(1);
+          }
+          seen[lin]++;
+        }
+      for (size_t i = 0; i < seen.size(); ++i)
+        if (seen[i] != 1) { printf("FAIL %s list coverage %zu %d\n", what, i, seen[i]); exit(1); }
+    };
+    if (NLIST) { check_list(gl, "load"); check_list(gs, P.rows2d ? "row store" : "column store"); }
+  }
   const int V = P.V, LA = P.LA, LB = P.LB;
   const long long bufn = (long long)P.nA * P.lap;
   std::vector<long long> buf(bufn, -1);
@@ -151,6 +191,47 @@ int main(int argc, char** argv) {
       for (int v = 0; v < P.nA * P.nvec; v += 7)
         if ((int)fdiv32((uint32_t)v, P.nv_magic, P.nv_shift) != v / P.nvec) fail("fdiv32 nvec", v, P.nvec);
     }
+    if (vecpath && full && NLIST) {
+      // full tile through the lists: vector loads, then vector reads of the
+      // stage feeding the row-copy or column-group stores
+      const int VB = P.vbytes, VW = VB / es;
+      std::vector<long long> vbuf(bufn, -1);
+      for (int tid = 0; tid < 256; ++tid)
+        for (int i = 0; i < NLIST; ++i) {
+          const int lin = tid + i * 256;
+          if (lin >= gl.nq * gl.np) break;
+          uint32_t a; int32_t b;
+          perm_list_entry(lin, gl.nq, (uint32_t)gl.Aq, (uint32_t)gl.Ap, (int32_t)gl.Bq, (int32_t)gl.Bp, &a, &b);
+          if (a % VB != 0) fail("list load smem misaligned", a, tid);
+          const long long src = in_base + b;
+          if ((src * es) % VB != 0) fail("list load source misaligned", src, tid);
+          if (src < 0 || (src * es + VB) > vol * es) fail("list load leaves the tensor", src, tid);
+          const long long e0 = a / es;
+          if (e0 + VW > bufn) fail("list load smem oob", e0, bufn);
+          for (int t = 0; t < VW; ++t)
+            if (src + t < vol) vbuf[e0 + t] = src + t;  // past a row's end: padding, never stored
+        }
+      for (int tid = 0; tid < 256; ++tid)
+        for (int i = 0; i < NLIST; ++i) {
+          const int lin = tid + i * 256;
+          if (lin >= gs.nq * gs.np) break;
+          uint32_t a; int32_t b;
+          perm_list_entry(lin, gs.nq, (uint32_t)gs.Aq, (uint32_t)gs.Ap, (int32_t)gs.Bq, (int32_t)gs.Bp, &a, &b);
+          if (a % VB != 0) fail("list store smem misaligned", a, tid);
+          const long long e0 = a / es;
+          if (e0 + VW > bufn) fail("list store smem oob", e0, bufn);
+          for (int t = 0; t < VW; ++t) {
+            const long long rel = P.rows2d ? (long long)b + t : (long long)b + (long long)t * P.chunk_sout;
+            if (rel >= ((long long)1 << 31)) fail("list store offset beyond 32 bits", rel, tid);
+            const long long dst = out_base + rel;
+            if (P.rows2d && P.out_vec && t == 0 && ((out_base + b) * es) % VB != 0) fail("row store misaligned", dst, tid);
+            if (dst < 0 || dst >= vol) fail("list store oob", dst, tid);
+            if (vbuf[e0 + t] < 0) fail("list store reads unloaded smem", e0 + t, tid);
+            if (out3[dst] != -1) fail("list double write", dst, tid);
+            out3[dst] = vbuf[e0 + t];
+          }
+        }
+    }
     if (P.lin2d) {
       int rows = P.nA;
       if (!full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = std::min(rows, rem_b);
@@ -176,6 +257,7 @@ int main(int argc, char** argv) {
           if (buf[ee] < 0) fail("2d store reads unloaded smem", ee, tile);
           if (out2[dst] != -1) fail("2d double write", dst, tile);
           out2[dst] = buf[ee];
+          if (vecpath && (!full || !NLIST)) out3[dst] = buf[ee];  // the general 2-D code
         }
       }
     }
@@ -183,7 +265,9 @@ int main(int argc, char** argv) {
   for (long long o = 0; o < vol; ++o) {
     if (out[o] != ref[o]) fail("wrong value at", o, out[o]);
     if (P.lin2d && out2[o] != ref[o]) fail("2d wrong value at", o, out2[o]);
+    if (vecpath && out3[o] != ref[o]) fail("walk wrong value at", o, out3[o]);
   }
-  printf("OK %lld %d %d %d tma=%d lin2d=%d vec2d=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok, P.lin2d, P.vec2d);
+  printf("OK %lld %d %d %d tma=%d lin2d=%d vec2d=%d rows2d=%d lists=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok,
+         P.lin2d, P.vec2d, P.rows2d, NLIST);
   return 0;
 }

@@ -79,6 +79,41 @@ def test_single_block_permutation_3142(xt, dev):
         assert np.array_equal(gpu_permute(xt, dev, x, dims, perm), ref)
 
 
+# Shapes whose plans run the 2-D kernel's vector paths: column-group
+# transposes (e.g. 2134) and row copies (1324, 1432: the fastest dim stays),
+# with partial tiles at the edges (90 and 30 do not divide every tile).
+TWO_D_SHAPES = [[90, 90, 30, 30], [90, 30, 90, 30], [66, 70, 18, 22], [100, 37, 45, 12], [38, 38, 38, 38]]
+TWO_D_PERMS = [(1, 3, 2, 4), (2, 1, 3, 4), (2, 4, 1, 3), (1, 4, 3, 2), (3, 1, 2, 4), (4, 2, 3, 1)]
+
+
+@pytest.mark.parametrize("dtk", KINDS)
+def test_two_dimensional_paths_bit_exact(xt, dev, dtk):
+    for i, dims in enumerate(TWO_D_SHAPES):
+        x = rand_host(dtk, int(np.prod(dims)), 40 + i)
+        for perm in TWO_D_PERMS:
+            ref = O.permute(x, dims, perm)
+            got = gpu_permute(xt, dev, x, dims, perm)
+            assert np.array_equal(got.view(np.uint8), ref.view(np.uint8)), (dims, perm)
+            if dtk in (O.C4, O.C8):  # conjugating stores (element-wise functor) on the same paths
+                got = gpu_permute(xt, dev, x, dims, perm, conj_bits=1)
+                assert np.array_equal(got.view(np.uint8), O.permute(x, dims, perm, conj=True).view(np.uint8))
+
+
+@pytest.mark.parametrize("dtk", [O.R4, O.R8])
+def test_two_dimensional_paths_permute_add(xt, dev, dtk):
+    # the fused permute+add functor (element-wise stores) on the same paths
+    for i, dims in enumerate(TWO_D_SHAPES[:3]):
+        vol = int(np.prod(dims))
+        l = rand_host(dtk, vol, 60 + i)
+        for perm in TWO_D_PERMS:
+            d0 = rand_host(dtk, vol, 70 + i)
+            ref = O.tensor_add(list(perm), d0.copy(), l, dims, 0.37)
+            dd, ld = dev.put(d0), dev.put(l)
+            xt.tensor_add(dtk, dims, perm, dd.data_ptr(), ld.data_ptr(), 0.37, 0, dev.stream())
+            got = dev.get(dd, d0.dtype, vol)
+            assert np.array_equal(got.view(np.uint8), ref.view(np.uint8)), (dims, perm)
+
+
 def test_skewed_extents(xt, dev):
     for dims, perm in [([3, 300, 250], [3, 1, 2]), ([2, 90, 90, 9], [4, 3, 2, 1]), ([700, 7, 5, 40], [2, 4, 1, 3]),
                        ([6, 5, 4, 3, 2, 30], [6, 1, 5, 2, 4, 3])]:

@@ -72,3 +72,12 @@ def test_skewed_and_large_leading(emul):
     run(emul, 8, [4099, 5], [2, 1])
     run(emul, 16, [1, 33, 1, 17], [2, 4, 1, 3])
     run(emul, 8, [13, 5, 5, 16, 10, 5], [2, 5, 3, 4, 6, 1])  # store block inside the load block
+
+
+@pytest.mark.parametrize("es", [4, 8])
+def test_two_dimensional_vector_paths(emul, es):
+    # shapes whose plans take the 2-D kernel's vector paths (column-group
+    # transposes and row copies), with partial tiles at the edges
+    for dims in ([90, 90, 30, 30], [90, 30, 90, 30], [66, 70, 18, 22], [100, 37, 45, 12], [38, 38, 38, 38]):
+        for perm in ([1, 3, 2, 4], [2, 1, 3, 4], [2, 4, 1, 3], [1, 4, 3, 2], [3, 1, 2, 4], [4, 2, 3, 1]):
+            run(emul, es, dims, perm)
