@@ -191,6 +191,24 @@ def time_steps(fn, steps, warmup, world, stream_obj, on_timed=None):
     return e0.elapsed_time(e1)
 
 
+def time_back_to_back(fn, steps, stream_obj):
+    """Device time (ms) of `steps` back-to-back calls of fn, with one untimed
+    call already queued when the start event is recorded, so that the host's
+    latency before the first launch is not counted (steady-state rate of a
+    kernel much shorter than a step of the headline workload)."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn()
+    e0.record(stream_obj)
+    for _ in range(steps):
+        fn()
+    e1.record(stream_obj)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
 def sample_error(X, case, method, nsamp=48):
     """Relative Frobenius and max-abs error of sampled D elements against the
     double-double oracle (each a K-length dot product), after one
@@ -248,9 +266,10 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs):
         X.fill_uniform(dtk, v, a.data_ptr(), 3, stream=stream)
         dims = [n] * 4
         for perm in itertools.permutations([1, 2, 3, 4]):
+            # the first call of a shape also picks its plan by timing (untimed here)
             X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream)
-            ms = time_steps(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream), 5, 1, 1,
-                            stream_obj) / 5
+            ms = time_back_to_back(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream),
+                                   10, stream_obj) / 10
             gb = 2.0 * v * es / 1e9
             rates.append(gb / (ms / 1e3))
             total_bytes += gb
@@ -266,7 +285,9 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs):
     agg = total_bytes / (total_ms / 1e3)
     out.update({"value": round(agg, 1), "unit": "GB/s", "min": round(min(rates), 1), "max": round(max(rates), 1),
                 "frac_of_measured_hbm": round(agg / hbm_gbs, 3), "frac_of_8000": round(agg / 8000.0, 3),
-                "cases": "24 rank-4 perms x {R8 76^4 (254.5 MiB), R4 90^4 (250.3 MiB)}, bit-exact"})
+                "cases": "24 rank-4 perms x {R8 76^4 (254.5 MiB), R4 90^4 (250.3 MiB)}, bit-exact",
+                "timing": "10 back-to-back calls per permutation, one queued before the start event; "
+                          "plans picked by the library's measured choice on the first call"})
     return out
 
 

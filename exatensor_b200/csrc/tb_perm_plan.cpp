@@ -11,7 +11,7 @@
 namespace tb {
 
 int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin_in,
-                    const int64_t* sout_in, PermParams* pp) {
+                    const int64_t* sout_in, PermParams* pp, int vmin_kb, int vmax_kb) {
   PermParams& P = *pp;
   std::memset(&P, 0, sizeof(P));
   P.es = es;
@@ -34,7 +34,7 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   for (int i = 0; i < r; ++i) Q[i] = i;
   std::stable_sort(Q.begin(), Q.end(), [&](int x, int y) { return SO[x] < SO[y]; });
   if (SO[Q[0]] != 1) return TB_ERR_NOT_IMPLEMENTED;
-  const int64_t T = std::max<int64_t>(1, 256 / es);
+  const int64_t T = std::max<int64_t>(1, 256 / es);  // minimum contiguous run of the load and store blocks
   // tile volume bounds (bytes; 16 KB .. 32 KB unless TB_PERM_VMIN_KB /
   // TB_PERM_VMAX_KB say otherwise -- tuning knobs that leave results unchanged)
   auto knob = [](const char* name, long dflt) {
@@ -42,7 +42,10 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     const long v = e ? std::atol(e) : 0;
     return (int64_t)(v >= 4 && v <= 96 ? v : dflt) * 1024;
   };
-  static const int64_t vmin_bytes = knob("TB_PERM_VMIN_KB", 16), vmax_bytes = knob("TB_PERM_VMAX_KB", 32);
+  static const int64_t vmin_env = knob("TB_PERM_VMIN_KB", 16), vmax_env = knob("TB_PERM_VMAX_KB", 32);
+  // explicit bounds (the measured plan choice) override the defaults
+  const int64_t vmin_bytes = vmin_kb > 0 ? (int64_t)vmin_kb * 1024 : vmin_env;
+  const int64_t vmax_bytes = vmax_kb > 0 ? (int64_t)vmax_kb * 1024 : vmax_env;
   const int64_t Vmax = std::max<int64_t>(1, vmax_bytes / es), Vmin = std::min(Vmax, std::max<int64_t>(1, vmin_bytes / es));
   std::vector<int64_t> t(r, 1);
   auto cdiv = [](int64_t x, int64_t y) { return (x + y - 1) / y; };
@@ -51,6 +54,16 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   auto even = [&](int64_t D, int64_t want) {
     want = std::max<int64_t>(1, std::min(D, want));
     return cdiv(D, cdiv(D, want));
+  };
+  // Store-run extent: a divisor of D in [want, 1.5 want] if there is one
+  // (5776 with want 32 -> 38: no partial tiles), else an even split into
+  // pieces of at least want (90 with want 64 -> 90): store runs never fall
+  // below the minimum run.
+  auto even_up = [&](int64_t D, int64_t want) {
+    want = std::max<int64_t>(1, std::min(D, want));
+    for (int64_t x = want; x <= std::min(D, want + want / 2); ++x)
+      if (D % x == 0) return x;
+    return cdiv(D, std::max<int64_t>(1, D / want));
   };
   // 2. load block: input dims 0..a
   int a = 0;
@@ -77,13 +90,13 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
         continue;
       }
       if (i == a) {
-        t[a] = std::max(t[a], even(D[a], cdiv(T, volB)));
+        t[a] = std::max(t[a], even_up(D[a], cdiv(T, volB)));
         inB[a] = 1; blast = a; volB *= t[a];
         if (t[a] == D[a] && volB < T) continue;  // became whole: the run may grow further
         break;
       }
       if (volB * D[i] <= T) { t[i] = D[i]; inB[i] = 1; blast = i; volB *= D[i]; continue; }
-      t[i] = even(D[i], cdiv(T, volB));
+      t[i] = even_up(D[i], cdiv(T, volB));
       inB[i] = 1; blast = i; volB *= t[i];
       break;
     }
@@ -179,7 +192,7 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     int dims_to_fix[2] = {blast, a};
     for (int k = 0; k < 2; ++k) {
       const int d = dims_to_fix[k];
-      if (d < 0 || t[d] >= D[d] || D[d] % t[d] == 0) continue;
+      if (d < 0 || t[d] >= D[d] || D[d] % t[d] == 0 || cdiv(D[d], t[d]) > 16) continue;  // few partial tiles
       if (k == 1 && d == blast) continue;  // same dim as the store block's last: already done
       const int64_t V = vol_of(), cur = t[d];
       int64_t best = 0, bestV = 0;
@@ -297,7 +310,7 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   // row copies: store chunk c is load row c (same dim, same run), rows of
   // whole vectors
   P.rows2d = (P.lin2d && P.vbytes && es <= P.vbytes && nA == nB && LA == LB && P.ej_pb_stride == 1 &&
-              P.chunk_eb == lap && (LA * es) % P.vbytes == 0) ? 1 : 0;
+              (P.chunk_eb == lap || nA == 1) && (LA * es) % P.vbytes == 0) ? 1 : 0;
   {
     bool ov = P.rows2d && (P.chunk_sout * es) % P.vbytes == 0;
     for (int i = 0; ov && i < r; ++i)
@@ -329,7 +342,8 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   return 0;
 }
 
-int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p) {
+int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p, int vmin_kb,
+                        int vmax_kb) {
   if (rank < 0 || rank > kPlanMaxRank) return TB_ERR_INVALID_ARGS;
   int64_t D[kPlanMaxRank], SI[kPlanMaxRank], SO[kPlanMaxRank], pos[kPlanMaxRank + 1];
   int seen[kPlanMaxRank + 1] = {0};
@@ -345,7 +359,7 @@ int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, Per
   s = 1;
   for (int q = 0; q < rank; ++q) { pos[q] = s; s *= oe[q]; }
   for (int i = 0; i < rank; ++i) SO[i] = pos[cptrn[i] - 1];
-  return build_perm_plan(es, rank, D, SI, SO, p);
+  return build_perm_plan(es, rank, D, SI, SO, p, vmin_kb, vmax_kb);
 }
 
 int perm2d_list_entries(const PermParams& P, bool rows, int nthr) {

@@ -91,8 +91,12 @@ TB_HD void perm_list_entry(int lin, int nq, uint32_t Aq, uint32_t Ap, int32_t Bq
 // Host-side plan builder.  dims/sin/sout describe the input dims (input
 // strides, output strides), first dim fastest in the input.  Returns 0 or a
 // TB_ERR code.  Dims of extent 1 are dropped and mergeable neighbours fused.
+// vmin_kb / vmax_kb bound the tile's bytes (0: the defaults, 16 and 32 KB).
 int build_perm_plan(int es, int rank, const int64_t* dims, const int64_t* sin, const int64_t* sout,
-                    PermParams* p);
+                    PermParams* p, int vmin_kb = 0, int vmax_kb = 0);
+// Convenience: plain O2N permutation of a dense tensor (cptrn 1-based).
+int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p, int vmin_kb = 0,
+                        int vmax_kb = 0);
 // Entries per thread of the 2-D kernel's full-tile offset lists for a plan
 // whose vector path is rows (row copies) or column groups (transposes): 8 or
 // 16, or 0 when the lists would not cover a tile, an offset would not fit in
@@ -100,9 +104,5 @@ int build_perm_plan(int es, int rank, const int64_t* dims, const int64_t* sin, c
 int perm2d_list_entries(const PermParams& P, bool rows, int nthr);
 // Bytes of one pipeline stage (a tile in shared memory).
 inline int64_t perm_stage_bytes(const PermParams& P) { return (int64_t)P.nA * P.lap * P.es; }
-// Convenience: plain O2N permutation of a dense tensor (cptrn 1-based).
-int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p);
-
-
 
 }  // namespace tb

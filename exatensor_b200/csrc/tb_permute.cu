@@ -3,6 +3,8 @@
 #include "tb_permute.cuh"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <vector>
 
 namespace tb {
@@ -121,6 +123,104 @@ double cmplx8_to_real8(double re, double im) {
 
 double real_scale_factor(double re, double im) { return cmplx8_to_real8(re, im); }
 
+// ---- measured plan choice for copies ----------------------------------------
+// Which tile size runs a permutation fastest depends on the permutation and
+// the element size in ways no simple rule captured (some run 10% faster with
+// smaller tiles, others 25% faster with larger ones).  The first copy of a
+// tensor of at least kTuneMinBytes with a given shape, permutation and
+// element size therefore times the distinct plans that the planner builds for
+// a few tile-size bounds, once each after an untimed run, on the caller's
+// stream, and keeps the fastest for later calls (the default unless another
+// is more than 2% faster).  Every plan writes the same bits, so the choice
+// changes speed only; the timed runs leave the copy done.  Not while the
+// stream is being captured into a graph (the default plan runs then), and
+// TB_PERM_TUNE=0 turns it off.  Only copies are timed: their output may be
+// written several times, unlike an accumulation's.
+struct TileBounds { int vmin_kb, vmax_kb; };
+constexpr TileBounds kTileCandidates[] = {{0, 0}, {8, 24}, {24, 48}};
+constexpr int kNumTileCandidates = 3;
+constexpr int64_t kTuneMinBytes = (int64_t)32 << 20;
+
+std::mutex g_tune_mu;
+std::map<std::vector<int>, int> g_tune;  // (es, rank, dims, cptrn) -> candidate
+
+bool same_work(const PermParams& a, const PermParams& b) {
+  if (a.rank != b.rank || a.V != b.V || a.LA != b.LA || a.nA != b.nA || a.LB != b.LB || a.nB != b.nB ||
+      a.lap != b.lap || a.ntiles != b.ntiles)
+    return false;
+  for (int i = 0; i < a.rank; ++i)
+    if (a.tile[i] != b.tile[i]) return false;
+  return true;
+}
+
+template <typename E, typename Store>
+int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, const Store& st, cudaStream_t s) {
+  int64_t vol = 1;
+  for (int i = 0; i < rank; ++i) vol *= dims[i];
+  std::vector<int> key{(int)sizeof(E), rank};
+  key.insert(key.end(), dims, dims + rank);
+  key.insert(key.end(), cptrn, cptrn + rank);
+  int pick = -1;
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) pick = it->second;
+  }
+  static const bool tune_on = [] { const char* e = getenv("TB_PERM_TUNE"); return !(e && e[0] == '0'); }();
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) { cudaGetLastError(); cap = cudaStreamCaptureStatusActive; }
+  const bool tune = pick < 0 && tune_on && vol * (int64_t)sizeof(E) >= kTuneMinBytes && cap == cudaStreamCaptureStatusNone;
+  if (!tune) {
+    const TileBounds b = kTileCandidates[pick < 0 ? 0 : pick];
+    PermParams P;
+    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb);
+    if (e == 0) return launch_perm<E, Store>(P, in, st, s);
+    if (e != TB_ERR_NOT_IMPLEMENTED) return e;
+    return run_scatter<E, Store>(rank, dims, cptrn, in, st, s);
+  }
+  static PermParams plans[kNumTileCandidates];  // large; built under the lock below
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  int n = 0, idx[kNumTileCandidates];
+  for (int c = 0; c < kNumTileCandidates; ++c) {
+    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &plans[n], kTileCandidates[c].vmin_kb,
+                                kTileCandidates[c].vmax_kb);
+    if (e == TB_ERR_NOT_IMPLEMENTED && c == 0) {
+      g_tune[key] = 0;
+      return run_scatter<E, Store>(rank, dims, cptrn, in, st, s);
+    }
+    if (e) { if (c == 0) return e; continue; }
+    bool dup = false;
+    for (int k = 0; k < n; ++k) dup = dup || same_work(plans[k], plans[n]);
+    if (!dup) idx[n++] = c;
+  }
+  if (n == 1) { g_tune[key] = 0; return launch_perm<E, Store>(plans[0], in, st, s); }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) { set_error("cudaEventCreate failed"); return TB_ERR_CUDA; }
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); set_error("cudaEventCreate failed"); return TB_ERR_CUDA; }
+  float best_ms = 0.f, ms0 = 0.f;
+  int best = 0, err = 0;
+  for (int k = 0; k < n && !err; ++k) {
+    if ((err = launch_perm<E, Store>(plans[k], in, st, s))) break;  // untimed: first launch of a variant
+    cudaEventRecord(e0, s);
+    if ((err = launch_perm<E, Store>(plans[k], in, st, s))) break;
+    cudaEventRecord(e1, s);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      set_error("timing a permutation plan failed");
+      err = TB_ERR_CUDA;
+      break;
+    }
+    if (k == 0) { ms0 = best_ms = ms; best = 0; }
+    else if (ms < best_ms) { best_ms = ms; best = k; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err) return err;
+  if (best != 0 && best_ms > 0.98f * ms0) best = 0;
+  g_tune[key] = idx[best];
+  return 0;
+}
+
 // Runs a permutation with the tiled engine, or the scatter kernel when the
 // plan builder declines the layout.
 template <typename E, typename Store>
@@ -144,19 +244,30 @@ int tensor_copy_impl(int dtk, int rank, const int* dims, const int* cptrn, const
   int ident[kMaxRank];
   if (!cptrn) { for (int i = 0; i < rank; ++i) ident[i] = i + 1; cptrn = ident; }
   bool conj = ((conj_bits & 1) ^ ((conj_bits >> 1) & 1)) && is_complex(dtk);
+  if (scatter) {
+    switch (es) {
+      case 4: return run_scatter<uint32_t>(rank, dims, cptrn, (const uint32_t*)in, StoreCopy<uint32_t>{(uint32_t*)out}, s);
+      case 8:
+        if (conj) return run_scatter<uint64_t>(rank, dims, cptrn, (const uint64_t*)in, StoreConjC4{(uint64_t*)out}, s);
+        return run_scatter<uint64_t>(rank, dims, cptrn, (const uint64_t*)in, StoreCopy<uint64_t>{(uint64_t*)out}, s);
+      case 16:
+        if (conj) return run_scatter<u128>(rank, dims, cptrn, (const u128*)in, StoreConjC8{(u128*)out}, s);
+        return run_scatter<u128>(rank, dims, cptrn, (const u128*)in, StoreCopy<u128>{(u128*)out}, s);
+    }
+    return TB_ERR_INVALID_ARGS;
+  }
   switch (es) {
-    case 4: return run_permutation<uint32_t>(rank, dims, cptrn, (const uint32_t*)in,
-                                             StoreCopy<uint32_t>{(uint32_t*)out}, s, scatter);
+    case 4: return run_copy_measured<uint32_t>(rank, dims, cptrn, (const uint32_t*)in,
+                                               StoreCopy<uint32_t>{(uint32_t*)out}, s);
     case 8:
-      if (conj) return run_permutation<uint64_t>(rank, dims, cptrn, (const uint64_t*)in,
-                                                 StoreConjC4{(uint64_t*)out}, s, scatter);
-      return run_permutation<uint64_t>(rank, dims, cptrn, (const uint64_t*)in,
-                                       StoreCopy<uint64_t>{(uint64_t*)out}, s, scatter);
+      if (conj) return run_copy_measured<uint64_t>(rank, dims, cptrn, (const uint64_t*)in,
+                                                   StoreConjC4{(uint64_t*)out}, s);
+      return run_copy_measured<uint64_t>(rank, dims, cptrn, (const uint64_t*)in,
+                                         StoreCopy<uint64_t>{(uint64_t*)out}, s);
     case 16:
-      if (conj) return run_permutation<u128>(rank, dims, cptrn, (const u128*)in,
-                                             StoreConjC8{(u128*)out}, s, scatter);
-      return run_permutation<u128>(rank, dims, cptrn, (const u128*)in, StoreCopy<u128>{(u128*)out},
-                                   s, scatter);
+      if (conj) return run_copy_measured<u128>(rank, dims, cptrn, (const u128*)in,
+                                               StoreConjC8{(u128*)out}, s);
+      return run_copy_measured<u128>(rank, dims, cptrn, (const u128*)in, StoreCopy<u128>{(u128*)out}, s);
   }
   return TB_ERR_INVALID_ARGS;
 }

@@ -51,8 +51,8 @@ int main(int argc, char** argv) {
   if (vecpath) {
     const int VB = P.vbytes, VW = VB / es;
     if (P.vec2d && P.rows2d) { printf("FAIL vec2d and rows2d both set\n"); return 1; }
-    if (P.rows2d && (P.nA != P.nB || P.LA != P.LB || P.ej_pb_stride != 1 || P.chunk_eb != P.lap ||
-                     P.chunk_sout == 0 || (P.LA * es) % VB != 0)) {
+    if (P.rows2d && (P.nA != P.nB || P.LA != P.LB || P.ej_pb_stride != 1 ||
+                     (P.nA > 1 && (P.chunk_eb != P.lap || P.chunk_sout == 0)) || (P.LA * es) % VB != 0)) {
       printf("FAIL rows2d shape\n"); return 1;
     }
     gl = {P.nvec, P.nA, VB, (long long)P.lap * es, VW, P.row_sin};

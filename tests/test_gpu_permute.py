@@ -114,6 +114,22 @@ def test_two_dimensional_paths_permute_add(xt, dev, dtk):
             assert np.array_equal(got.view(np.uint8), ref.view(np.uint8)), (dims, perm)
 
 
+@pytest.mark.parametrize("dtk,dims,perm", [(O.R8, [64, 64, 48, 32], (2, 3, 1, 4)),
+                                           (O.R4, [96, 80, 60, 40], (3, 4, 1, 2)),
+                                           (O.C4, [64, 64, 48, 32], (4, 3, 2, 1))])
+def test_measured_plan_choice_bit_exact(xt, dev, dtk, dims, perm):
+    """Copies of 32 MB and more time a few plans on their first call and keep
+    the fastest: the first (timing) call and the later (cached) ones all give
+    the oracle's bits."""
+    x = rand_host(dtk, int(np.prod(dims)), 91)
+    ref = O.permute(x, dims, perm).view(np.uint8)
+    for _ in range(2):
+        assert np.array_equal(gpu_permute(xt, dev, x, dims, perm).view(np.uint8), ref)
+    if dtk == O.C4:
+        got = gpu_permute(xt, dev, x, dims, perm, conj_bits=1)
+        assert np.array_equal(got.view(np.uint8), O.permute(x, dims, perm, conj=True).view(np.uint8))
+
+
 def test_skewed_extents(xt, dev):
     for dims, perm in [([3, 300, 250], [3, 1, 2]), ([2, 90, 90, 9], [4, 3, 2, 1]), ([700, 7, 5, 40], [2, 4, 1, 3]),
                        ([6, 5, 4, 3, 2, 30], [6, 1, 5, 2, 4, 3])]:

@@ -27,9 +27,9 @@ def emul():
     return exe
 
 
-def run(exe, es, dims, perm):
+def run(exe, es, dims, perm, env=None):
     out = subprocess.run([exe, str(es), str(len(dims))] + [str(x) for x in dims] + [str(p) for p in perm],
-                         capture_output=True, text=True)
+                         capture_output=True, text=True, env=env)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.startswith("OK"), (dims, perm, out.stdout)
 
@@ -81,3 +81,32 @@ def test_two_dimensional_vector_paths(emul, es):
     for dims in ([90, 90, 30, 30], [90, 30, 90, 30], [66, 70, 18, 22], [100, 37, 45, 12], [38, 38, 38, 38]):
         for perm in ([1, 3, 2, 4], [2, 1, 3, 4], [2, 4, 1, 3], [1, 4, 3, 2], [3, 1, 2, 4], [4, 2, 3, 1]):
             run(emul, es, dims, perm)
+
+
+@pytest.mark.parametrize("vmin,vmax", [(8, 24), (24, 48)])
+def test_measured_choice_tile_bounds(emul, vmin, vmax):
+    # the other tile-size bounds that large copies may be timed with and run
+    env = dict(os.environ, TB_PERM_VMIN_KB=str(vmin), TB_PERM_VMAX_KB=str(vmax))
+    for es in (4, 8, 16):
+        for perm in itertools.permutations([1, 2, 3, 4]):
+            run(emul, es, [40, 40, 40, 40] if es != 16 else [20, 20, 20, 20], perm, env)
+            run(emul, es, [7, 5, 3, 9], perm, env)
+    for es in (4, 8):
+        for dims in ([90, 90, 30, 30], [66, 70, 18, 22], [100, 37, 45, 12]):
+            for perm in ([1, 3, 2, 4], [2, 1, 3, 4], [2, 4, 1, 3], [3, 4, 1, 2], [4, 3, 2, 1]):
+                run(emul, es, dims, perm, env)
+    rng = random.Random(77 + vmin)
+    for _ in range(60):
+        rank = rng.randint(2, 6)
+        dims = [rng.randint(2, 40) for _ in range(rank)]
+        while True:
+            vol = 1
+            for x in dims:
+                vol *= x
+            if vol <= 400000:
+                break
+            i = max(range(rank), key=lambda k: dims[k])
+            dims[i] = max(1, dims[i] // 2)
+        perm = list(range(1, rank + 1))
+        rng.shuffle(perm)
+        run(emul, rng.choice([4, 8, 16]), dims, perm, env)
