@@ -81,7 +81,7 @@ class Clocks:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -288,6 +288,49 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs):
                 "cases": "24 rank-4 perms x {R8 76^4 (254.5 MiB), R4 90^4 (250.3 MiB)}, bit-exact",
                 "timing": "10 back-to-back calls per permutation, one queued before the start event; "
                           "plans picked by the library's measured choice on the first call"})
+    return out
+
+
+def permute_sweep_repeated(X, stream, stream_obj, reps=3):
+    """The permutation sweep's 48 cases, `reps` times after 0.5 s of copies
+    that let the clocks settle; per-case medians, their aggregate
+    (bytes over time) and the mean relative spread of the repetitions.
+    Library knobs set in the environment (TB_PERM_TUNE, TB_PERM_FAST,
+    TB_PERM_VMIN_KB/VMAX_KB) apply, so variants can be compared."""
+    import itertools
+
+    import torch
+    bufs = {}
+    for dtk, n in ((8, 76), (4, 90)):
+        es = X.ELEM_BYTES[dtk]
+        v = n ** 4
+        a = torch.empty(v * es, dtype=torch.uint8, device="cuda")
+        b = torch.empty_like(a)
+        X.fill_uniform(dtk, v, a.data_ptr(), 3, stream=stream)
+        bufs[dtk] = (n, v, es, a, b)
+    t0 = time.time()
+    while time.time() - t0 < 0.5:
+        for dtk, (n, v, es, a, b) in bufs.items():
+            X.tensor_copy(dtk, [n] * 4, (2, 1, 3, 4), a.data_ptr(), b.data_ptr(), 0, stream)
+        torch.cuda.synchronize()
+    perms = list(itertools.permutations([1, 2, 3, 4]))
+    runs = {dtk: [[] for _ in perms] for dtk in bufs}
+    for _ in range(reps):
+        for dtk, (n, v, es, a, b) in bufs.items():
+            for i, perm in enumerate(perms):
+                ms = time_back_to_back(lambda: X.tensor_copy(dtk, [n] * 4, perm, a.data_ptr(), b.data_ptr(), 0,
+                                                             stream), 10, stream_obj) / 10
+                runs[dtk][i].append(2.0 * v * es / 1e9 / (ms / 1e3))
+    out, tot_b, tot_s = {}, 0.0, 0.0
+    for dtk, key in ((8, "r8"), (4, "r4")):
+        n, v, es, _, _ = bufs[dtk]
+        med = [statistics.median(x) for x in runs[dtk]]
+        out[key] = {"".join(map(str, p)): round(m) for p, m in zip(perms, med)}
+        out[key + "_spread"] = round(statistics.mean((max(x) - min(x)) / statistics.median(x) for x in runs[dtk]), 3)
+        tot_b += 24 * 2.0 * v * es / 1e9
+        tot_s += sum(2.0 * v * es / 1e9 / m for m in med)
+    out["GB/s"] = round(tot_b / tot_s, 1)
+    out["env"] = {k: os.environ.get(k) for k in ("TB_PERM_TUNE", "TB_PERM_FAST", "TB_PERM_VMIN_KB", "TB_PERM_VMAX_KB")}
     return out
 
 
@@ -632,6 +675,9 @@ def run_profile(args):
                                                                 nseg=args.v or None, hi=args.o or None,
                                                                 run_loop=not (args.v or args.o))}))
         return
+    if args.profile == "permsweep":
+        print(json.dumps({"profile": "permsweep", **permute_sweep_repeated(X, s, s_obj, reps=max(1, args.steps))}))
+        return
     if args.profile == "permute":
         n = args.v or 76
         v = n ** 4
@@ -666,7 +712,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
     ap.add_argument("--no-block-sparse", action="store_true", help="skip the block-sparse measurement")
-    ap.add_argument("--profile", choices=["contract", "plain", "permute", "bsc", "selector"], default=None,
+    ap.add_argument("--profile", choices=["contract", "plain", "permute", "permsweep", "bsc", "selector"], default=None,
                     help="run one part on a small case for a profiler (no bench line)")
     ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n; bsc: segments per index)")
     ap.add_argument("--o", type=int, default=0, help="--profile: occupied extent (bsc: largest segment)")
