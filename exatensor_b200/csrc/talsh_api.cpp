@@ -26,6 +26,7 @@ namespace {
 struct DevState {
   bool on = false;
   cudaStream_t stream = nullptr;
+  cudaStream_t xstream = nullptr;  // host-to-device slices of streamed contractions
   bool fast_math = true;
   double flops = 0.0;
 };
@@ -162,6 +163,7 @@ extern "C" int talshShutdown(void) {
     cudaSetDevice(g);
     cudaStreamSynchronize(g_dev[g].stream);
     cudaStreamDestroy(g_dev[g].stream);
+    if (g_dev[g].xstream) { cudaStreamSynchronize(g_dev[g].xstream); cudaStreamDestroy(g_dev[g].xstream); }
     g_dev[g] = DevState();
   }
   g_ngpu = 0;
@@ -633,15 +635,22 @@ struct Operand {
   talsh_tens_t* t = nullptr;
   int src = -1;          // source image index
   bool moved = false;    // a new image was created on the execution GPU
+  bool sliced = false;   // streamed to the GPU in slices by the computation itself
   void* dptr = nullptr;  // body on the execution GPU
   size_t bytes = 0;
 };
 
 // Prepares one operand on the execution GPU (H2D when its image is elsewhere).
+// A sliced operand only gets its source: its host image.
 int stage_operand(Operand& op, int gpu, int dtk, cudaStream_t s) {
   talsh_tens_t* t = op.t;
   const int flat = flat_gpu(gpu);
   op.bytes = volume_of(t) * elem_size(dtk);
+  if (op.sliced) {
+    for (int j = 0; j < t->ndev; ++j)
+      if (t->avail[j] == YEP && t->data_kind[j] == dtk && t->dev_rsc[j].dev_id == 0) { op.src = j; return 0; }
+    return TALSH_NOT_FOUND;
+  }
   int i = find_image(t, flat);
   if (i >= 0 && t->data_kind[i] == dtk) { op.src = i; op.dptr = t->dev_rsc[i].gmem_p; return 0; }
   i = -1;
@@ -665,6 +674,15 @@ int stage_operand(Operand& op, int gpu, int dtk, cudaStream_t s) {
 void settle_operand(Operand& op, int coh, bool is_out, int gpu, int dtk, cudaStream_t s, TaskImpl* ti) {
   talsh_tens_t* t = op.t;
   const int flat = flat_gpu(gpu);
+  if (op.sliced) {  // an input read from its host image: only COPY_D has something to do
+    if (coh == COPY_D) {
+      void* p = t->dev_rsc[op.src].gmem_p;
+      ti->finalize.push_back([t, p]() {
+        for (int i = 0; i < t->ndev; ++i) if (t->dev_rsc[i].gmem_p == p) { remove_image(t, i); break; }
+      });
+    }
+    return;
+  }
   if (!op.moved) {
     if (coh == COPY_D) ti->finalize.push_back([t, flat]() { int i = find_image(t, flat); if (i >= 0) remove_image(t, i); });
     return;
@@ -699,7 +717,7 @@ using Compute = std::function<int(cudaStream_t, std::vector<Operand>&)>;
 
 // Runs an operation on a GPU: stages operands, computes, settles coherence.
 int run_op(std::vector<talsh_tens_t*> args, int copy_ctrl, int dev_id, int dev_kind, talsh_task_t* task,
-           const Compute& compute, double flops) {
+           const Compute& compute, double flops, const std::vector<char>* sliced = nullptr) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (!g_on) return TALSH_NOT_INITIALIZED;
   for (auto* t : args) {
@@ -723,6 +741,7 @@ int run_op(std::vector<talsh_tens_t*> args, int copy_ctrl, int dev_id, int dev_k
   int err = 0;
   for (size_t i = 0; i < args.size() && !err; ++i) {
     ops[i].t = args[i];
+    ops[i].sliced = sliced && i < sliced->size() && (*sliced)[i];
     err = stage_operand(ops[i], gpu, dtk, s);
   }
   if (err) {
@@ -835,6 +854,172 @@ extern "C" int talshTensorAdd(const char* cptrn, talsh_tens_t* dtens, talsh_tens
                 }, flops);
 }
 
+namespace {
+
+// ---- streamed contractions -------------------------------------------------
+// TAL-SH splits an operation whose operands exceed the device buffer into
+// sub-operations by halving dimensions (talshTensorOpDecompose2,
+// talshc.cpp:3150) and runs them from the host (talshTensorOpProgress :2929,
+// ContractXL :5394).  Here a contraction whose inputs L and R live only on
+// the host (copy control COPY_T or COPY_D) and are large streams instead:
+//   - it is split along the slowest index of L (or of R) when that index is
+//     contracted, so that L's slices are contiguous host ranges; the other
+//     operand's slices are one 2-D strided copy each;
+//   - slices move host-to-device on a copy stream into a ring of three
+//     buffers while the compute stream contracts the previous slices into D
+//     (D += slice products; the first slice applies the caller's
+//     accumulative flag), ordered by events;
+//   - D is staged whole, as for any contraction.
+// Transfers overlap the computation, and L and R need not fit in HBM.  Each
+// slice is an ordinary contraction (same method choice), so results agree
+// with the unsliced contraction within its error bound, not bit for bit
+// (the sums are split along K).  TB_STREAM=0 turns it off;
+// TB_STREAM_MIN_MB (default 1024) is the size of L plus R from which it runs.
+struct SliceSpec {
+  int big = 0;              // 1: slices of L are contiguous (its slowest index), 2: of R
+  int bpos = -1, opos = -1; // position of the sliced index in that operand and in the other
+  int64_t ext = 0, step = 0;
+};
+
+constexpr int kSliceRing = 3;
+constexpr int64_t kSliceTargetBytes = (int64_t)512 << 20;
+
+int64_t prod_dims(const int* d, int a, int b) {
+  int64_t p = 1;
+  for (int i = a; i < b; ++i) p *= d[i];
+  return p;
+}
+
+bool host_only(const talsh_tens_t* t, int dtk, int gpu) {
+  bool host = false;
+  for (int j = 0; j < t->ndev; ++j) {
+    if (t->avail[j] != YEP) continue;
+    if (t->dev_rsc[j].dev_id == flat_gpu(gpu)) return false;
+    if (t->dev_rsc[j].dev_id == 0 && t->data_kind[j] == dtk) host = true;
+  }
+  return host;
+}
+
+SliceSpec plan_slices(const tb::ParsedPattern& P, const talsh_tens_t* l, const talsh_tens_t* r, int dtk,
+                      int copy_ctrl, int dev_id, int dev_kind) {
+  SliceSpec sp;
+  const char* on = std::getenv("TB_STREAM");
+  if (on && on[0] == '0') return sp;
+  const char* mb = std::getenv("TB_STREAM_MIN_MB");
+  const int64_t min_bytes = (mb ? std::atoll(mb) : 1024) << 20;
+  int gpu = -1;
+  if (resolve_gpu(dev_id, dev_kind, &gpu) || P.hyper) return sp;
+  for (int a = 1; a <= 2; ++a) {
+    const int c = coh_of(copy_ctrl, 3, a);
+    if (c != COPY_T && c != COPY_D) return sp;
+  }
+  if (!host_only(l, dtk, gpu) || !host_only(r, dtk, gpu)) return sp;
+  const int64_t es = elem_size(dtk);
+  const int64_t bytes = ((int64_t)volume_of(l) + (int64_t)volume_of(r)) * es;
+  if (bytes < min_bytes || bytes == 0) return sp;
+  const int* ld = l->shape_p->dims;
+  const int* rd = r->shape_p->dims;
+  if (P.lrank >= 1 && P.cptrn[P.lrank - 1] < 0) {
+    sp.big = 1; sp.bpos = P.lrank - 1; sp.opos = -P.cptrn[P.lrank - 1] - 1; sp.ext = ld[sp.bpos];
+  } else if (P.rrank >= 1 && P.cptrn[P.lrank + P.rrank - 1] < 0) {
+    sp.big = 2; sp.bpos = P.rrank - 1; sp.opos = -P.cptrn[P.lrank + P.rrank - 1] - 1; sp.ext = rd[sp.bpos];
+  } else {
+    return SliceSpec();
+  }
+  if (sp.ext < 2) return SliceSpec();
+  // the other operand's slices are 2-D copies: its row pitch must be legal
+  const int* od = sp.big == 1 ? rd : ld;
+  const int orank = sp.big == 1 ? P.rrank : P.lrank;
+  const int64_t opitch = prod_dims(od, 0, sp.opos) * sp.ext * es;
+  if (prod_dims(od, sp.opos + 1, orank) > 1 && opitch >= ((int64_t)1 << 31)) return SliceSpec();
+  const int64_t bigbytes = (int64_t)volume_of(sp.big == 1 ? l : r) * es;
+  int64_t nsl = std::max<int64_t>(kSliceRing, (bigbytes + kSliceTargetBytes - 1) / kSliceTargetBytes);
+  nsl = std::min<int64_t>(nsl, sp.ext);
+  sp.step = (sp.ext + nsl - 1) / nsl;
+  return sp;
+}
+
+// The streamed computation (runs as run_op's compute step on stream s).
+int contract_streamed(const tb::ParsedPattern& P, const SliceSpec& sp, int dtk, talsh_tens_t* dtens,
+                      talsh_tens_t* ltens, talsh_tens_t* rtens, double sr, double si, int accumulative,
+                      const tb_plan_t* plan, cudaStream_t s, std::vector<Operand>& o) {
+  int g = 0;
+  cudaGetDevice(&g);
+  if (!g_dev[g].xstream && cudaStreamCreateWithFlags(&g_dev[g].xstream, cudaStreamNonBlocking) != cudaSuccess)
+    return TALSH_FAILURE;
+  cudaStream_t xs = g_dev[g].xstream;
+  const int64_t es = elem_size(dtk);
+  talsh_tens_t* big = sp.big == 1 ? ltens : rtens;
+  talsh_tens_t* oth = sp.big == 1 ? rtens : ltens;
+  const int brank = sp.big == 1 ? P.lrank : P.rrank, orank = sp.big == 1 ? P.rrank : P.lrank;
+  const char* bh = (const char*)big->dev_rsc[o[sp.big].src].gmem_p;
+  const char* oh = (const char*)oth->dev_rsc[o[3 - sp.big].src].gmem_p;
+  int bd[MAX_TENSOR_RANK], od[MAX_TENSOR_RANK];
+  std::memcpy(bd, big->shape_p->dims, sizeof(int) * brank);
+  std::memcpy(od, oth->shape_p->dims, sizeof(int) * orank);
+  const int64_t inner_b = prod_dims(bd, 0, sp.bpos);
+  const int64_t inner_o = prod_dims(od, 0, sp.opos), outer_o = prod_dims(od, sp.opos + 1, orank);
+  const size_t bslice = (size_t)(inner_b * sp.step * es), oslice = (size_t)(inner_o * sp.step * outer_o * es);
+  void* bb[kSliceRing] = {nullptr, nullptr, nullptr};
+  void* ob[kSliceRing] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ready[kSliceRing], freed[kSliceRing], start = nullptr, copies_done = nullptr;
+  int err = 0, nev = 0;
+  for (int i = 0; i < kSliceRing && !err; ++i) {
+    if ((err = alloc_on(flat_gpu(g), bslice, &bb[i], s))) break;
+    if ((err = alloc_on(flat_gpu(g), oslice, &ob[i], s))) break;
+  }
+  for (int i = 0; i < kSliceRing && !err; ++i, ++nev)
+    if (cudaEventCreateWithFlags(&ready[i], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&freed[i], cudaEventDisableTiming) != cudaSuccess)
+      err = TALSH_FAILURE;
+  if (!err && (cudaEventCreateWithFlags(&start, cudaEventDisableTiming) != cudaSuccess ||
+               cudaEventCreateWithFlags(&copies_done, cudaEventDisableTiming) != cudaSuccess))
+    err = TALSH_FAILURE;
+  if (!err) {
+    cudaEventRecord(start, s);  // buffers allocated (stream-ordered on s)
+    cudaStreamWaitEvent(xs, start, 0);
+    const int64_t nsl = (sp.ext + sp.step - 1) / sp.step;
+    for (int64_t k = 0; k < nsl && !err; ++k) {
+      const int slot = (int)(k % kSliceRing);
+      const int64_t x0 = k * sp.step, w = std::min(sp.step, sp.ext - x0);
+      if (k >= kSliceRing) cudaStreamWaitEvent(xs, freed[slot], 0);
+      if (cudaMemcpyAsync(bb[slot], bh + x0 * inner_b * es, (size_t)(w * inner_b * es), cudaMemcpyHostToDevice, xs) !=
+          cudaSuccess) { err = TALSH_FAILURE; break; }
+      const size_t width = (size_t)(inner_o * w * es);
+      const cudaError_t ce =
+          outer_o == 1 ? cudaMemcpyAsync(ob[slot], oh + x0 * inner_o * es, width, cudaMemcpyHostToDevice, xs)
+                       : cudaMemcpy2DAsync(ob[slot], width, oh + x0 * inner_o * es, (size_t)(inner_o * sp.ext * es),
+                                           width, (size_t)outer_o, cudaMemcpyHostToDevice, xs);
+      if (ce != cudaSuccess) { err = TALSH_FAILURE; break; }
+      cudaEventRecord(ready[slot], xs);
+      cudaStreamWaitEvent(s, ready[slot], 0);
+      bd[sp.bpos] = (int)w;
+      od[sp.opos] = (int)w;
+      const void* lp = sp.big == 1 ? bb[slot] : ob[slot];
+      const void* rp = sp.big == 1 ? ob[slot] : bb[slot];
+      const int* ldims = sp.big == 1 ? bd : od;
+      const int* rdims = sp.big == 1 ? od : bd;
+      err = map_tb(tb_tensor_contract(P.cptrn, dtk, P.drank, dtens->shape_p->dims, o[0].dptr, P.lrank, ldims, lp,
+                                      P.rrank, rdims, rp, sr, si, P.conj_bits, k == 0 ? accumulative : YEP, plan, s));
+      cudaEventRecord(freed[slot], s);
+    }
+    // every copy into the ring precedes s before the buffers are released
+    cudaEventRecord(copies_done, xs);
+    cudaStreamWaitEvent(s, copies_done, 0);
+  }
+  if (err) cudaGetLastError();
+  for (int i = 0; i < kSliceRing; ++i) {
+    if (bb[i]) cudaFreeAsync(bb[i], s);
+    if (ob[i]) cudaFreeAsync(ob[i], s);
+  }
+  for (int i = 0; i < nev; ++i) { cudaEventDestroy(ready[i]); cudaEventDestroy(freed[i]); }
+  if (start) cudaEventDestroy(start);
+  if (copies_done) cudaEventDestroy(copies_done);
+  return err;
+}
+
+}  // namespace
+
 extern "C" int talshTensorContract(const char* cptrn, talsh_tens_t* dtens, talsh_tens_t* ltens, talsh_tens_t* rtens,
                                    double sr, double si, int dev_id, int dev_kind, int copy_ctrl, int accumulative,
                                    talsh_task_t* task) {
@@ -853,6 +1038,17 @@ extern "C" int talshTensorContract(const char* cptrn, talsh_tens_t* dtens, talsh
                     rtens->shape_p->dims, &Z))
     return TALSH_INVALID_ARGS;
   const double flops = ((dtk == C4 || dtk == C8) ? 8.0 : 2.0) * (double)Z.M * (double)Z.N * (double)Z.K;
+  const SliceSpec sp = plan_slices(P, ltens, rtens, dtk, copy_ctrl, dev_id, dev_kind);
+  if (sp.big) {
+    const std::vector<char> sliced{0, 1, 1};
+    return run_op({dtens, ltens, rtens}, copy_ctrl, dev_id, dev_kind, task,
+                  [&](cudaStream_t s, std::vector<Operand>& o) {
+                    int g = 0; cudaGetDevice(&g);
+                    tb_plan_t plan; std::memset(&plan, 0, sizeof(plan));
+                    plan.method = g_dev[g].fast_math ? TB_METHOD_AUTO : TB_METHOD_TTGT;
+                    return contract_streamed(P, sp, dtk, dtens, ltens, rtens, sr, si, accumulative, &plan, s, o);
+                  }, flops, &sliced);
+  }
   return run_op({dtens, ltens, rtens}, copy_ctrl, dev_id, dev_kind, task,
                 [&](cudaStream_t s, std::vector<Operand>& o) {
                   int g = 0; cudaGetDevice(&g);
@@ -866,9 +1062,9 @@ extern "C" int talshTensorContract(const char* cptrn, talsh_tens_t* dtens, talsh
 
 extern "C" int talshTensorContractXL(const char* cptrn, talsh_tens_t* dtens, talsh_tens_t* ltens, talsh_tens_t* rtens,
                                      double sr, double si, int dev_id, int dev_kind, int accumulative) {
-  // Every operand of this library's single-GPU scope fits in HBM, so the XL
-  // form runs as one blocking contraction (talshc.cpp:5394 splits only when
-  // the operands exceed the device buffer, :5517).
+  // The XL form is a blocking contraction (talshc.cpp:5394).  Host-resident
+  // inputs of 1 GiB and more stream through the GPU in slices (see
+  // contract_streamed), so they need not fit in HBM; D is staged whole.
   return talshTensorContract(cptrn, dtens, ltens, rtens, sr, si, dev_id, dev_kind, COPY_MTT, accumulative, nullptr);
 }
 

@@ -67,3 +67,113 @@ def test_error_codes(talsh):
     assert T.contract("D(a,b)+=L(a,k,b)*R(k,b)", d, h, r) == T.TALSH_NOT_IMPLEMENTED
     c = T.Tensor([4, 4], C4)
     assert T.contract("D(a,b)+=L(k,a)*R(k,b)", d, c, r) == T.TALSH_INVALID_ARGS
+
+
+# ---- streamed contractions (host-resident inputs in slices) ----------------
+def _fortran(x, dims):
+    return x.reshape(dims, order="F")
+
+
+def _contract_host(pattern, dd, ld, rd, l, r, d0, alpha, copy_ctrl, stream, dtk=R8):
+    """Runs one contraction through talshTensorContract with host tensors
+    (external memory) and returns D's host array; stream selects the sliced
+    path (TB_STREAM_MIN_MB=0) or the ordinary one (TB_STREAM=0)."""
+    import os
+    env = {"TB_STREAM": None if stream else "0", "TB_STREAM_MIN_MB": "0" if stream else None}
+    old = {k: os.environ.get(k) for k in env}
+    for k, v in env.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
+    try:
+        d = d0.copy()
+        td, tl, tr = T.Tensor(dd, dtk, ext=d), T.Tensor(ld, dtk, ext=l), T.Tensor(rd, dtk, ext=r)
+        assert T.contract(pattern, td, tl, tr, alpha, copy_ctrl=copy_ctrl) == 0
+        return d, (td, tl, tr)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_streamed_contraction_slices_left_operand(talsh):
+    # V(a,b,c,d): its slowest index d is contracted, so V streams in contiguous
+    # slices and T(c,d,i,j) in 2-D strided ones; D accumulates the slices
+    rng = np.random.default_rng(5)
+    v, o = 24, 8
+    ld, rd, dd = [v, v, v, v], [v, v, o, o], [v, v, o, o]
+    l = rng.uniform(-1, 1, int(np.prod(ld)))
+    r = rng.uniform(-1, 1, int(np.prod(rd)))
+    d0 = rng.uniform(-1, 1, int(np.prod(dd)))
+    pat = "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)"
+    got, _ = _contract_host(pat, dd, ld, rd, l, r, d0, 0.75, T.COPY_TTT, stream=True)
+    ref_dev, _ = _contract_host(pat, dd, ld, rd, l, r, d0, 0.75, T.COPY_TTT, stream=False)
+    ref = d0 + 0.75 * np.einsum("abcd,cdij->abij", _fortran(l, ld), _fortran(r, rd)).ravel(order="F")
+    assert _rel(got, ref) <= 1e-13
+    assert _rel(got, ref_dev) <= 1e-13
+
+
+def test_streamed_contraction_slices_right_operand(talsh):
+    # L's slowest index is free, R's slowest (k) is contracted: R streams in
+    # contiguous slices, L's slices are rows of a 2-D copy with inner extent 1
+    rng = np.random.default_rng(6)
+    ld, rd, dd = [50, 37], [41, 50], [37, 41]
+    l = rng.uniform(-1, 1, 50 * 37)
+    r = rng.uniform(-1, 1, 41 * 50)
+    d0 = np.zeros(37 * 41)
+    pat = "D(a,i)+=L(k,a)*R(i,k)"
+    got, _ = _contract_host(pat, dd, ld, rd, l, r, d0, 1.0, T.COPY_TTT, stream=True)
+    ref = np.einsum("ka,ik->ai", _fortran(l, ld), _fortran(r, rd)).ravel(order="F")
+    assert _rel(got, ref) <= 1e-13
+
+
+def test_streamed_contraction_complex_tensor_cores(talsh):
+    # large enough for the tensor-core path per slice (M = N = K = 1296),
+    # complex with a conjugated left operand; slices of d = 12 each
+    from exatensor_b200 import C8
+    rng = np.random.default_rng(7)
+    n = 36
+    ld, rd, dd = [n] * 4, [n] * 4, [n] * 4
+    vol = n ** 4
+    l = (rng.uniform(-1, 1, vol) + 1j * rng.uniform(-1, 1, vol)).astype(np.complex128)
+    r = (rng.uniform(-1, 1, vol) + 1j * rng.uniform(-1, 1, vol)).astype(np.complex128)
+    d0 = np.zeros(vol, dtype=np.complex128)
+    pat = "D(a,b,i,j)+=L+(a,b,c,d)*R(c,d,i,j)"
+    got, _ = _contract_host(pat, dd, ld, rd, l, r, d0, 1.0, T.COPY_TTT, stream=True, dtk=C8)
+    ref_dev, _ = _contract_host(pat, dd, ld, rd, l, r, d0, 1.0, T.COPY_TTT, stream=False, dtk=C8)
+    ref = np.einsum("abcd,cdij->abij", np.conj(_fortran(l, ld)), _fortran(r, rd)).ravel(order="F")
+    assert _rel(got, ref) <= 1e-12
+    assert _rel(ref_dev, ref) <= 1e-12
+
+
+def test_streamed_contraction_discards_inputs_on_copy_d(talsh):
+    rng = np.random.default_rng(8)
+    ld, rd, dd = [16, 16, 12], [12, 10], [16, 16, 10]
+    l = rng.uniform(-1, 1, 16 * 16 * 12)
+    r = rng.uniform(-1, 1, 120)
+    d0 = np.zeros(16 * 16 * 10)
+    copy_tdt = (T.COPY_T << 4) | (T.COPY_D << 2) | T.COPY_T
+    got, (td, tl, tr) = _contract_host("D(a,b,i)+=L(a,b,k)*R(k,i)", dd, ld, rd, l, r, d0, 1.0, copy_tdt,
+                                       stream=True)
+    ref = np.einsum("abk,ki->abi", _fortran(l, ld), _fortran(r, rd)).ravel(order="F")
+    assert _rel(got, ref) <= 1e-13
+    assert tl.presence() == [] and tr.presence() == [0]
+
+
+def test_streamed_contraction_uneven_slices(talsh):
+    # extent 7 in three slices of 3, 3 and 1
+    rng = np.random.default_rng(9)
+    ld, rd, dd = [30, 20, 7], [7, 25], [30, 20, 25]
+    l = rng.uniform(-1, 1, 30 * 20 * 7)
+    r = rng.uniform(-1, 1, 7 * 25)
+    d0 = rng.uniform(-1, 1, 30 * 20 * 25)
+    got, _ = _contract_host("D(a,b,i)+=L(a,b,k)*R(k,i)", dd, ld, rd, l, r, d0, -1.5, T.COPY_TTT, stream=True)
+    ref = d0 - 1.5 * np.einsum("abk,ki->abi", _fortran(l, ld), _fortran(r, rd)).ravel(order="F")
+    assert _rel(got, ref) <= 1e-13
