@@ -34,7 +34,10 @@ METRIC = "contraction TFLOP/s + permute GB/s, chosen vs plain form at stated FP6
 WORKLOADS = {
     "ccsd1_r8": dict(pattern="D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)", v=192, o=48, dtk=8),
     "ccsd2_r8": dict(pattern="D(a,i,b,j)+=W(a,k,c,i)*T(c,b,k,j)", v=192, o=48, dtk=8),
+    "ccsd1_c8": dict(pattern="D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)", v=192, o=48, dtk=18),
+    "ccsd2_c8": dict(pattern="D(a,i,b,j)+=W(a,k,c,i)*T(c,b,k,j)", v=192, o=48, dtk=18),
     "ccsd1_r4": dict(pattern="D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)", v=192, o=48, dtk=4),
+    "ccsd2_r4": dict(pattern="D(a,i,b,j)+=W(a,k,c,i)*T(c,b,k,j)", v=192, o=48, dtk=4),
 }
 VIRT = set("abcd")
 # dram__bytes_read.sum + dram__bytes_write.sum of tc_gemm_kernel on the v=96 case
@@ -161,12 +164,14 @@ class ContractionCase:
         X.tensor_init(wl["dtk"], vol(self.dd), self.D.data_ptr(), 0.0, stream=stream)
         cp, *_ = X.parse_pattern(wl["pattern"])
         self.cptrn = cp
-        self.flops = 2.0 * vol(self.dd) * (vol(self.ld) * vol(self.rd) / vol(self.dd)) ** 0.5
+        # 2*M*N*K, or 8*M*N*K for complex data (the reference's accounting)
+        cplx = wl["dtk"] in (14, 18)
+        self.flops = (8.0 if cplx else 2.0) * vol(self.dd) * (vol(self.ld) * vol(self.rd) / vol(self.dd)) ** 0.5
 
-    def run(self, method, accumulative=True):
+    def run(self, method, accumulative=True, plan=None):
         X = self.X
         X.tensor_contract(self.cptrn, self.wl["dtk"], self.dd, self.D.data_ptr(), self.ld, self.L.data_ptr(),
-                          self.rd, self.R.data_ptr(), 1.0, 0, accumulative, X.make_plan(method), self.s)
+                          self.rd, self.R.data_ptr(), 1.0, 0, accumulative, plan or X.make_plan(method), self.s)
 
 
 def time_steps(fn, steps, warmup, world, stream_obj, on_timed=None):
@@ -211,43 +216,78 @@ def time_back_to_back(fn, steps, stream_obj):
 
 def sample_error(X, case, method, nsamp=48):
     """Relative Frobenius and max-abs error of sampled D elements against the
-    double-double oracle (each a K-length dot product), after one
-    non-accumulating contraction."""
+    double-double oracle (each a K-length dot product of the operands'
+    elements gathered on the device), after one non-accumulating contraction.
+    Any contraction pattern without conjugation; real or complex data."""
     import numpy as np
     import torch
 
     import oracle as O
     case.run(method, accumulative=False)
     torch.cuda.synchronize()
-    M = 1
-    cptrn = case.cptrn
-    lrank = len(case.ld)
-    for i, c in enumerate(cptrn[:lrank]):
-        if c > 0:
-            M *= case.ld[i]
-    N = vol(case.dd) // M
-    K = vol(case.ld) // M
     dt = O.NP_DTYPE[case.wl["dtk"]]
-    tdt = {np.float64: torch.float64, np.float32: torch.float32}[dt]
-    Dm = case.D.view(tdt)
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32,
+           np.dtype(np.complex128): torch.complex128, np.dtype(np.complex64): torch.complex64}[np.dtype(dt)]
+
+    def strides(d):
+        st = [1]
+        for x in d[:-1]:
+            st.append(st[-1] * x)
+        return st
+    cptrn = list(case.cptrn)
+    lr, rr = len(case.ld), len(case.rd)
+    Ls, Rs, Ds = strides(case.ld), strides(case.rd), strides(case.dd)
+    pairs = [(i, -cptrn[i] - 1) for i in range(lr) if cptrn[i] < 0]
+    grids = torch.meshgrid(*[torch.arange(case.ld[i], device="cuda", dtype=torch.int64) for i, _ in pairs],
+                           indexing="ij")
+    loff = sum(g.reshape(-1) * Ls[i] for g, (i, _) in zip(grids, pairs))
+    roff = sum(g.reshape(-1) * Rs[j] for g, (_, j) in zip(grids, pairs))
+    K = int(loff.numel())
+    Lv, Rv, Dv = case.L.view(tdt), case.R.view(tdt), case.D.view(tdt)
     rng = np.random.default_rng(5)
-    # only the V(a,b,c,d)*T(c,d,i,j) layout is sampled directly: L = [K][M] m-fastest, R = [N][K]
-    if case.wl["pattern"] != "D(a,b,i,j)+=V(a,b,c,d)*T(c,d,i,j)":
-        return None
-    Lm = case.L.view(tdt).view(K, M)
-    Rm = case.R.view(tdt).view(N, K)
     num = den = mx = 0.0
     for _ in range(nsamp):
-        m, n = int(rng.integers(M)), int(rng.integers(N))
-        lv = Lm[:, m].double().cpu().numpy()
-        rv = Rm[n, :].double().cpu().numpy()
-        ref = np.zeros(1)
+        dix = [int(rng.integers(x)) for x in case.dd]
+        lb = sum(dix[cptrn[i] - 1] * Ls[i] for i in range(lr) if cptrn[i] > 0)
+        rb = sum(dix[cptrn[lr + j] - 1] * Rs[j] for j in range(rr) if cptrn[lr + j] > 0)
+        lv = np.ascontiguousarray(Lv[lb + loff].cpu().numpy())
+        rv = np.ascontiguousarray(Rv[rb + roff].cpu().numpy())
+        ref = np.zeros(1, dtype=dt)
         O.contract([-1, -1], ref, [], lv, [K], rv, [K], 1.0, 0, True, mode=1)
-        got = float(Dm[m + n * M].item())
-        num += (got - ref[0]) ** 2
-        den += ref[0] ** 2
-        mx = max(mx, abs(got - ref[0]))
+        got = complex(Dv[sum(x * st for x, st in zip(dix, Ds))].item())
+        e = abs(got - complex(ref[0]))
+        num += e * e
+        den += abs(complex(ref[0])) ** 2
+        mx = max(mx, e)
     return {"rel_frobenius": (num / den) ** 0.5, "max_abs": mx, "samples": nsamp}
+
+
+def configs_case(X, s, s_obj, names, steps, warmup):
+    """Chosen (plan selector) and plain TTGT forms of each CCSD-like workload:
+    device-timed TFLOP/s and sampled errors against the double-double oracle."""
+    import torch
+    out = []
+    for name in names:
+        wl = WORKLOADS[name]
+        case = ContractionCase(X, wl, s)
+        ms = time_steps(lambda: case.run(X.METHOD_AUTO), steps, warmup, 1, s_obj) / steps
+        st = X.last_contract_stats()
+        pms = time_steps(lambda: case.run(X.METHOD_TTGT), steps, 1, 1, s_obj) / steps
+        e_c = sample_error(X, case, X.METHOD_AUTO, 24)
+        e_p = sample_error(X, case, X.METHOD_TTGT, 24)
+        rec = {"workload": name, "pattern": wl["pattern"], "data_kind": wl["dtk"], "flop": case.flops,
+               "chosen": {"method": {1: "ttgt", 2: "tensor cores"}.get(st.method, st.method), "slices": st.slices,
+                          "products": st.products, "tile_n": st.tile_n, "tile_m": st.tile_m, "ms": round(ms, 3),
+                          "TFLOP/s": round(case.flops / (ms / 1e3) / 1e12, 2), "rel_frobenius": e_c["rel_frobenius"]},
+               "plain": {"ms": round(pms, 3), "TFLOP/s": round(case.flops / (pms / 1e3) / 1e12, 2),
+                         "rel_frobenius": e_p["rel_frobenius"]},
+               "chosen_over_plain": round(pms / ms, 3)}
+        out.append(rec)
+        print(json.dumps(rec), flush=True)
+        del case
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
 
 
 def permute_sweep(X, stream, stream_obj, hbm_gbs):
@@ -635,10 +675,11 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if wl["dtk"] == 8 else "f32",
+            "scaling": "weak", "vs_baseline": None, "dtype": {4: "f32", 8: "f64", 14: "c64", 18: "c128"}[wl["dtk"]],
             "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v, D=0)",
             "config": {"workload": f"{args.workload}: {wl['pattern']} v={wl['v']} o={wl['o']}",
-                       "method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products, "tile_n": st.tile_n,
+                       "method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products,
+                       "tile_n": st.tile_n, "tile_m": st.tile_m,
                        "l2": "inputs larger than L2 (V alone is 10.9 GB)", "parallelism": f"replicas x{world}"},
             "plain": {"value": round(plain, 3), "unit": "TFLOP/s", "method": "ttgt (permute + FP64 DMMA GEMM)",
                       "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),
@@ -678,6 +719,10 @@ def run_profile(args):
                                                                 nseg=args.v or None, hi=args.o or None,
                                                                 run_loop=not (args.v or args.o))}))
         return
+    if args.profile == "configs":
+        names = [w for w in (args.workloads or "").split(",") if w] or list(WORKLOADS)
+        configs_case(X, s, s_obj, names, max(1, args.steps), max(1, args.warmup))
+        return
     if args.profile == "e2e":
         wl = dict(WORKLOADS[args.workload])
         wl["v"] = args.v or wl["v"]
@@ -704,11 +749,16 @@ def run_profile(args):
     wl["o"] = args.o or wl["o"]
     case = ContractionCase(X, wl, s)
     method = X.METHOD_AUTO if args.profile == "contract" else X.METHOD_TTGT
-    ms = time_steps(lambda: case.run(method), args.steps, args.warmup, 1, s_obj)
+    plan = None
+    if args.plan:  # e.g. "method=2,tile_n=256,tile_m=256,slices=6"
+        kw = {k: int(v) for k, v in (x.split("=") for x in args.plan.split(","))}
+        plan = X.make_plan(**kw)
+    ms = time_steps(lambda: case.run(method, plan=plan), args.steps, args.warmup, 1, s_obj)
     X.device_check(s)
     st = X.last_contract_stats()
     print(json.dumps({"profile": args.profile, "workload": args.workload, "v": wl["v"], "o": wl["o"],
                       "method": st.method, "slices": st.slices, "products": st.products, "tile_n": st.tile_n,
+                      "tile_m": st.tile_m,
                       "ms_per_step": round(ms / args.steps, 3),
                       "TFLOP/s": round(case.flops * args.steps / (ms / 1e3) / 1e12, 3)}))
 
@@ -720,8 +770,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
+    ap.add_argument("--workloads", default=None, help="--profile configs: comma-separated workloads (default all)")
+    ap.add_argument("--plan", default=None, help="--profile contract: explicit plan, e.g. method=2,tile_n=256,tile_m=256")
     ap.add_argument("--no-block-sparse", action="store_true", help="skip the block-sparse measurement")
-    ap.add_argument("--profile", choices=["contract", "plain", "permute", "permsweep", "bsc", "selector", "e2e"],
+    ap.add_argument("--profile", choices=["contract", "plain", "permute", "permsweep", "bsc", "selector", "e2e",
+                                          "configs"],
                     default=None,
                     help="run one part on a small case for a profiler (no bench line)")
     ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n; bsc: segments per index)")

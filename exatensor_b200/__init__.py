@@ -43,7 +43,7 @@ class Plan(C.Structure):
 class ContractStats(C.Structure):
     _fields_ = [("method", C.c_int), ("slices", C.c_int), ("passes", C.c_int), ("gemm_launches", C.c_int),
                 ("m", C.c_longlong), ("n", C.c_longlong), ("k", C.c_longlong), ("flops", C.c_double),
-                ("products", C.c_int), ("tile_n", C.c_int)]
+                ("products", C.c_int), ("tile_n", C.c_int), ("tile_m", C.c_int)]
 
 
 class BlockTask(C.Structure):

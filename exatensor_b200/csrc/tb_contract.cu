@@ -328,20 +328,26 @@ int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* 
     // learned selector when installed, else the size rule
     float f[TB_DESC_FEATURES];
     int idx = -1;
-    bool ambiguous = false;
+    unsigned tune = 0;
     uint64_t key = 0;
     descriptor_of(Z, dtk, f);
-    if (selector_pick(f, &idx, &ambiguous, &key) == 0) {
-      if (ambiguous) {
-        // too close to call: time every candidate once with alpha = 0, beta = 1 (D unchanged)
+    auto candidate = [&](int c) {
+      tb_plan_t cp = plan ? *plan : tb_plan_t{};
+      cp.method = c == 0 ? TB_METHOD_TTGT : TB_METHOD_FUSED;
+      cp.tile_n = c == 1 ? 128 : (c >= 2 ? 256 : 0);
+      cp.tile_m = c == kCandPair ? 256 : 0;
+      return cp;
+    };
+    if (selector_pick(f, &idx, &tune, &key) == 0) {
+      if (tune) {
+        // time each candidate in the mask once with alpha = 0, beta = 1 (D unchanged)
         float best = 1e30f;
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        for (int c = 0; c < TB_SELECT_PLANS; ++c) {
-          tb_plan_t cp = plan ? *plan : tb_plan_t{};
-          cp.method = c == 0 ? TB_METHOD_TTGT : TB_METHOD_FUSED;
-          cp.tile_n = c == 1 ? 128 : (c == 2 ? 256 : 0);
+        for (int c = 0; c < kNumCandidates; ++c) {
+          if (!(tune & (1u << c))) continue;
+          tb_plan_t cp = candidate(c);
           // one untimed run (first-use costs), then the timed one
           int ce = run_method(Z, dtk, ddims, d, ldims, l, rdims, r, 0.0, 0.0, 1, lconj, rconj, &cp, s);
           cudaEventRecord(e0, s);
@@ -362,9 +368,7 @@ int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* 
         g_stats.m = Z.M; g_stats.n = Z.N; g_stats.k = Z.K;
         g_stats.flops = (cplx ? 8.0 : 2.0) * (double)Z.M * (double)Z.N * (double)Z.K;
       }
-      learned = plan ? *plan : tb_plan_t{};
-      learned.method = idx == 0 ? TB_METHOD_TTGT : TB_METHOD_FUSED;
-      learned.tile_n = idx == 1 ? 128 : (idx == 2 ? 256 : 0);
+      learned = candidate(idx);
       return run_method(Z, dtk, ddims, d, ldims, l, rdims, r, ar, ai, accumulative, lconj, rconj, &learned, s,
                         /*fallback=*/true);
     }

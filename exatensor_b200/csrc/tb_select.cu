@@ -122,7 +122,7 @@ int descriptor_of(const Matricization& Z0, int dtk, float* f) {
   return 0;
 }
 
-int selector_pick(const float* f, int* idx, bool* ambiguous, uint64_t* key) {
+int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) {
   Selector& S = sel();
   std::lock_guard<std::mutex> lk(S.mu);
   if (!S.on) return -1;
@@ -141,20 +141,30 @@ int selector_pick(const float* f, int* idx, bool* ambiguous, uint64_t* key) {
     h *= 1099511628211ull;
   }
   *key = h;
-  // timing the candidates costs a few contractions: only worth it for large ones
+  // Timing candidates costs a few contractions: only worth it for large ones.
+  // Close predictions time the three plans; a large fused prediction also
+  // times the CTA-pair form of the 256-wide tile (kCandPair), which the
+  // network does not predict: it pays off where long K panels stop fitting
+  // in L2 (C8 CCSD-like, K' = 73728: 20% faster; R8, K = 36864: 5% slower).
   constexpr float kTuneMinLog2Flops = 34.0f;  // about 1.7e10 FLOP
-  *ambiguous = S.autotune && second >= 0 && (y[second] - y[best]) < S.margin && f[3] >= kTuneMinLog2Flops;
-  if (*ambiguous) {
+  constexpr float kPairMinLog2Flops = 36.0f;  // about 6.9e10 FLOP
+  unsigned mask = 0;
+  if (S.autotune && second >= 0 && (y[second] - y[best]) < S.margin && f[3] >= kTuneMinLog2Flops)
+    mask = (1u << TB_SELECT_PLANS) - 1;
+  if (S.autotune && f[3] >= kPairMinLog2Flops && (best != 0 || mask))
+    mask |= (1u << best) | (1u << kCandPair);
+  if (mask) {
     auto it = S.cache.find(h);
     if (it != S.cache.end()) {
       *idx = it->second;
-      *ambiguous = false;
+      mask = 0;
     } else if (S.seen.insert(h).second) {
       // first time this shape is seen: take the prediction; time the
       // candidates only if the same shape comes back (one-off shapes never pay)
-      *ambiguous = false;
+      mask = 0;
     }
   }
+  *tune_mask = mask;
   return 0;
 }
 

@@ -41,6 +41,7 @@ namespace {
 // ---- driver ----------------------------------------------------------------------
 constexpr int kDefaultSlices = 6;
 constexpr int kMaxSlices = 7;  // 7 slices hold all 55 bits of the fixed-point value
+constexpr int kBf16PassKBlocks = 32;  // split-BF16: K blocks (64 values each) per accumulator pass
 
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
@@ -179,20 +180,30 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     if (S < 2 || S > kMaxSlices) { set_error("slice count %d outside 2..%d", S, kMaxSlices); return TB_ERR_INVALID_ARGS; }
     // |slice| <= 128, so one K block (128 products) adds at most 128^3.
     const int64_t cap = INT32_MAX;
+    // The products of one i + j share a pass while the sum stays exact
+    // (at most cap / 128^3 = 1023 K blocks per pass).  A group that needs
+    // several passes gets passes of equal size, so that each pass's MMAs are
+    // long enough to hide the previous pass's epilogue (1152 blocks: 576 +
+    // 576, not 1023 + 129).
+    const int64_t per_block = (int64_t)128 * 128 * 128;
+    const int64_t max_blocks = cap / per_block;
     for (int dsum = 2; dsum <= S + 1; ++dsum) {   // 1-based slice indices with i + j = dsum
+      int64_t total = 0;
+      for (int i = 1; i < dsum; ++i)
+        if (i <= S && dsum - i <= S) total += kblocks;
+      if (total == 0) continue;
+      const int64_t npass = (total + max_blocks - 1) / max_blocks;
+      const int64_t room_max = (total + npass - 1) / npass;  // <= max_blocks
       std::vector<Entry> cur;
       int64_t load = 0;
       for (int i = 1; i < dsum; ++i) {
         const int j = dsum - i;
         if (i > S || j > S) continue;
-        const int64_t per_block = (int64_t)128 * 128 * 128;
-        const int64_t max_blocks = cap / per_block;
         for (int kb = 0; kb < kblocks;) {
-          int64_t room = (cap - load) / per_block;
-          if (room < 1) { passes.push_back(cur); shifts.push_back(8 * dsum - 2); cur.clear(); load = 0; room = max_blocks; }
-          const int n = (int)std::min<int64_t>(room, kblocks - kb);
+          if (load >= room_max) { passes.push_back(cur); shifts.push_back(8 * dsum - 2); cur.clear(); load = 0; }
+          const int n = (int)std::min<int64_t>(room_max - load, kblocks - kb);
           cur.push_back({i - 1, j - 1, kb, kb + n});
-          load += per_block * n;
+          load += n;
           kb += n;
         }
       }
@@ -200,11 +211,25 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     }
     npa = npb = S;
   } else {
+    // The FP32 accumulation of the tensor cores loses accuracy about linearly
+    // with K (R4 CCSD-like, K = 36864: 1.8e-4 relative in one pass), so the K
+    // range is cut into passes of kBf16PassKBlocks blocks (longer where the
+    // entry limit requires) that the epilogue adds into D, one rounding each.
+    static const int pass_kb = [] {
+      const char* e = getenv("TB_BF16_PASS_KB");  // tuning knob
+      const int v = e ? atoi(e) : 0;
+      return v > 0 ? v : kBf16PassKBlocks;
+    }();
     const int terms = (plan && plan->bf16_terms == 4) ? 4 : 3;
-    std::vector<Entry> p3 = {{0, 0, 0, kblocks}, {0, 1, 0, kblocks}, {1, 0, 0, kblocks}};
-    if (terms == 4) p3.push_back({1, 1, 0, kblocks});
-    passes.push_back(p3);
-    shifts.push_back(0);
+    const int max_passes = kMaxProducts / terms;  // the parameter block holds kMaxProducts entries
+    const int step = std::max(pass_kb, (kblocks + max_passes - 1) / max_passes);
+    for (int kb = 0; kb < kblocks; kb += step) {
+      const int k1 = std::min(kblocks, kb + step);
+      std::vector<Entry> p3 = {{0, 0, kb, k1}, {0, 1, kb, k1}, {1, 0, kb, k1}};
+      if (terms == 4) p3.push_back({1, 1, kb, k1});
+      passes.push_back(p3);
+      shifts.push_back(0);
+    }
   }
   int nprod = 0, nplane_products = 0;
   for (auto& p : passes) {
@@ -320,6 +345,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       stats->passes = (int)passes.size();
       stats->products = nplane_products;
       stats->tile_n = BN;
+      stats->tile_m = TM;
       stats->gemm_launches = 1;
       stats->m = M; stats->n = Nr; stats->k = Kr;
     }

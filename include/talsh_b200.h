@@ -267,6 +267,7 @@ typedef struct {
   int products;      /* plane products the tensor-core GEMM ran (INT8 slice pairs or BF16
                         terms); its tensor-core work is products * flops */
   int tile_n;        /* tensor-core N tile of the executed plan */
+  int tile_m;        /* tensor-core M tile: 128 (one SM) or 256 (an SM pair, cta_group::2) */
 } tb_contract_stats_t;
 int tb_last_contract_stats(tb_contract_stats_t* stats);
 

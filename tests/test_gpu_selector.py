@@ -134,3 +134,40 @@ def test_auto_uses_the_installed_selector(xt, dev):
     finally:
         XB.selector_install(0, None, None, None)
     xt.device_check(dev.stream())
+
+
+def test_large_fused_prediction_times_the_sm_pair_tile(xt, dev):
+    """A large contraction (>= 2^36 FLOP) predicted fused is timed on its
+    second call against the 256-wide tile on SM pairs, which the network does
+    not predict.  Whichever tile is kept, the INT8 sums are exact, so D equals
+    the single-SM plan's result bit for bit."""
+    from tests.test_gpu_permute import rand_host
+    m = 3328  # 2 * m^3 = 7.4e10 FLOP
+    pattern = "D(i,j)+=L(k,i)*R(k,j)"
+    d, l, r = rand_host(O.R8, m * m, 7), rand_host(O.R8, m * m, 8), rand_host(O.R8, m * m, 9)
+    ld, rd = dev.put(l), dev.put(r)
+    dd = dev.put(d)
+    xt.tensor_contract(pattern, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(), 1.0,
+                       plan=xt.make_plan(XB.METHOD_FUSED, tile_n=256), stream=dev.stream())
+    want = dev.get(dd, np.float64, d.size)
+    nh = 8
+    n = 16 * nh + nh + nh * nh + nh + nh * 3 + 3
+    p = np.zeros(n, np.float32)
+    p[-3:] = 5.0
+    p[-1] = 1.0  # the network predicts the 256-wide tile fastest, far ahead of the rest
+    XB.selector_install(nh, p, np.zeros(16, np.float32), np.ones(16, np.float32), margin=0.25, autotune=True)
+    try:
+        tiles = []
+        for _ in range(3):  # first: prediction; second: prediction against the SM pair; third: kept choice
+            dd = dev.put(d)
+            xt.tensor_contract(pattern, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(),
+                               1.0, stream=dev.stream())
+            got = dev.get(dd, np.float64, d.size)
+            st = xt.last_contract_stats()
+            assert st.method == XB.METHOD_FUSED and st.tile_n == 256
+            tiles.append(st.tile_m)
+            assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+        assert tiles[0] == 128 and tiles[1] == tiles[2] and tiles[2] in (128, 256)
+    finally:
+        XB.selector_install(0, None, None, None)
+    xt.device_check(dev.stream())
