@@ -423,14 +423,36 @@ def block_sparse_case(X, stream, stream_obj, dtk=8, steps=1, nseg=None, hi=None,
     plan.close()
     base = D.data.data_ptr()
 
+    def reference():
+        # FP64 sums of the sampled output blocks from the operand blocks
+        # (the pattern is D(a,b,i,j) += L(a,b,c,d) * R(c,d,i,j))
+        # as matrices: L block [ab][cd] times R block [cd][ij] (dlf order), BLAS
+        def block(T, k, rows):
+            off, dims = T.blocks[k]
+            n = int(np.prod(dims))
+            x = T.data[off * es:(off + n) * es].cpu().numpy().view(dt).astype(np.float64)
+            return x.reshape((rows, n // rows), order="F")
+        out = []
+        for k in pick:
+            dd = D.blocks[k][1]
+            acc = np.zeros((dd[0] * dd[1], dd[2] * dd[3]), dtype=np.float64)
+            for dk, lk, rk in pairs:
+                if dk == k:
+                    ld, rd = L.blocks[lk][1], R.blocks[rk][1]
+                    acc += block(L, lk, ld[0] * ld[1]) @ block(R, rk, rd[0] * rd[1])
+            out.append(acc.ravel(order="F"))
+        return np.concatenate(out)
+    ref = reference()
+
     def loop():
         D.data.zero_()
         for dp, dd, lp, ld, rp, rd in tasks:
             X.tensor_contract(cfg["pattern"], dtk, dd, dp, ld, lp, rd, rp, 1.0, 0, True, None, stream)
 
+    rel_of = lambda x: float(np.linalg.norm(x.astype(np.float64) - ref) / np.linalg.norm(ref))
     if not run_loop:
         return {"pairs": len(tasks), "flops": inf.flops, "grouped_ms": round(gms, 2),
-                "grouped_tflops": round(inf.flops / (gms / 1e3) / 1e12, 3)}
+                "grouped_tflops": round(inf.flops / (gms / 1e3) / 1e12, 3), "rel_frobenius_vs_fp64": rel_of(got)}
     lms = time_steps(loop, 1, 0, 1, stream_obj)
     want = sample()
     del base
@@ -444,6 +466,8 @@ def block_sparse_case(X, stream, stream_obj, dtk=8, steps=1, nseg=None, hi=None,
                               "ms": round(lms, 2), "launch": f"{len(tasks)} tb_tensor_contract calls"},
            "grouped_over_loop": round(lms / gms, 2),
            "rel_frobenius_grouped_vs_loop": rel,
+           "rel_frobenius_vs_fp64": {"grouped": rel_of(got), "per_block_loop": rel_of(want),
+                                     "blocks_sampled": len(pick)},
            "autotune": {"tile_n": inf.tile_n, "slices": inf.slices, "tune_ms": [round(x, 2) for x in inf.tune_ms]},
            "plan_seconds": round(plan_s, 2)}
     del L, R, D, tasks
@@ -715,7 +739,7 @@ def run_profile(args):
         print(json.dumps({"profile": "selector", **(selector_case(X) or {"error": "no corpus"})}))
         return
     if args.profile == "bsc":
-        print(json.dumps({"profile": "bsc", **block_sparse_case(X, s, s_obj, 8, steps=max(1, args.steps),
+        print(json.dumps({"profile": "bsc", **block_sparse_case(X, s, s_obj, args.dtk, steps=max(1, args.steps),
                                                                 nseg=args.v or None, hi=args.o or None,
                                                                 run_loop=not (args.v or args.o))}))
         return
@@ -771,6 +795,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ccsd1_r8")
     ap.add_argument("--workloads", default=None, help="--profile configs: comma-separated workloads (default all)")
+    ap.add_argument("--dtk", type=int, choices=[4, 8], default=8, help="--profile bsc: data kind (R4 or R8)")
     ap.add_argument("--plan", default=None, help="--profile contract: explicit plan, e.g. method=2,tile_n=256,tile_m=256")
     ap.add_argument("--no-block-sparse", action="store_true", help="skip the block-sparse measurement")
     ap.add_argument("--profile", choices=["contract", "plain", "permute", "permsweep", "bsc", "selector", "e2e",

@@ -16,7 +16,9 @@
 //            in a small shared-memory ring read by the other roles
 //   warp 1   TMEM allocation and the single MMA-issuing thread
 //   warps 2-5 epilogue
-// Every wait is bounded.
+// Every wait is bounded; one that gives up records its site in the device
+// error word: 11/12 producer (item slot, stage), 13/14/15 MMA issuer (item,
+// accumulator, stage), 16/17 epilogue (item, accumulator).
 #pragma once
 #include "tb_tc_gemm.cuh"
 
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
       uint32_t it = 0;
       for (uint32_t k = 0; ok; ++k) {
         const int slot = (int)(k % kBscRing);
-        if (!(ok = mbar_wait(&bars->item_empty[slot], ((k / kBscRing) & 1) ^ 1, P.err))) break;
+        if (!(ok = mbar_wait(&bars->item_empty[slot], ((k / kBscRing) & 1) ^ 1, P.err, 11u))) break;
         const int item = (int)atomicAdd(P.queue, 1u);
         const int cur = item < P.nitems ? item : -1;
         bars->ring[slot] = cur;
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
               for (int kb = 0; kb < lo.kblocks; ++kb, ++it) {
                 const int s = (int)(it % kStagesTC);
                 const uint32_t ph = (it / kStagesTC) & 1;
-                if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err))) break;
+                if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err, 12u))) break;
                 mbar_expect_tx(&bars->full[s], 128 * 128 + BN * 128);
                 tma_load_3d(smA + (size_t)s * 128 * 128, lo.map, kb * (I8 ? 128 : 64), I.mt * 128, ch.a,
                             &bars->full[s]);
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
       uint32_t it = 0, acc_it = 0;
       for (uint32_t k = 0; ok; ++k) {
         const int slot = (int)(k % kBscRing);
-        if (!(ok = mbar_wait(&bars->item_full[slot], (k / kBscRing) & 1, P.err))) break;
+        if (!(ok = mbar_wait(&bars->item_full[slot], (k / kBscRing) & 1, P.err, 13u))) break;
         const int cur = bars->ring[slot];
         if (cur < 0) break;
         const BscItem I = P.items[cur];
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
           const BscPass ps = P.passes[p];
           const int a = acc_it & 1;
           const uint32_t aph = (acc_it >> 1) & 1;
-          if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err))) break;
+          if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err, 14u))) break;
           tc_fence_after();
           const uint32_t dcol = tmem + (uint32_t)(a * BN);
           bool first = true;
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
               for (int kb = 0; kb < kblocks; ++kb, ++it) {
                 const int s = (int)(it % kStagesTC);
                 const uint32_t ph = (it / kStagesTC) & 1;
-                if (!(ok = mbar_wait(&bars->full[s], ph, P.err))) break;
+                if (!(ok = mbar_wait(&bars->full[s], ph, P.err, 15u))) break;
                 tc_fence_after();
                 const uint32_t sa = smem_u32(smA + (size_t)s * 128 * 128);
                 const uint32_t sb = smem_u32(smB + (size_t)s * BN * 128);
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
     uint32_t acc_it = 0;
     for (uint32_t k = 0; ok; ++k) {
       const int slot = (int)(k % kBscRing);
-      if (!(ok = mbar_wait(&bars->item_full[slot], (k / kBscRing) & 1, P.err))) break;
+      if (!(ok = mbar_wait(&bars->item_full[slot], (k / kBscRing) & 1, P.err, 16u))) break;
       const int cur = bars->ring[slot];
       if (cur < 0) break;
       const BscItem I = P.items[cur];
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
       for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err))) break;
+        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err, 17u))) break;
         tc_fence_after();
         const int shift = (EPI == EPI_OZAKI_R) ? P.passes[p].shift : 0;
         epilogue_pass<BN, EPI>(V, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, I.nt,

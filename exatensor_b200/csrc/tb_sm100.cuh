@@ -28,8 +28,22 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 // Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err) {
+// Global nanosecond timer.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for phase `parity` of an mbarrier.  Bounded in time: after about
+// kWaitNanos (far longer than any pipeline wait, which lasts microseconds to
+// milliseconds) it records `code` in the device error word, if still clear,
+// and returns false, so that a barrier that never completes ends the kernel
+// with an error status that names the wait.
+constexpr uint64_t kWaitNanos = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err, unsigned code = 1u) {
   uint32_t done = 0;
+  uint64_t t0 = 0;
   for (uint32_t it = 0; it < kSpinLimit; ++it) {
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -37,8 +51,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 1023u) == 0) {
+      const uint64_t t = global_ns();
+      if (it == 0) t0 = t;
+      else if (t - t0 > kWaitNanos) break;
+    }
   }
-  if (err) atomicCAS(err, 0u, 1u);
+  if (err) atomicCAS(err, 0u, code);
   return false;
 }
 
