@@ -179,7 +179,11 @@ void drop_graph(tb_bsc_plan_s* pl) {
 // INT8: slice pairs (i, j) of equal i + j share a pass while the K blocks
 // summed into it stay within 1023 (each adds at most 128^3 = 2^21, so the
 // INT32 sum is exact); a product over many pairs is split at pair boundaries.
-// BF16: one pass with the three products over all pairs.
+// BF16: passes of at most kBscBf16PassKBlocks K blocks, each with the three
+// products, over the pairs in order (a pass may end inside a pair's K range):
+// the FP32 accumulation of the tensor cores loses accuracy with the length
+// of the sum, and the epilogue adds each pass into D with one rounding.
+constexpr int kBscBf16PassKBlocks = 32;
 void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, std::vector<BscChunk>& chunks,
                  std::vector<BscDBlk>* dbl) {
   passes.clear();
@@ -189,10 +193,23 @@ void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, s
     const int p0 = pl->dpair0[d], np = (int)kb.size();
     const int pass0 = (int)passes.size();
     if (!pl->i8) {
-      passes.push_back(BscPass{(int)chunks.size(), 3, 0, 0});
-      chunks.push_back(BscChunk{0, 0, p0, p0 + np});
-      chunks.push_back(BscChunk{0, 1, p0, p0 + np});
-      chunks.push_back(BscChunk{1, 0, p0, p0 + np});
+      int load = kBscBf16PassKBlocks;  // forces a new pass first
+      for (int q = 0; q < np; ++q) {
+        for (int k0 = 0; k0 < kb[q];) {
+          if (load >= kBscBf16PassKBlocks) {
+            passes.push_back(BscPass{(int)chunks.size(), 0, 0, 0});
+            load = 0;
+          }
+          const int n = std::min(kBscBf16PassKBlocks - load, kb[q] - k0);
+          const bool whole = k0 == 0 && n == kb[q];
+          const int terms[3][2] = {{0, 0}, {0, 1}, {1, 0}};
+          for (auto& t : terms)
+            chunks.push_back(BscChunk{t[0], t[1], p0 + q, p0 + q + 1, whole ? 0 : k0, whole ? 0 : k0 + n});
+          passes.back().nchunk += 3;
+          load += n;
+          k0 += n;
+        }
+      }
     } else {
       for (int dsum = 2; dsum <= S + 1; ++dsum) {
         int load = 1 << 30;  // forces a new pass for every diagonal
@@ -207,7 +224,7 @@ void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, s
             }
             int e = q, l = load;
             while (e < np && l + kb[e] <= 1023) l += kb[e++];
-            chunks.push_back(BscChunk{i - 1, j - 1, p0 + q, p0 + e});
+            chunks.push_back(BscChunk{i - 1, j - 1, p0 + q, p0 + e, 0, 0});
             passes.back().nchunk++;
             load = l;
             q = e;

@@ -51,7 +51,10 @@ struct BscItem { int d, mt, nt, pad_; };
 // pass's weight is 2^-shift; the operand blocks of one output block share
 // their row (column) scales, so their products add up exactly in INT32.
 struct BscPass { int chunk0, nchunk, shift, pad_; };
-struct BscChunk { int a, b, p0, p1; };
+// kb1 > 0: the chunk covers only pair p0, over its K blocks [kb0, kb1)
+// (split-BF16 passes end inside a pair's K range); else all K blocks of the
+// pairs p0 .. p1 - 1.
+struct BscChunk { int a, b, p0, p1, kb0, kb1; };
 
 constexpr int kBscRing = 4;
 
@@ -133,7 +136,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
               const BscPair pr = P.pairs[pp];
               const BscLOp lo = P.lops[pr.l];
               const CUtensorMap* rmap = P.rops[pr.r].map;
-              for (int kb = 0; kb < lo.kblocks; ++kb, ++it) {
+              const int kbeg = ch.kb1 > 0 ? ch.kb0 : 0, kend = ch.kb1 > 0 ? ch.kb1 : lo.kblocks;
+              for (int kb = kbeg; kb < kend; ++kb, ++it) {
                 const int s = (int)(it % kStagesTC);
                 const uint32_t ph = (it / kStagesTC) & 1;
                 if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err, 12u))) break;
@@ -172,7 +176,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
             const BscChunk ch = P.chunks[c];
             for (int pp = ch.p0; pp < ch.p1 && ok; ++pp) {
               const int kblocks = P.lops[P.pairs[pp].l].kblocks;
-              for (int kb = 0; kb < kblocks; ++kb, ++it) {
+              const int kbeg = ch.kb1 > 0 ? ch.kb0 : 0, kend = ch.kb1 > 0 ? ch.kb1 : kblocks;
+              for (int kb = kbeg; kb < kend; ++kb, ++it) {
                 const int s = (int)(it % kStagesTC);
                 const uint32_t ph = (it / kStagesTC) & 1;
                 if (!(ok = mbar_wait(&bars->full[s], ph, P.err, 15u))) break;
