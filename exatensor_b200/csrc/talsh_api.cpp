@@ -962,13 +962,14 @@ int contract_streamed(const tb::ParsedPattern& P, const SliceSpec& sp, int dtk, 
   const size_t bslice = (size_t)(inner_b * sp.step * es), oslice = (size_t)(inner_o * sp.step * outer_o * es);
   void* bb[kSliceRing] = {nullptr, nullptr, nullptr};
   void* ob[kSliceRing] = {nullptr, nullptr, nullptr};
-  cudaEvent_t ready[kSliceRing], freed[kSliceRing], start = nullptr, copies_done = nullptr;
-  int err = 0, nev = 0;
+  cudaEvent_t ready[kSliceRing] = {nullptr, nullptr, nullptr}, freed[kSliceRing] = {nullptr, nullptr, nullptr};
+  cudaEvent_t start = nullptr, copies_done = nullptr;
+  int err = 0;
   for (int i = 0; i < kSliceRing && !err; ++i) {
     if ((err = alloc_on(flat_gpu(g), bslice, &bb[i], s))) break;
     if ((err = alloc_on(flat_gpu(g), oslice, &ob[i], s))) break;
   }
-  for (int i = 0; i < kSliceRing && !err; ++i, ++nev)
+  for (int i = 0; i < kSliceRing && !err; ++i)
     if (cudaEventCreateWithFlags(&ready[i], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&freed[i], cudaEventDisableTiming) != cudaSuccess)
       err = TALSH_FAILURE;
@@ -1012,7 +1013,10 @@ int contract_streamed(const tb::ParsedPattern& P, const SliceSpec& sp, int dtk, 
     if (bb[i]) cudaFreeAsync(bb[i], s);
     if (ob[i]) cudaFreeAsync(ob[i], s);
   }
-  for (int i = 0; i < nev; ++i) { cudaEventDestroy(ready[i]); cudaEventDestroy(freed[i]); }
+  for (int i = 0; i < kSliceRing; ++i) {
+    if (ready[i]) cudaEventDestroy(ready[i]);
+    if (freed[i]) cudaEventDestroy(freed[i]);
+  }
   if (start) cudaEventDestroy(start);
   if (copies_done) cudaEventDestroy(copies_done);
   return err;
