@@ -110,3 +110,29 @@ def test_measured_choice_tile_bounds(emul, vmin, vmax):
         perm = list(range(1, rank + 1))
         rng.shuffle(perm)
         run(emul, rng.choice([4, 8, 16]), dims, perm, env)
+
+
+@pytest.fixture(scope="module")
+def plan_info():
+    d = tempfile.mkdtemp()
+    exe = os.path.join(d, "perm_plan_info")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", exe,
+                    os.path.join(ROOT, "tests", "emul", "perm_plan_info.cpp"),
+                    os.path.join(ROOT, "exatensor_b200", "csrc", "tb_perm_plan.cpp")], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("es,n", [(8, 76), (4, 90)])
+def test_sweep_plans_take_the_fast_paths(plan_info, es, n):
+    """The 24 rank-4 permutations of the 256 MiB sweep tensors plan onto the
+    2-D kernel's fast paths: every plan is two-dimensional with full-tile
+    offset lists (or the one-dimensional plain copy), no dimension split into
+    a few tiles leaves a partial one, and store runs are at least 256 bytes."""
+    for perm in itertools.permutations([1, 2, 3, 4]):
+        out = subprocess.run([plan_info, str(es), "4"] + [str(n)] * 4 + [str(p) for p in perm],
+                             capture_output=True, text=True, check=True).stdout.split()
+        lin2d, vec2d, rows2d, lists, LB, pes, partial_small, ntiles = map(int, out)
+        assert lin2d == 1, perm
+        assert (vec2d or rows2d) and lists in (8, 16), (perm, out)
+        assert partial_small == 0, (perm, out)
+        assert LB * pes >= 256, (perm, out)
