@@ -79,6 +79,11 @@ int tb_parse_pattern(const char* pattern, int* cptrn, int* drank, int* lrank, in
 /* out = permute(in): copy with an O2N index permutation given as the digital
  * copy pattern (1-based, cptrn[i] = destination position of input dim i).
  * conj_bits bit0 (D) xor bit1 (L) conjugates complex data.  Bit-exact.
+ * The first copy of 32 MB or more with a given shape, permutation and
+ * element size times a few plans on the stream and waits for them (one host
+ * synchronisation per shape; not while the stream is capturing; the copy is
+ * done when it returns); later calls are asynchronous.  TB_PERM_TUNE=0
+ * turns that off.
  * Replaces gpu_tensor_block_copy (TALSH/tensor_algebra_gpu_nvidia.cu:4806;
  * kernel gpu_tensor_block_copy_dlf__ :1126). */
 int tb_tensor_copy(int data_kind, int rank, const int* in_dims, const int* cptrn,
@@ -114,7 +119,10 @@ int tb_tensor_norm(int data_kind, size_t volume, const void* d, int which, doubl
 /* Tensor contraction D = beta*D + alpha * op(L) * op(R) with beta = 1 when
  * accumulative != 0, else 0.  cptrn is the digital contraction pattern
  * (lrank+rrank entries), conj_bits bit0 D, bit1 L, bit2 R.  plan may be
- * NULL.  Replaces gpu_tensor_block_contract_dlf
+ * NULL (TB_METHOD_AUTO).  With AUTO, a large contraction (>= 2^34 FLOP) whose
+ * shape comes back may, on its second call, time candidate plans with
+ * alpha = 0, beta = 1 and wait for them (one host synchronisation per
+ * shape) before running the fastest.  Replaces gpu_tensor_block_contract_dlf
  * (TALSH/tensor_algebra_gpu_nvidia.cu:5847). */
 int tb_tensor_contract(const int* cptrn, int data_kind, int drank, const int* d_dims, void* d,
                        int lrank, const int* l_dims, const void* l, int rrank,
