@@ -340,6 +340,14 @@ int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* 
     };
     if (selector_pick(f, &idx, &tune, &key) == 0) {
       if (tune) {
+        // no timing (it waits on the host) while the stream is captured into a graph
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+          cudaGetLastError();
+          tune = 0;
+        }
+      }
+      if (tune) {
         // time each candidate in the mask once with alpha = 0, beta = 1 (D unchanged)
         float best = 1e30f;
         cudaEvent_t e0, e1;

@@ -122,7 +122,8 @@ int tb_tensor_norm(int data_kind, size_t volume, const void* d, int which, doubl
  * NULL (TB_METHOD_AUTO).  With AUTO, a large contraction (>= 2^34 FLOP) whose
  * shape comes back may, on its second call, time candidate plans with
  * alpha = 0, beta = 1 and wait for them (one host synchronisation per
- * shape) before running the fastest.  Replaces gpu_tensor_block_contract_dlf
+ * shape; not while the stream is capturing) before running the fastest.
+ * Replaces gpu_tensor_block_contract_dlf
  * (TALSH/tensor_algebra_gpu_nvidia.cu:5847). */
 int tb_tensor_contract(const int* cptrn, int data_kind, int drank, const int* d_dims, void* d,
                        int lrank, const int* l_dims, const void* l, int rrank,
