@@ -3,7 +3,7 @@ FP64 (R8/C8) and split-BF16 FP32 (R4/C4) through tcgen05, against the
 double-double FP64 oracle.
 
 Tolerances (relative Frobenius error vs the oracle), stated per data kind:
-  R8/C8: 1e-12 with the default 6 slices
+  R8/C8: 1e-12 with the default 6 slices (the FP64 accuracy target)
   R4/C4: 1e-4  (3-term split-BF16; its products keep about 16 mantissa bits)
 """
 import numpy as np
