@@ -73,6 +73,9 @@ struct PermParams {
   // vbytes boundary of the output (relative to an aligned output pointer).
   int rows2d;
   int out_vec;
+  // Set by the caller, not the planner: long row copies (rows2d with rows of
+  // 4 KB or more) run in the bulk-copy kernel instead of the 2-D kernel.
+  int bulk_rows;
 };
 
 // Full-tile offset lists of the 2-D kernel.  A thread's i-th copy in a full

@@ -131,22 +131,29 @@ double real_scale_factor(double re, double im) { return cmplx8_to_real8(re, im);
 // element size therefore times the distinct plans that the planner builds for
 // a few tile-size bounds, once each after an untimed run, on the caller's
 // stream, and keeps the fastest for later calls (the default unless another
-// is more than 2% faster).  Every plan writes the same bits, so the choice
-// changes speed only; the timed runs leave the copy done.  Not while the
-// stream is being captured into a graph (the default plan runs then), and
-// TB_PERM_TUNE=0 turns it off.  Only copies are timed: their output may be
-// written several times, unlike an accumulation's.
+// is more than 2% faster).  Long row copies also try the bulk-copy kernel.
+// Every plan writes the same bits, so the choice changes speed only; the
+// timed runs leave the copy done.  Not while the stream is being captured
+// into a graph (the default plan runs then), and TB_PERM_TUNE=0 turns it
+// off.  Only copies are timed: their output may be written several times,
+// unlike an accumulation's.
 struct TileBounds { int vmin_kb, vmax_kb; };
 constexpr TileBounds kTileCandidates[] = {{0, 0}, {8, 24}, {24, 48}};
 constexpr int kNumTileCandidates = 3;
 constexpr int64_t kTuneMinBytes = (int64_t)32 << 20;
+// A further candidate for long row copies: the default plan in the bulk-copy
+// kernel (measured faster for 4-byte elements, slower for 8-byte ones).
+constexpr int kBulkRowsCand = kNumTileCandidates;
+constexpr int kNumPlanCandidates = kNumTileCandidates + 1;
+
+bool long_row_copy(const PermParams& P) { return P.rows2d && P.tma_ok && (int64_t)P.LA * P.es >= 4096; }
 
 std::mutex g_tune_mu;
 std::map<std::vector<int>, int> g_tune;  // (es, rank, dims, cptrn) -> candidate
 
 bool same_work(const PermParams& a, const PermParams& b) {
   if (a.rank != b.rank || a.V != b.V || a.LA != b.LA || a.nA != b.nA || a.LB != b.LB || a.nB != b.nB ||
-      a.lap != b.lap || a.ntiles != b.ntiles)
+      a.lap != b.lap || a.ntiles != b.ntiles || a.bulk_rows != b.bulk_rows)
     return false;
   for (int i = 0; i < a.rank; ++i)
     if (a.tile[i] != b.tile[i]) return false;
@@ -171,16 +178,20 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
   if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) { cudaGetLastError(); cap = cudaStreamCaptureStatusActive; }
   const bool tune = pick < 0 && tune_on && vol * (int64_t)sizeof(E) >= kTuneMinBytes && cap == cudaStreamCaptureStatusNone;
   if (!tune) {
-    const TileBounds b = kTileCandidates[pick < 0 ? 0 : pick];
+    const int c = pick < 0 ? 0 : pick;
+    const TileBounds b = kTileCandidates[c == kBulkRowsCand ? 0 : c];
     PermParams P;
     int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb);
-    if (e == 0) return launch_perm<E, Store>(P, in, st, s);
+    if (e == 0) {
+      if (c == kBulkRowsCand && long_row_copy(P)) P.bulk_rows = 1;
+      return launch_perm<E, Store>(P, in, st, s);
+    }
     if (e != TB_ERR_NOT_IMPLEMENTED) return e;
     return run_scatter<E, Store>(rank, dims, cptrn, in, st, s);
   }
-  static PermParams plans[kNumTileCandidates];  // large; built under the lock below
+  static PermParams plans[kNumPlanCandidates];  // large; built under the lock below
   std::lock_guard<std::mutex> g(g_tune_mu);
-  int n = 0, idx[kNumTileCandidates];
+  int n = 0, idx[kNumPlanCandidates];
   for (int c = 0; c < kNumTileCandidates; ++c) {
     int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &plans[n], kTileCandidates[c].vmin_kb,
                                 kTileCandidates[c].vmax_kb);
@@ -192,6 +203,11 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
     bool dup = false;
     for (int k = 0; k < n; ++k) dup = dup || same_work(plans[k], plans[n]);
     if (!dup) idx[n++] = c;
+  }
+  if (long_row_copy(plans[0])) {  // plans[0] is the default plan (c == 0 always builds first)
+    plans[n] = plans[0];
+    plans[n].bulk_rows = 1;
+    idx[n++] = kBulkRowsCand;
   }
   if (n == 1) { g_tune[key] = 0; return launch_perm<E, Store>(plans[0], in, st, s); }
   cudaEvent_t e0, e1;

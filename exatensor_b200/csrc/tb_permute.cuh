@@ -561,7 +561,8 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
   // long rows move as bulk copies, except row copies (rows2d), whose 2-D
   // kernel stores whole vectors (TB_PERM_LONGROWS=bulk: those too)
   static const bool longrows_bulk = [] { const char* e = getenv("TB_PERM_LONGROWS"); return e && !strcmp(e, "bulk"); }();
-  const bool bulk = eligible && (mode == 1 || (mode == 0 && (int64_t)P.LA * P.es >= 4096 && (!P.rows2d || longrows_bulk)));
+  const bool bulk = eligible && (mode == 1 || (mode == 0 && (int64_t)P.LA * P.es >= 4096 &&
+                                               (!P.rows2d || longrows_bulk || P.bulk_rows)));
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(perm_pipe_kernel<Elem, Store, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);

@@ -116,7 +116,8 @@ def test_two_dimensional_paths_permute_add(xt, dev, dtk):
 
 @pytest.mark.parametrize("dtk,dims,perm", [(O.R8, [64, 64, 48, 32], (2, 3, 1, 4)),
                                            (O.R4, [96, 80, 60, 40], (3, 4, 1, 2)),
-                                           (O.C4, [64, 64, 48, 32], (4, 3, 2, 1))])
+                                           (O.C4, [64, 64, 48, 32], (4, 3, 2, 1)),
+                                           (O.R4, [96, 96, 40, 30], (1, 2, 4, 3))])  # long rows: bulk kernel tried
 def test_measured_plan_choice_bit_exact(xt, dev, dtk, dims, perm):
     """Copies of 32 MB and more time a few plans on their first call and keep
     the fastest: the first (timing) call and the later (cached) ones all give
