@@ -150,6 +150,12 @@ bool long_row_copy(const PermParams& P) { return P.rows2d && P.tma_ok && (int64_
 
 std::mutex g_tune_mu;
 std::map<std::vector<int>, int> g_tune;  // (es, rank, dims, cptrn) -> candidate
+constexpr size_t kMaxTuned = 4096;       // past this many shapes the choices are forgotten (bounded memory)
+
+void remember_choice(const std::vector<int>& key, int c) {
+  if (g_tune.size() >= kMaxTuned) g_tune.clear();
+  g_tune[key] = c;
+}
 
 bool same_work(const PermParams& a, const PermParams& b) {
   if (a.rank != b.rank || a.V != b.V || a.LA != b.LA || a.nA != b.nA || a.LB != b.LB || a.nB != b.nB ||
@@ -196,7 +202,7 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
     int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &plans[n], kTileCandidates[c].vmin_kb,
                                 kTileCandidates[c].vmax_kb);
     if (e == TB_ERR_NOT_IMPLEMENTED && c == 0) {
-      g_tune[key] = 0;
+      remember_choice(key, 0);
       return run_scatter<E, Store>(rank, dims, cptrn, in, st, s);
     }
     if (e) { if (c == 0) return e; continue; }
@@ -209,7 +215,7 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
     plans[n].bulk_rows = 1;
     idx[n++] = kBulkRowsCand;
   }
-  if (n == 1) { g_tune[key] = 0; return launch_perm<E, Store>(plans[0], in, st, s); }
+  if (n == 1) { remember_choice(key, 0); return launch_perm<E, Store>(plans[0], in, st, s); }
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) { set_error("cudaEventCreate failed"); return TB_ERR_CUDA; }
   if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); set_error("cudaEventCreate failed"); return TB_ERR_CUDA; }
@@ -233,7 +239,7 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
   cudaEventDestroy(e1);
   if (err) return err;
   if (best != 0 && best_ms > 0.98f * ms0) best = 0;
-  g_tune[key] = idx[best];
+  remember_choice(key, idx[best]);
   return 0;
 }
 

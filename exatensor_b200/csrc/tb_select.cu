@@ -122,6 +122,10 @@ int descriptor_of(const Matricization& Z0, int dtk, float* f) {
   return 0;
 }
 
+// Shapes remembered by the measured fallback (seen once, or decided); past
+// this many the sets are cleared, so memory stays bounded in long runs.
+constexpr size_t kMaxRemembered = (size_t)1 << 16;
+
 int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) {
   Selector& S = sel();
   std::lock_guard<std::mutex> lk(S.mu);
@@ -158,10 +162,13 @@ int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) 
     if (it != S.cache.end()) {
       *idx = it->second;
       mask = 0;
-    } else if (S.seen.insert(h).second) {
-      // first time this shape is seen: take the prediction; time the
-      // candidates only if the same shape comes back (one-off shapes never pay)
-      mask = 0;
+    } else {
+      if (S.seen.size() >= kMaxRemembered) S.seen.clear();
+      if (S.seen.insert(h).second) {
+        // first time this shape is seen: take the prediction; time the
+        // candidates only if the same shape comes back (one-off shapes never pay)
+        mask = 0;
+      }
     }
   }
   *tune_mask = mask;
@@ -171,6 +178,7 @@ int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) 
 void selector_remember(uint64_t key, int idx) {
   Selector& S = sel();
   std::lock_guard<std::mutex> lk(S.mu);
+  if (S.cache.size() >= kMaxRemembered) S.cache.clear();  // bounded memory: decisions are re-measured
   S.cache[key] = idx;
 }
 
