@@ -136,3 +136,21 @@ def test_sweep_plans_take_the_fast_paths(plan_info, es, n):
         assert (vec2d or rows2d) and lists in (8, 16), (perm, out)
         assert partial_small == 0, (perm, out)
         assert LB * pes >= 256, (perm, out)
+
+
+def test_offset_lists_decline_offsets_beyond_32_bits(plan_info):
+    """The 2-D kernel's full-tile lists hold 32-bit offsets from a tile's
+    origin.  For tensors whose tiles span more than 2^31 elements of output
+    the planner must leave them off (the general code, with 64-bit offsets,
+    runs); where the offsets fit, the lists stay on.  Planning only: no
+    tensor of this size is allocated."""
+    huge = [(8, [64, 1048576, 40], [3, 2, 1]), (8, [64, 67108864], [2, 1]),
+            (4, [90, 90, 300000], [1, 3, 2]), (8, [76, 40000000, 76], [3, 2, 1])]
+    for es, dims, perm in huge:
+        out = subprocess.run([plan_info, str(es), str(len(dims))] + [str(x) for x in dims] + [str(p) for p in perm],
+                             capture_output=True, text=True, check=True).stdout.split()
+        lin2d, vec2d, rows2d, lists = map(int, out[:4])
+        assert lin2d == 1 and (vec2d or rows2d) and lists == 0, (dims, perm, out)
+    out = subprocess.run([plan_info, "8", "3", "76", "76", "1000000", "2", "1", "3"], capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert int(out[3]) == 8, out
