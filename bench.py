@@ -6,14 +6,20 @@ Headline workload: the CCSD-like R8 contraction
 (M = N_ab = 36864, N = 2304, K = 36864; 6.262e12 FLOP by TAL-SH's 2*M*N*K
 accounting), inputs seeded U[-1,1) with V scaled by 1/192, D = 0.  A "step" is
 one contraction by the chosen method (the library's plan selector).  The same
-line reports the plain FP64 TTGT form, the error against a double-double
-FP64 oracle on sampled elements, the permutation sweep (all 24 rank-4
-permutations of 256 MiB R8 and R4 tensors, bit-exact) in GB/s, the
+line reports the plain FP64 TTGT form (chosen_over_plain), the error of the
+chosen D against the plain D over the whole tensor and against a
+double-double FP64 oracle on 4096 sampled elements, the other five CCSD-like
+configurations (R8/C8/R4, both patterns), the single-block 40^4
+configuration, the permutation and add sweeps (256 MiB R8/R4 tensors of rank
+2-6, uniform and skewed extents, every case checked bit for bit) in GB/s, the
+block-sparse grouped launch, the learned plan selector, the tensor-core peaks
+measured by the library's own probes (the roofline denominators), the
 end-to-end rate through talshTensorContract with host-resident tensors, and
 the reference's OpenMP+BLAS CPU path timed on this host.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-       (N > 1: launched by torchrun, one process per GPU, replicas)
+       (N > 1: launched by torchrun, one process per GPU, replicas; the line
+       then holds the headline contraction only)
 """
 from __future__ import annotations
 
@@ -214,20 +220,19 @@ def time_back_to_back(fn, steps, stream_obj):
     return e0.elapsed_time(e1)
 
 
-def sample_error(X, case, method, nsamp=48):
-    """Relative Frobenius and max-abs error of sampled D elements against the
-    double-double oracle (each a K-length dot product of the operands'
-    elements gathered on the device), after one non-accumulating contraction.
-    Any contraction pattern without conjugation; real or complex data."""
+def sample_error(X, case, nsamp, seed=5, chunk=256):
+    """Sampled check of the D now held by `case` (a non-accumulating
+    contraction of the case's operands): `nsamp` seeded D elements, each
+    against a K-long dot product with double-double accumulation (the FP64
+    error oracle, oracle.dd_dot_batch).  The operand elements of each sampled
+    dot product are gathered on the device.  R8 and C8 data."""
     import numpy as np
     import torch
 
     import oracle as O
-    case.run(method, accumulative=False)
     torch.cuda.synchronize()
-    dt = O.NP_DTYPE[case.wl["dtk"]]
-    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32,
-           np.dtype(np.complex128): torch.complex128, np.dtype(np.complex64): torch.complex64}[np.dtype(dt)]
+    cplx = case.wl["dtk"] in (14, 18)
+    tdt = torch.complex128 if cplx else torch.float64
 
     def strides(d):
         st = [1]
@@ -242,93 +247,301 @@ def sample_error(X, case, method, nsamp=48):
                            indexing="ij")
     loff = sum(g.reshape(-1) * Ls[i] for g, (i, _) in zip(grids, pairs))
     roff = sum(g.reshape(-1) * Rs[j] for g, (_, j) in zip(grids, pairs))
-    K = int(loff.numel())
     Lv, Rv, Dv = case.L.view(tdt), case.R.view(tdt), case.D.view(tdt)
-    rng = np.random.default_rng(5)
-    num = den = mx = 0.0
-    for _ in range(nsamp):
-        dix = [int(rng.integers(x)) for x in case.dd]
-        lb = sum(dix[cptrn[i] - 1] * Ls[i] for i in range(lr) if cptrn[i] > 0)
-        rb = sum(dix[cptrn[lr + j] - 1] * Rs[j] for j in range(rr) if cptrn[lr + j] > 0)
-        lv = np.ascontiguousarray(Lv[lb + loff].cpu().numpy())
-        rv = np.ascontiguousarray(Rv[rb + roff].cpu().numpy())
-        ref = np.zeros(1, dtype=dt)
-        O.contract([-1, -1], ref, [], lv, [K], rv, [K], 1.0, 0, True, mode=1)
-        got = complex(Dv[sum(x * st for x, st in zip(dix, Ds))].item())
-        e = abs(got - complex(ref[0]))
-        num += e * e
-        den += abs(complex(ref[0])) ** 2
-        mx = max(mx, e)
-    return {"rel_frobenius": (num / den) ** 0.5, "max_abs": mx, "samples": nsamp}
+    rng = np.random.default_rng(seed)
+    dix = np.stack([rng.integers(0, x, nsamp) for x in case.dd], axis=1)
+    zero = np.zeros(nsamp, dtype=np.int64)
+    lb = zero + sum(dix[:, cptrn[i] - 1] * Ls[i] for i in range(lr) if cptrn[i] > 0)
+    rb = zero + sum(dix[:, cptrn[lr + j] - 1] * Rs[j] for j in range(rr) if cptrn[lr + j] > 0)
+    doff = torch.from_numpy((dix * np.array(Ds, dtype=np.int64)).sum(axis=1)).cuda()
+    got = Dv[doff].cpu().numpy()
+    ref = np.empty(nsamp, dtype=np.complex128 if cplx else np.float64)
+    lb_t, rb_t = torch.from_numpy(lb).cuda(), torch.from_numpy(rb).cuda()
+    for c0 in range(0, nsamp, chunk):
+        c1 = min(nsamp, c0 + chunk)
+        lv = Lv[lb_t[c0:c1, None] + loff[None, :]].cpu().numpy()
+        rv = Rv[rb_t[c0:c1, None] + roff[None, :]].cpu().numpy()
+        ref[c0:c1] = O.dd_dot_batch(lv, rv)
+    e = np.abs(got - ref)
+    return {"rel_frobenius": float(np.sqrt((e ** 2).sum() / (np.abs(ref) ** 2).sum())), "max_abs": float(e.max()),
+            "samples": nsamp}
 
 
-def configs_case(X, s, s_obj, names, steps, warmup):
-    """Chosen (plan selector) and plain TTGT forms of each CCSD-like workload:
-    device-timed TFLOP/s and sampled errors against the double-double oracle."""
+def full_rel(a, b, fp32=False):
+    """Relative Frobenius difference of two device tensors holding the same
+    data kind (real and imaginary parts alike; sums in FP64)."""
     import torch
-    out = []
-    for name in names:
-        wl = WORKLOADS[name]
-        case = ContractionCase(X, wl, s)
-        ms = time_steps(lambda: case.run(X.METHOD_AUTO), steps, warmup, 1, s_obj) / steps
-        st = X.last_contract_stats()
-        pms = time_steps(lambda: case.run(X.METHOD_TTGT), steps, 1, 1, s_obj) / steps
-        e_c = sample_error(X, case, X.METHOD_AUTO, 24)
-        e_p = sample_error(X, case, X.METHOD_TTGT, 24)
-        rec = {"workload": name, "pattern": wl["pattern"], "data_kind": wl["dtk"], "flop": case.flops,
-               "chosen": {"method": {1: "ttgt", 2: "tensor cores"}.get(st.method, st.method), "slices": st.slices,
-                          "products": st.products, "tile_n": st.tile_n, "tile_m": st.tile_m, "ms": round(ms, 3),
-                          "TFLOP/s": round(case.flops / (ms / 1e3) / 1e12, 2), "rel_frobenius": e_c["rel_frobenius"]},
-               "plain": {"ms": round(pms, 3), "TFLOP/s": round(case.flops / (pms / 1e3) / 1e12, 2),
-                         "rel_frobenius": e_p["rel_frobenius"]},
-               "chosen_over_plain": round(pms / ms, 3)}
-        out.append(rec)
-        print(json.dumps(rec), flush=True)
-        del case
-        torch.cuda.synchronize()
-        torch.cuda.empty_cache()
+    dt = torch.float32 if fp32 else torch.float64
+    x, y = a.view(dt).double(), b.view(dt).double()
+    return float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+
+
+def sig(x, n=4):
+    """x rounded to n significant digits (keeps the bench line short)."""
+    if x is None or x == 0 or x != x or x in (float("inf"), float("-inf")):
+        return x
+    from math import floor, log10
+    return round(x, -int(floor(log10(abs(x)))) + (n - 1))
+
+
+def ccsd_case(X, s, s_obj, name, steps, warmup, nsamp, psteps=None, world=1, on_timed=None, after_timed=None):
+    """Chosen (METHOD_AUTO: the plan selector) against plain TTGT for one
+    CCSD-like workload: device-timed TFLOP/s of both, the chosen D compared with
+    the plain D over the WHOLE output tensor, and (R8/C8) both against the
+    double-double oracle on `nsamp` sampled elements.  Returns the compact
+    record, the device case and (chosen ms, plain ms, stats, timed-GEMM ms and
+    count of the chosen steps, of the plain steps)."""
+    import torch
+    wl = WORKLOADS[name]
+    case = ContractionCase(X, wl, s)
+    case.run(X.METHOD_AUTO)  # first call of a shape: the selector may time close candidates
+    torch.cuda.synchronize()
+    X.timing_enable(True)  # CUDA events around the GEMM launches, read after each timed region
+
+    def hook():
+        X.timing_read()
+        if on_timed:
+            on_timed()
+    ms = time_steps(lambda: case.run(X.METHOD_AUTO), steps, warmup, world, s_obj, on_timed=hook) / steps
+    if after_timed:
+        after_timed()
+    gemm = X.timing_read()
+    st = X.last_contract_stats()
+    psteps = psteps or max(1, steps // 2)
+    pms = time_steps(lambda: case.run(X.METHOD_TTGT), psteps, 1, world, s_obj,
+                     on_timed=lambda: X.timing_read()) / psteps
+    pgemm = X.timing_read()
+    X.timing_enable(False)
+    # whole-tensor comparison: plain D, then chosen D (both non-accumulating)
+    case.run(X.METHOD_TTGT, accumulative=False)
+    torch.cuda.synchronize()
+    dplain = case.D.clone()
+    err_p = sample_error(X, case, nsamp) if nsamp and wl["dtk"] in (8, 18) else None
+    case.run(X.METHOD_AUTO, accumulative=False)
+    torch.cuda.synchronize()
+    err_c = sample_error(X, case, nsamp) if nsamp and wl["dtk"] in (8, 18) else None
+    rel = full_rel(case.D, dplain, fp32=wl["dtk"] in (4, 14))
+    case.dchosen = case.D.clone()
+    del dplain
+    rec = {"chosen": {"method": {1: "ttgt", 2: "fused"}.get(st.method, st.method), "slices": st.slices,
+                      "tile_n": st.tile_n, "tile_m": st.tile_m, "ms": sig(ms), "TFLOP/s": sig(case.flops / ms / 1e9)},
+           "plain": {"ms": sig(pms), "TFLOP/s": sig(case.flops / pms / 1e9)},
+           "chosen_over_plain": sig(pms / ms, 3),
+           "rel_frob_chosen_vs_plain_whole_D": sig(rel, 3)}
+    if err_c:
+        rec["dd_samples"] = {"n": nsamp, "chosen_rel_frob": sig(err_c["rel_frobenius"], 3),
+                             "plain_rel_frob": sig(err_p["rel_frobenius"], 3),
+                             "chosen_max_abs": sig(err_c["max_abs"], 3)}
+    return rec, case, (ms, pms, st, gemm, pgemm)
+
+
+def c1_case(X, s, s_obj):
+    """The single-block 40^4 R8 configuration: D(a,b,c,d) += 0.5 *
+    L(c,k,a,l) * R(l,d,k,b), L and R from one seeded stream (seed 0, L first),
+    D = 0; chosen and plain rates, the error of both against the double-double
+    oracle over the whole tensor, and the (3,1,4,2) permutation of L."""
+    import numpy as np
+    import torch
+
+    import oracle as O
+    pat, n = "D(a,b,c,d)+=L(c,k,a,l)*R(l,d,k,b)", 40
+    dims, nvol = [n] * 4, n ** 4
+    u = O.splitmix64_uniform(2 * nvol, 0)
+    L, R = u[:nvol].copy(), u[nvol:].copy()
+    ref = np.zeros(nvol)
+    cptrn, *_ = O.parse_pattern(pat)
+    O.contract(cptrn, ref, dims, L, dims, R, dims, 0.5, mode=1)
+    dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    dD = torch.zeros(nvol, dtype=torch.float64, device="cuda")
+    out = {"workload": f"{pat} 40^4 R8 alpha 0.5, seed 0, D=0"}
+    flops = 2.0 * 1600 ** 3
+    for key, method in (("chosen", X.METHOD_AUTO), ("plain", X.METHOD_TTGT)):
+        def run(acc=True, method=method):
+            X.tensor_contract(pat, 8, dims, dD.data_ptr(), dims, dL.data_ptr(), dims, dR.data_ptr(), 0.5, 0, acc,
+                              X.make_plan(method), s)
+        run()
+        ms = time_back_to_back(run, 20, s_obj) / 20
+        dD.zero_()
+        run()
+        err = O.rel_frobenius(dD.cpu().numpy(), ref)
+        out[key] = {"method": {1: "ttgt", 2: "fused"}.get(X.last_contract_stats().method), "ms": sig(ms),
+                    "TFLOP/s": sig(flops / ms / 1e9), "rel_frob_vs_dd": sig(err, 3)}
+    dP = torch.empty_like(dL)
+    cp = lambda: X.tensor_copy(8, dims, (3, 1, 4, 2), dL.data_ptr(), dP.data_ptr(), 0, s)
+    cp()
+    pms = time_back_to_back(cp, 20, s_obj) / 20
+    exact = bool(np.array_equal(dP.cpu().numpy(), O.permute(L, dims, [3, 1, 4, 2])))
+    out["permute_3142"] = {"GB/s": sig(2.0 * nvol * 8 / pms / 1e6), "bit_exact_vs_oracle": exact}
     return out
 
 
-def permute_sweep(X, stream, stream_obj, hbm_gbs):
-    """All 24 rank-4 permutations of 256 MiB-class R8 (76^4) and R4 (90^4)."""
+# ----------------------------------------------------------------------- permutations
+SWEEP_DIMS = {8: {2: [5793] * 2, 3: [322] * 3, 4: [76] * 4, 5: [32] * 5, 6: [18] * 6},
+              4: {2: [8192] * 2, 3: [406] * 3, 4: [90] * 4, 5: [37] * 5, 6: [20] * 6}}
+# skewed shapes: (rank, small extent, its position); the other extents are
+# balanced to the governing 256 MiB volume
+SKEWED = [(3, 3, 0), (3, 2, 2), (4, 5, 0), (4, 7, 3), (6, 2, 0), (6, 4, 5)]
+
+
+def skewed_dims(dtk, rank, small, pos):
+    target = 2 ** 25 if dtk == 8 else 2 ** 26
+    rest = int(round((target / small) ** (1.0 / (rank - 1))))
+    dims = [rest] * rank
+    dims[pos] = small
+    return dims
+
+
+def sweep_cases():
+    """The permutation sweep: 256 MiB-class R8 and R4 tensors of rank 2-6
+    (extents in SWEEP_DIMS: all permutations at ranks 2-4, 24 seeded random
+    ones at rank 5, 40 at rank 6) and skewed shapes (one extent of 2-7, six
+    seeded permutations each, the reversal first).  Returns dicts with dtk,
+    dims, perm and the class name ("r8_4", "r4_6", "r8_4s", ...)."""
     import itertools
+    import random
+    rng = random.Random(20240601)
 
-    import torch
-    out = {}
-    total_bytes = total_ms = 0.0
-    rates = []
-    for dtk, n in ((8, 76), (4, 90)):
-        es = X.ELEM_BYTES[dtk]
-        v = n ** 4
-        a = torch.empty(v * es, dtype=torch.uint8, device="cuda")
-        b = torch.empty_like(a)
-        X.fill_uniform(dtk, v, a.data_ptr(), 3, stream=stream)
-        dims = [n] * 4
-        for perm in itertools.permutations([1, 2, 3, 4]):
-            # the first call of a shape also picks its plan by timing (untimed here)
-            X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream)
-            ms = time_back_to_back(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream),
-                                   10, stream_obj) / 10
-            gb = 2.0 * v * es / 1e9
-            rates.append(gb / (ms / 1e3))
-            total_bytes += gb
-            total_ms += ms
-        # plain scatter form for reference (two permutations)
-        sc = []
-        for perm in ((4, 3, 2, 1), (2, 4, 1, 3)):
-            ms = time_steps(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream, True), 3,
-                            1, 1, stream_obj) / 3
-            sc.append(2.0 * v * es / 1e9 / (ms / 1e3))
-        out[f"scatter_gbs_{'r8' if dtk == 8 else 'r4'}"] = round(statistics.mean(sc), 1)
-        del a, b
-    agg = total_bytes / (total_ms / 1e3)
-    out.update({"value": round(agg, 1), "unit": "GB/s", "min": round(min(rates), 1), "max": round(max(rates), 1),
-                "frac_of_measured_hbm": round(agg / hbm_gbs, 3), "frac_of_8000": round(agg / 8000.0, 3),
-                "cases": "24 rank-4 perms x {R8 76^4 (254.5 MiB), R4 90^4 (250.3 MiB)}, bit-exact",
-                "timing": "10 back-to-back calls per permutation, one queued before the start event; "
-                          "plans picked by the library's measured choice on the first call"})
+    def random_perms(rank, n, first=()):
+        perms = list(first)
+        while len(perms) < n:
+            p = list(range(1, rank + 1))
+            rng.shuffle(p)
+            if tuple(p) not in perms:
+                perms.append(tuple(p))
+        return perms
+    out = []
+    for dtk in (8, 4):
+        tag = "r8" if dtk == 8 else "r4"
+        for rank, dims in SWEEP_DIMS[dtk].items():
+            perms = (list(itertools.permutations(range(1, rank + 1))) if rank <= 4
+                     else random_perms(rank, 24 if rank == 5 else 40))
+            out += [dict(dtk=dtk, dims=list(dims), perm=tuple(p), cls=f"{tag}_{rank}") for p in perms]
+        for rank, small, pos in SKEWED:
+            dims = skewed_dims(dtk, rank, small, pos)
+            out += [dict(dtk=dtk, dims=dims, perm=p, cls=f"{tag}_{rank}s")
+                    for p in random_perms(rank, 6, [tuple(range(rank, 0, -1))])]
     return out
+
+
+def add_cases():
+    """The add sweep (D += 0.37 * permute(L)): all 24 rank-4 permutations and
+    the first 10 rank-6 ones, R8 and R4, at the sweep's 256 MiB sizes."""
+    cases = sweep_cases()
+    out = [c for c in cases if c["cls"] in ("r8_4", "r4_4")]
+    for tag in ("r8_6", "r4_6"):
+        out += [c for c in cases if c["cls"] == tag][:10]
+    return out
+
+
+def torch_order(perm):
+    """torch.permute order that applies the O2N permutation `perm` (input
+    dimension i goes to output position perm[i]) to a dlf tensor viewed as a
+    C-order torch tensor of reversed extents."""
+    r = len(perm)
+    q = [0] * r
+    for i, p in enumerate(perm):
+        q[p - 1] = i
+    return [r - 1 - q[r - 1 - a] for a in range(r)]
+
+
+def torch_permuted(t, dims, perm, word):
+    """permute(t) computed by torch, as an independent check of the bits: t
+    holds a dlf tensor of extents dims, viewed as words of dtype `word`."""
+    x = t.view(word)
+    if len(dims) > 1:
+        x = x.view(*reversed(dims)).permute(*torch_order(perm)).contiguous()
+    return x.view(-1)
+
+
+def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True):
+    """Every sweep case: 10 back-to-back timed copies after the first call (where
+    the library's measured plan choice runs), and a bit-for-bit comparison of
+    the result with torch's permute of the same device data.  Per class the
+    aggregate (bytes over time) and the slowest case, in GB/s; then the add
+    sweep."""
+    import torch
+    cases = sweep_cases()
+    stats, rates, mism = {}, [], 0
+    tot_b = tot_s = 0.0
+    cur, a, b = None, None, None
+    for c in cases:
+        dtk, dims, perm = c["dtk"], c["dims"], c["perm"]
+        es = X.ELEM_BYTES[dtk]
+        nvol = vol(dims)
+        if cur != (dtk, tuple(dims)):
+            a = b = None
+            torch.cuda.empty_cache()
+            a = torch.empty(nvol * es, dtype=torch.uint8, device="cuda")
+            b = torch.empty_like(a)
+            X.fill_uniform(dtk, nvol, a.data_ptr(), 3, stream=stream)
+            cur = (dtk, tuple(dims))
+        fn = lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, stream)
+        fn()
+        ms = time_back_to_back(fn, 10, stream_obj) / 10
+        word = torch.int64 if es == 8 else torch.int32
+        if not torch.equal(b.view(word), torch_permuted(a, dims, perm, word)):
+            mism += 1
+        gb = 2.0 * nvol * es / 1e9
+        rates.append(gb / (ms / 1e3))
+        tot_b += gb
+        tot_s += ms / 1e3
+        st = stats.setdefault(c["cls"], [0.0, 0.0, 1e30])
+        st[0] += gb
+        st[1] += ms / 1e3
+        st[2] = min(st[2], gb / (ms / 1e3))
+    a = b = None
+    agg = tot_b / tot_s
+    r4 = [(2.0 * vol(c["dims"]) * X.ELEM_BYTES[c["dtk"]] / 1e9, r) for c, r in zip(cases, rates)
+          if c["cls"] in ("r8_4", "r4_4")]
+    out = {"GB/s": round(agg, 1), "min_GB/s": round(min(rates), 1), "frac_measured_hbm": sig(agg / hbm_gbs, 3),
+           "frac_8000": sig(agg / 8000.0, 3), "min_frac_measured_hbm": sig(min(rates) / hbm_gbs, 3),
+           "cases": len(cases), "bit_exact": len(cases) - mism,
+           "rank4_48": {"GB/s": round(sum(g for g, _ in r4) / sum(g / r for g, r in r4), 1),
+                        "min": round(min(r for _, r in r4), 1)},
+           "by_class_agg_min": {k: [round(v[0] / v[1]), round(v[2])] for k, v in stats.items()}}
+    if with_add:
+        out["add"] = add_sweep(X, stream, stream_obj, hbm_gbs)
+    out["timing"] = "10 back-to-back calls per case after the first; bits checked against torch.permute"
+    return out
+
+
+def add_sweep(X, stream, stream_obj, hbm_gbs, scale=0.37):
+    """D += scale * permute(L) over add_cases(): 3 * vol * elem bytes per call;
+    one call per case from a fresh D compared bit for bit with torch's
+    d + permute(l) * scale (two roundings), then 10 back-to-back timed calls."""
+    import torch
+    cases = add_cases()
+    cur, tot_b, tot_s, rates, mism = None, 0.0, 0.0, [], 0
+    l = d0 = d = None
+    for c in cases:
+        dtk, dims, perm = c["dtk"], c["dims"], c["perm"]
+        es = X.ELEM_BYTES[dtk]
+        nvol = vol(dims)
+        if cur != (dtk, tuple(dims)):
+            l = d0 = d = None
+            torch.cuda.empty_cache()
+            l = torch.empty(nvol * es, dtype=torch.uint8, device="cuda")
+            d0 = torch.empty_like(l)
+            d = torch.empty_like(l)
+            X.fill_uniform(dtk, nvol, l.data_ptr(), 4, stream=stream)
+            X.fill_uniform(dtk, nvol, d0.data_ptr(), 5, stream=stream)
+            cur = (dtk, tuple(dims))
+        fdt = torch.float64 if es == 8 else torch.float32
+        d.copy_(d0)
+        X.tensor_add(dtk, dims, perm, d.data_ptr(), l.data_ptr(), scale, 0, stream)
+        ref = d0.view(fdt) + torch_permuted(l, dims, perm, fdt) * scale
+        if not torch.equal(d.view(torch.uint8), ref.view(torch.uint8)):
+            mism += 1
+        fn = lambda: X.tensor_add(dtk, dims, perm, d.data_ptr(), l.data_ptr(), scale, 0, stream)
+        ms = time_back_to_back(fn, 10, stream_obj) / 10
+        gb = 3.0 * nvol * es / 1e9
+        rates.append(gb / (ms / 1e3))
+        tot_b += gb
+        tot_s += ms / 1e3
+    l = d0 = d = None
+    agg = tot_b / tot_s
+    return {"GB/s": round(agg, 1), "min_GB/s": round(min(rates), 1), "frac_measured_hbm": sig(agg / hbm_gbs, 3),
+            "cases": len(cases), "bit_exact": len(cases) - mism}
 
 
 def permute_sweep_repeated(X, stream, stream_obj, reps=3):
@@ -531,16 +744,27 @@ def selector_case(X):
             "selection_us_host": round(host_us, 2), "selection_us_gpu_batched": round(gpu_us, 4)}
 
 
-def e2e_talsh(X, wl, steps):
-    """Same contraction through talshTensorContract with Host-resident tensors:
-    each step copies V, T, D to the GPU and D back (copy control TTT)."""
+def e2e_talsh(X, wl, steps, case=None):
+    """The same contraction through talshTensorContract (the reference-facing
+    API) with Host-resident tensors: every call copies V, T and D to the GPU
+    and D back (copy control TTT).  The host tensors hold the device case's
+    seeded data; after the calls D / (number of calls) is compared with the
+    device result of the chosen method over the whole tensor."""
+    import numpy as np
+    import torch
+
     import exatensor_b200.talsh as T
     T.init((int(os.environ.get("LOCAL_RANK", "0")),))
     dd, ld, rd = shapes(wl["pattern"], wl["v"], wl["o"])
     es = X.ELEM_BYTES[wl["dtk"]]
     D = T.Tensor(dd, wl["dtk"], 0.0)
-    L = T.Tensor(ld, wl["dtk"], 1.0 / (3 * wl["v"]))
-    R = T.Tensor(rd, wl["dtk"], 0.5)
+    L = T.Tensor(ld, wl["dtk"], 0.0)
+    R = T.Tensor(rd, wl["dtk"], 0.0)
+    seeded = case is not None
+    if seeded:
+        for t, src in ((L, case.L), (R, case.R)):
+            torch.from_numpy(t.host_array().view(np.uint8)).copy_(src)
+        torch.cuda.synchronize()
     run = lambda: T.check(T.contract(wl["pattern"], D, L, R, 1.0, 0, T.DEV_NVIDIA_GPU, T.COPY_TTT, True),
                           "talshTensorContract")
     for _ in range(2):  # the second call of a shape may time close plan candidates once
@@ -550,71 +774,109 @@ def e2e_talsh(X, wl, steps):
         run()
     dt = (time.perf_counter() - t0) / steps
     flops = 2.0 * vol(dd) * (vol(ld) * vol(rd) / vol(dd)) ** 0.5
-    res = {"value": round(flops / dt / 1e12, 3), "unit": "TFLOP/s", "ms_per_step": round(dt * 1e3, 2),
+    res = {"value": sig(flops / dt / 1e12), "unit": "TFLOP/s", "ms_per_step": sig(dt * 1e3),
            "h2d_bytes_per_step": (vol(dd) + vol(ld) + vol(rd)) * es, "d2h_bytes_per_step": vol(dd) * es,
            "api": "talshTensorContract(COPY_TTT), host tensors, wall clock incl. H2D/D2H",
            "path": ("inputs streamed to the GPU in slices under the computation" if os.environ.get("TB_STREAM") != "0"
                     else "inputs staged whole, then the contraction")}
+    if seeded and getattr(case, "dchosen", None) is not None:
+        got = torch.from_numpy(D.host_array().copy()).cuda() / float(2 + steps)
+        res["rel_frob_vs_device_result"] = sig(full_rel(got.view(torch.uint8), case.dchosen), 3)
+        del got
     del D, L, R
     return res
 
 
+def measure_peaks(X, s):
+    """Tensor-core rates of this GPU from the library's own probes
+    (tb_peak_measure: operands on chip, no DRAM traffic), in T(FL)OP/s: INT8
+    tcgen05 as a burst (one ~20 ms launch) and sustained (~1.5 s at the power
+    cap), BF16 tcgen05 (burst; compare with the cuBLAS figure in
+    MEASURED_PEAKS.json) and FP64 DMMA."""
+    i8, _ = X.peak_measure(X.PEAK_I8, 280000, s)
+    i8s, i8s_ms = X.peak_measure(X.PEAK_I8, 14000000, s)
+    bf, _ = X.peak_measure(X.PEAK_BF16, 280000, s)
+    f64, _ = X.peak_measure(X.PEAK_F64, 60000, s)
+    return {"i8_tops_burst": sig(i8 / 1e12), "i8_tops_sustained": sig(i8s / 1e12), "sustained_ms": sig(i8s_ms),
+            "bf16_tflops_burst": sig(bf / 1e12), "f64_tflops": sig(f64 / 1e12),
+            "how": "tb_peak_measure: back-to-back MMAs on shared-memory operands, one CTA per SM (DMMA: 4 chains "
+                   "per warp), CUDA events"}
+
+
 # ----------------------------------------------------------------------------- CPU
-def cpu_contraction_sample(steps=1):
-    """The reference's OpenMP+BLAS CPU path (oracle restatement) on a bounded
-    sample of the CCSD-like contraction: v=96, o=48 (same pattern and index
-    map, 1/16 of the FLOPs)."""
+CPU_SAMPLE_A = 48  # the CPU legs contract rows a < 48 of the v=192 workload (1/4 of its FLOPs)
+
+
+def cpu_contraction_sample(steps=1, warmup=1, workload="ccsd1_r8"):
+    """The reference's OpenMP+BLAS CPU contraction path (restated in oracle/:
+    cache-blocked OpenMP permutes and OpenBLAS dgemm, as tensor_block_contract
+    runs them) on a bounded sample of the headline workload: the output rows
+    a < 48 of the v=192 contraction, i.e. the same pattern with the extent of
+    a cut to 48 (M = 9216 of 36864, N and K as in the full workload).
+    Returns the mean over `steps` timed calls after `warmup` untimed ones."""
     import numpy as np
 
     import oracle as O
     nthr = O.nthreads_default()
     if not O.blas_available():
         return None
-    v, o = 96, 48
-    pattern = WORKLOADS["ccsd1_r8"]["pattern"]
-    dd, ld, rd = shapes(pattern, v, o)
-    cptrn, *_ = O.parse_pattern(pattern)
-    L = O.splitmix64_uniform(vol(ld), 1) / v
-    R = O.splitmix64_uniform(vol(rd), 2)
+    wl = WORKLOADS[workload]
+    dd, ld, rd = shapes(wl["pattern"], wl["v"], wl["o"])
+    dd[0], ld[0] = CPU_SAMPLE_A, CPU_SAMPLE_A  # a is the first index of D and of V
+    cptrn, *_ = O.parse_pattern(wl["pattern"])
+    L = O.fill_uniform(vol(ld), 1) / wl["v"]
+    R = O.fill_uniform(vol(rd), 2)
     D = np.zeros(vol(dd))
-    O.contract_blas(cptrn, D, dd, L, ld, R, rd, 1.0, True, nthr)
-    best = None
+    for _ in range(max(0, warmup)):
+        O.contract_blas(cptrn, D, dd, L, ld, R, rd, 1.0, True, nthr)
+    times = []
     for _ in range(max(1, steps)):
         t0 = time.perf_counter()
         O.contract_blas(cptrn, D, dd, L, ld, R, rd, 1.0, True, nthr)
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
+        times.append(time.perf_counter() - t0)
     flops = 2.0 * vol(dd) * (vol(ld) * vol(rd) / vol(dd)) ** 0.5
-    return {"value": round(flops / best / 1e12, 4), "unit": "TFLOP/s", "cores": nthr, "kind": "port",
-            "sample": f"{pattern} v={v} o={o} R8 ({flops:.3e} FLOP), OpenMP permutes + OpenBLAS dgemm, "
-                      f"best of {max(1, steps)}"}
+    mean = sum(times) / len(times)
+    return {"value": sig(flops / mean / 1e12), "unit": "TFLOP/s", "cores": nthr, "kind": "port",
+            "ms_per_step": sig(mean * 1e3),
+            "sample": f"rows a<{CPU_SAMPLE_A} of the v={wl['v']} workload ({flops:.3e} FLOP per step, 1/4 of it): "
+                      f"OpenMP blocked permutes + OpenBLAS dgemm, mean of {len(times)} after {max(0, warmup)}"}
+
+
+def config_of(name):
+    """The bench line's config, identical in both arms."""
+    wl = WORKLOADS[name]
+    return {"workload": f"{name}: {wl['pattern']} v={wl['v']} o={wl['o']}",
+            "l2": "inputs larger than L2 (V alone is 10.9 GB in R8)"}
+
+
+DATA = "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v, D=0)"
 
 
 def run_reference(args):
     """Reference arm: the reference's CPU implementation of the path (its
     OpenMP+BLAS CP-TAL contraction, restated in oracle/ because the Fortran
-    reference cannot be compiled here), on this host's cores."""
+    reference cannot be compiled here), on this host's cores, rank 0 only."""
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
         return
     import oracle as O
     O.build()
-    res = cpu_contraction_sample(steps=max(1, args.steps))
+    res = cpu_contraction_sample(steps=max(1, args.steps), warmup=args.warmup, workload=args.workload)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "bundled OpenBLAS not found"}))
         return
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": "TFLOP/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v)",
-            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['pattern']} "
-                                   f"v={WORKLOADS[args.workload]['v']} o={WORKLOADS[args.workload]['o']}",
-                       "parallelism": "host threads", "sample": res["sample"]},
-            "cpu_baseline": res,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": {4: "f32", 8: "f64"}[WORKLOADS[args.workload]["dtk"]],
+            "data": DATA, "config": config_of(args.workload), "cpu_baseline": res,
             "e2e": {"value": res["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 # ----------------------------------------------------------------------------- main
+OTHER_CONFIGS = ["ccsd2_r8", "ccsd1_c8", "ccsd2_c8", "ccsd1_r4", "ccsd2_r4"]
+
+
 def run_ours(args):
     import torch
 
@@ -626,99 +888,108 @@ def run_ours(args):
     s_obj = torch.cuda.current_stream()
     s = s_obj.cuda_stream
     wl = WORKLOADS[args.workload]
+    extras = world == 1 and not args.headline_only  # the rest of the line runs on one GPU only
+    pk = measure_peaks(X, s) if rank == 0 else None
     bsc = None
-    if rank == 0 and not args.no_block_sparse:
+    if extras and not args.no_block_sparse:
         try:
             bsc = block_sparse_case(X, s, s_obj, 8, steps=1)
         except Exception as exc:  # reported, not fatal: the headline contraction still runs
             bsc = {"error": str(exc)[:300]}
             torch.cuda.synchronize()
             torch.cuda.empty_cache()
-    case = ContractionCase(X, wl, s)
-    torch.cuda.synchronize()
-    # chosen form (plan selector)
-    case.run(X.METHOD_AUTO)
-    torch.cuda.synchronize()
     clocks = Clocks(local)
-    n0 = [0]
+    cnt = {}
 
-    def start_counters():
-        # the warm-up calls include the selector's one-time timing of close
-        # candidates; launches and GEMM events count the timed calls only
-        n0[0] = X.launch_count()
-        X.timing_enable(True)
-        X.timing_read()
+    def start():
+        cnt["n0"] = X.launch_count()
         clocks.start()
-    ms = time_steps(lambda: case.run(X.METHOD_AUTO), args.steps, args.warmup, world, s_obj, on_timed=start_counters)
-    clk = clocks.stop()
-    gemm_ms, gemm_n = X.timing_read()
-    X.timing_enable(False)
-    launches = X.launch_count() - n0[0]
-    st = X.last_contract_stats()
-    chosen_method = {1: "ttgt", 2: "fused"}.get(st.method, str(st.method))
+
+    def stop():
+        cnt["clk"] = clocks.stop()
+        cnt["launches"] = X.launch_count() - cnt["n0"]
+    rec, case, (ms, pms, st, gemm, pgemm) = ccsd_case(
+        X, s, s_obj, args.workload, args.steps, args.warmup, nsamp=4096 if rank == 0 else 0,
+        psteps=max(1, args.steps // 2), world=world, on_timed=start, after_timed=stop)
     ms_max = max_over_ranks(ms, world)
-    value = world * args.steps * case.flops / (ms_max / 1e3) / 1e12
-    # plain form
-    psteps = max(1, args.steps // 2)
-    pms = time_steps(lambda: case.run(X.METHOD_TTGT), psteps, 1, world, s_obj,
-                     on_timed=lambda: (X.timing_enable(True), X.timing_read()))
-    pgemm_ms, pgemm_n = X.timing_read()
-    X.timing_enable(False)
-    plain = case.flops / (max_over_ranks(pms, world) / psteps / 1e3) / 1e12
+    pms_max = max_over_ranks(pms, world)
+    value = world * case.flops / (ms_max / 1e3) / 1e12
+    plain = case.flops / (pms_max / 1e3) / 1e12
+    chosen_method = {1: "ttgt", 2: "fused"}.get(st.method, str(st.method))
     line = None
     if rank == 0:
-        err_chosen = sample_error(X, case, X.METHOD_AUTO)
-        err_plain = sample_error(X, case, X.METHOD_TTGT)
-        perm = permute_sweep(X, s, s_obj, hbm_gbs)
-        try:
-            sel = selector_case(X)
-        except Exception as exc:  # reported, not fatal
-            sel = {"error": str(exc)[:300]}
-        # dominant kernel of the chosen step
+        gemm_ms, gemm_n = gemm
         per_launch_ms = gemm_ms / max(1, gemm_n)
+        i8 = wl["dtk"] in (8, 18)
         if chosen_method == "fused":
-            kern = "tcgen05 INT8-slice GEMM" if wl["dtk"] in (8, 18) else "tcgen05 split-BF16 GEMM"
+            kern = "tc_gemm_kernel: tcgen05 INT8-slice GEMM" if i8 else "tc_gemm_kernel: tcgen05 split-BF16 GEMM"
             hw_ops = case.flops * max(1, st.products)  # each slice pair / BF16 term is a full GEMM
-            peak = 2 * bf16_tflops if wl["dtk"] in (8, 18) else bf16_tflops
-            peak_note = (f"2 x {peak_src} bf16 dense (INT8 dense rate)" if wl["dtk"] in (8, 18)
-                         else f"{peak_src} bf16 dense")
+            peak = pk["i8_tops_sustained"] if i8 else bf16_tflops
+            peak_note = ("measured: tb_peak_measure INT8 tcgen05, sustained (the GEMM runs back to back for the "
+                         "whole timed region)" if i8 else f"{peak_src} cuBLAS bf16 burst (MEASURED_PEAKS.json)")
         else:
-            kern = "FP64 DMMA GEMM (mma.sync m8n8k4)" if wl["dtk"] in (8, 18) else "FP32 FFMA GEMM"
+            kern = "dgemm_tn_kernel: FP64 DMMA" if i8 else "sgemm_tn_kernel: FP32 FFMA"
             hw_ops = case.flops
-            peak = 40.0 if wl["dtk"] in (8, 18) else 75.0
-            peak_note = "nominal B200 FP64 tensor-core rate (not in MEASURED_PEAKS.json)"
+            peak = pk["f64_tflops"]
+            peak_note = "measured: tb_peak_measure FP64 DMMA"
         achieved = hw_ops / (per_launch_ms / 1e3) / 1e12 if gemm_n else None
-        roofline = {"bound": "tensor", "kernel": kern, "achieved": round(achieved, 2) if achieved else None,
-                    "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 3) if achieved else None,
+        roofline = {"bound": "tensor", "kernel": kern, "achieved": sig(achieved) if achieved else None,
+                    "peak": peak, "unit": "TFLOP/s", "frac": sig(achieved / peak, 3) if achieved else None,
                     "traffic": TC_GEMM_TRAFFIC if (chosen_method == "fused" and args.workload == "ccsd1_r8") else None,
-                    "traffic_note": "DRAM read+write bytes per launch: ncu capture of the v=96 case "
-                                    "scaled by the 16x work of v=192",
-                    "peak_source": peak_note, "launch_ms": round(per_launch_ms, 3), "launches_timed": gemm_n}
-        e2e = e2e_talsh(X, wl, steps=max(1, min(2, args.steps)))
-        cpu = cpu_contraction_sample(steps=1) if world == 1 else None
+                    "traffic_note": "dram read+write bytes per launch (ncu, v=96 case scaled by the 16x work)",
+                    "peak_source": peak_note, "frac_of_burst": sig(achieved / pk["i8_tops_burst"], 3)
+                    if (achieved and chosen_method == "fused" and i8) else None,
+                    "launch_ms": sig(per_launch_ms), "launches_timed": gemm_n}
+        plain_rec = {"value": sig(plain), "unit": "TFLOP/s", "method": "ttgt: permute + FP64 DMMA GEMM + permute",
+                     "gemm_ms_per_launch": sig(pgemm[0] / max(1, pgemm[1])),
+                     "gemm_frac_of_measured_f64": sig(case.flops / (pgemm[0] / max(1, pgemm[1]) / 1e3) / 1e12
+                                                      / pk["f64_tflops"], 3) if pgemm[1] else None}
+        error = {"chosen_vs_plain_whole_D_rel_frob": rec["rel_frob_chosen_vs_plain_whole_D"],
+                 "dd_samples": rec.get("dd_samples"), "bound": 1e-12}
+        e2e = configs = c1 = perm = sel = cpu = None
+        if extras:
+            e2e = e2e_talsh(X, wl, steps=max(1, min(2, args.steps)), case=case)
+        del case
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        if extras:
+            configs = {}
+            for name in OTHER_CONFIGS:
+                try:
+                    r, c, _ = ccsd_case(X, s, s_obj, name, 3, 1, nsamp=256, psteps=1)
+                    configs[name] = r
+                    del c
+                except Exception as exc:  # reported, not fatal
+                    configs[name] = {"error": str(exc)[:200]}
+                torch.cuda.synchronize()
+                torch.cuda.empty_cache()
+            c1 = c1_case(X, s, s_obj)
+            perm = permute_sweep(X, s, s_obj, hbm_gbs)
+            try:
+                sel = selector_case(X)
+            except Exception as exc:  # reported, not fatal
+                sel = {"error": str(exc)[:300]}
+            cpu = cpu_contraction_sample(steps=3, warmup=1)
+        if e2e is None:
+            e2e = {"value": None, "note": "end-to-end leg runs at N=1"}
         line = {
-            "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": {4: "f32", 8: "f64", 14: "c64", 18: "c128"}[wl["dtk"]],
-            "data": "synthetic (seeded splitmix64 U[-1,1), V scaled 1/v, D=0)",
-            "config": {"workload": f"{args.workload}: {wl['pattern']} v={wl['v']} o={wl['o']}",
-                       "method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products,
-                       "tile_n": st.tile_n, "tile_m": st.tile_m,
-                       "l2": "inputs larger than L2 (V alone is 10.9 GB)", "parallelism": f"replicas x{world}"},
-            "plain": {"value": round(plain, 3), "unit": "TFLOP/s", "method": "ttgt (permute + FP64 DMMA GEMM)",
-                      "gemm_ms_per_launch": round(pgemm_ms / max(1, pgemm_n), 3),
-                      "chosen_over_plain": round(value / world / plain, 3)},
-            "error": {"chosen": err_chosen, "plain": err_plain, "oracle": "double-double dot products"},
-            "permute": perm, "block_sparse": bsc, "selector": sel, "roofline": roofline, "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": launches, "clocks": clk,
+            "metric": METRIC, "value": sig(value, 5), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sig(ms_max, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {4: "f32", 8: "f64", 14: "c64", 18: "c128"}[wl["dtk"]], "data": DATA,
+            "config": config_of(args.workload),
+            "permute": perm, "configs": configs, "c1": c1, "block_sparse": bsc, "selector": sel, "peaks": pk,
+            "plan": {"method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products,
+                     "tile_n": st.tile_n, "tile_m": st.tile_m, "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": cnt.get("clk"),
+            "gpu_launches": cnt.get("launches"),
+            "plain": plain_rec, "chosen_over_plain": sig(value / world / plain, 3), "error": error,
         }
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     if line is not None:
-        print(json.dumps(line))
+        print(json.dumps(line, separators=(",", ":")))
 
 
 def run_profile(args):
@@ -745,7 +1016,21 @@ def run_profile(args):
         return
     if args.profile == "configs":
         names = [w for w in (args.workloads or "").split(",") if w] or list(WORKLOADS)
-        configs_case(X, s, s_obj, names, max(1, args.steps), max(1, args.warmup))
+        for name in names:
+            rec, c, _ = ccsd_case(X, s, s_obj, name, max(1, args.steps), max(1, args.warmup), nsamp=256, psteps=1)
+            print(json.dumps({"profile": "configs", "workload": name, **rec}), flush=True)
+            del c
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        return
+    if args.profile == "sweep":
+        print(json.dumps({"profile": "sweep", **permute_sweep(X, s, s_obj, peaks()[0])}))
+        return
+    if args.profile == "peaks":
+        print(json.dumps({"profile": "peaks", **measure_peaks(X, s)}))
+        return
+    if args.profile == "c1":
+        print(json.dumps({"profile": "c1", **c1_case(X, s, s_obj)}))
         return
     if args.profile == "e2e":
         wl = dict(WORKLOADS[args.workload])
@@ -798,8 +1083,10 @@ def main():
     ap.add_argument("--dtk", type=int, choices=[4, 8], default=8, help="--profile bsc: data kind (R4 or R8)")
     ap.add_argument("--plan", default=None, help="--profile contract: explicit plan, e.g. method=2,tile_n=256,tile_m=256")
     ap.add_argument("--no-block-sparse", action="store_true", help="skip the block-sparse measurement")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the headline contraction (no sweep, configs, selector, e2e or CPU legs)")
     ap.add_argument("--profile", choices=["contract", "plain", "permute", "permsweep", "bsc", "selector", "e2e",
-                                          "configs"],
+                                          "configs", "sweep", "peaks", "c1"],
                     default=None,
                     help="run one part on a small case for a profiler (no bench line)")
     ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n; bsc: segments per index)")

@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
     L.tb_selector_choose.argtypes = [fp, fp]
     L.tb_fill_uniform.argtypes = [C.c_int, C.c_size_t, vp, C.c_uint64, C.c_double, C.c_double, vp]
     L.tb_last_contract_stats.argtypes = [C.POINTER(ContractStats)]
+    L.tb_peak_measure.argtypes = [C.c_int, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), vp]
     _lib = L
     return L
 
@@ -373,3 +374,15 @@ def last_contract_stats() -> ContractStats:
     st = ContractStats()
     _check(lib().tb_last_contract_stats(C.byref(st)))
     return st
+
+
+PEAK_I8, PEAK_BF16, PEAK_F64 = 1, 2, 3
+
+
+def peak_measure(kind, iters, stream=None):
+    """(operations per second, milliseconds) of a tensor-core throughput probe
+    (PEAK_I8, PEAK_BF16 or PEAK_F64) with operands resident on chip; see
+    tb_peak_measure in include/talsh_b200.h.  Synchronizes the stream."""
+    rate, ms = C.c_double(), C.c_double()
+    _check(lib().tb_peak_measure(int(kind), int(iters), C.byref(rate), C.byref(ms), _stream(stream)))
+    return rate.value, ms.value

@@ -113,13 +113,9 @@ namespace {
 template <int BN, bool I8, int EPI>
 int launch_bsc(const BscParams& P, int grid, cudaStream_t s) {
   constexpr size_t smem = bsc_smem_bytes<BN>();
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(bsc_gemm_kernel<BN, I8, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) { set_error("grouped GEMM smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
-    attr = true;
-  }
+  static DeviceOnce attr;
+  const cudaError_t e = smem_limit_once(attr, bsc_gemm_kernel<BN, I8, EPI>, (int)smem);
+  if (e != cudaSuccess) { set_error("grouped GEMM smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
   bsc_gemm_kernel<BN, I8, EPI><<<grid, kTcThreads, smem, s>>>(P);
   TB_CHECK_LAUNCH();
   return 0;

@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
     uint32_t acc_it = 0;
     for (uint32_t k = 0; ok; ++k) {
       const int slot = (int)(k % kBscRing);
-      if (!(ok = mbar_wait(&bars->item_full[slot], (k / kBscRing) & 1, P.err, 16u))) break;
+      if (!(ok = mbar_wait_warp(&bars->item_full[slot], (k / kBscRing) & 1, P.err, 16u))) break;
       const int cur = bars->ring[slot];
       if (cur < 0) break;
       const BscItem I = P.items[cur];
@@ -215,11 +215,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
       // all pairs of an output block share its row and column scales
       const BscPair pr0 = P.pairs[P.chunks[P.passes[Dd.pass0].chunk0].p0];
       const int re = (EPI == EPI_OZAKI_R) && mval ? P.lops[pr0.l].rowexp[m] : 0;
-      const EpiView V{Dd.D, Dd.dn, P.rops[pr0.r].colexp, Dd.N, P.ar, P.ai, P.br, P.bi};
+      const EpiView V{Dd.D, Dd.dn, P.rops[pr0.r].colexp, Dd.N, P.ar, P.ai, P.br, P.bi, 0};
       for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err, 17u))) break;
+        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 17u))) break;
         tc_fence_after();
         const int shift = (EPI == EPI_OZAKI_R) ? P.passes[p].shift : 0;
         epilogue_pass<BN, EPI>(V, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, I.nt,

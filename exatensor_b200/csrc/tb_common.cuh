@@ -1,6 +1,7 @@
 // tb_common.cuh -- shared definitions for the B200 tensor-algebra kernels.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -52,6 +53,30 @@ void timed_end(int slot, cudaStream_t s);
 
 // Number of SMs of the current device (cached).
 int num_sms();
+
+// The current CUDA device, 0..63 (0 when the query fails).
+int current_device();
+
+// Once-per-device flags.  Function attributes (the dynamic shared-memory
+// limit) and occupancy results belong to one device's context, so each
+// device sets or measures them on its first launch.  Devices are a bit mask;
+// concurrent first launches may both set the attribute, which is harmless.
+struct DeviceOnce {
+  std::atomic<unsigned long long> bits{0};
+  bool done(int dev) const { return (bits.load(std::memory_order_acquire) >> dev) & 1ull; }
+  void mark(int dev) { bits.fetch_or(1ull << dev, std::memory_order_acq_rel); }
+};
+
+// Raises the dynamic shared-memory limit of `kern` to `bytes` on the current
+// device the first time it is asked for that device.
+template <typename K>
+inline cudaError_t smem_limit_once(DeviceOnce& once, K kern, int bytes) {
+  const int dev = current_device();
+  if (once.done(dev)) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) once.mark(dev);
+  return e;
+}
 
 // Stream-ordered scratch from the device's default memory pool.
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s);

@@ -374,12 +374,9 @@ int gemm_plain_tn(int dtk, int64_t M, int64_t N, int64_t K, const void* A, int64
   switch (dtk) {
     case kR8: {
       const size_t smem = (size_t)D_ST * (D_BM + D_BN) * D_LD * sizeof(double);
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(dgemm_tn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(dgemm_tn_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-      }
+      static DeviceOnce attr16, attr8;
+      TB_CUDA(smem_limit_once(attr16, dgemm_tn_kernel<true>, (int)smem));
+      TB_CUDA(smem_limit_once(attr8, dgemm_tn_kernel<false>, (int)smem));
       dim3 grid((unsigned)((N + D_BN - 1) / D_BN), (unsigned)((M + D_BM - 1) / D_BM));
       const bool v16 = (lda % 2 == 0) && (ldb % 2 == 0) && ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0);
       if (v16)
@@ -392,11 +389,8 @@ int gemm_plain_tn(int dtk, int64_t M, int64_t N, int64_t K, const void* A, int64
     }
     case kC8: {
       const size_t smem = (size_t)Z_ST * (Z_BM + Z_BN) * Z_LD * sizeof(double2);
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(zgemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-      }
+      static DeviceOnce attr;
+      TB_CUDA(smem_limit_once(attr, zgemm_tn_kernel, (int)smem));
       dim3 grid((unsigned)((N + Z_BN - 1) / Z_BN), (unsigned)((M + Z_BM - 1) / Z_BM));
       zgemm_tn_kernel<<<grid, 256, smem, s>>>((int)M, (int)N, (int)K, (const double2*)A, lda, (const double2*)B,
                                              ldb, (double2*)C, ldc, ar, ai, br, bi, lconj, rconj);

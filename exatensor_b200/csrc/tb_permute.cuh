@@ -14,6 +14,7 @@
 #pragma once
 #include "tb_common.cuh"
 #include "tb_perm_plan.h"
+#include "tb_sm100.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -35,7 +36,6 @@ constexpr int kPermThreads = 256;
 // the Store functor:  __device__ void operator()(int64_t out_off, const Elem&).
 // ---------------------------------------------------------------------------
 constexpr int kStages = 3;
-constexpr uint32_t kWaitLimit = 1u << 26;  // bounded mbarrier polling
 
 struct PermSmem {
   int64_t ld_base[kMaxChunks];
@@ -224,24 +224,22 @@ perm_pipe_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ 
     else if (!BULK) asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
   bool failed = false;
-  for (int64_t k = 0; k < mine; ++k) {
+  int64_t k = 0;
+  for (; k < mine; ++k) {
     const int stg = (int)(k % kStages);
     if (BULK) {
+      // Every thread waits for the stage itself (its wait makes the bulk
+      // copies' bytes visible to it); the wait is bounded in time (about two
+      // seconds on the global timer) and the decision to give up is taken for
+      // the whole CTA at once, so that no thread leaves the others behind at
+      // a barrier.
       const uint32_t parity = (uint32_t)((k / kStages) & 1);
-      uint32_t done = 0, it = 0;
-      while (!done) {
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(smem_addr(&T.mbar[stg])), "r"(parity)
-            : "memory");
-        if (!done && ++it > kWaitLimit) { failed = true; break; }
-      }
+      const bool ok = sm100::mbar_wait(reinterpret_cast<uint64_t*>(&T.mbar[stg]), parity, nullptr);
+      if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
     } else {
       asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+      __syncthreads();
     }
-    if (failed) break;
-    __syncthreads();
     const int64_t nk = k + kStages - 1;
     const int nstg = (int)(nk % kStages);
     if (nk < mine) perm_issue<Elem, BULK>(P, T, in, bufs + (size_t)nstg * stage_elems, &T.mbar[nstg], first + nk * step);
@@ -249,6 +247,12 @@ perm_pipe_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ 
     perm_store<Elem, Store>(P, T, SL, bufs + (size_t)stg * stage_elems, first + k * step, st);
   }
   if (failed) {
+    // leave no bulk copy in flight into this CTA's shared memory: wait, again
+    // bounded, for the stages still loading (tiles k .. k + kStages - 2)
+    if (threadIdx.x == 0)
+      for (int64_t j = k; j < mine && j < k + kStages - 1; ++j)
+        sm100::mbar_wait(reinterpret_cast<uint64_t*>(&T.mbar[j % kStages]), (uint32_t)((j / kStages) & 1), nullptr);
+    __syncthreads();
     record_device_error(err, 1u);
     return;
   }
@@ -522,20 +526,24 @@ void launch_2d(int N, int64_t ntiles, size_t smem, cudaStream_t s, const PermPar
   const Kern kern = idx == 2 ? (Kern)perm2d_kernel<Elem, Store, VB, ROWS, (VB > 0 ? 16 : 0)>
                   : idx == 1 ? (Kern)perm2d_kernel<Elem, Store, VB, ROWS, (VB > 0 ? 8 : 0)>
                              : (Kern)perm2d_kernel<Elem, Store, VB, ROWS, 0>;
-  static bool attr[3] = {false, false, false};
-  static size_t occ_smem[3] = {0, 0, 0};
-  static int occ_blocks[3] = {0, 0, 0};
-  if (!attr[idx]) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    attr[idx] = true;
-  }
-  if (occ_smem[idx] != smem) {
+  // per variant and device: the shared-memory limit, and the resident CTAs
+  // per SM of the last shared-memory size (packed as smem << 8 | blocks)
+  static DeviceOnce attr[3];
+  static std::atomic<unsigned long long> occ[3][64];
+  const int dev = current_device();
+  smem_limit_once(attr[idx], kern, 220 * 1024);
+  unsigned long long o = occ[idx][dev].load(std::memory_order_relaxed);
+  int blocks = (int)(o & 0xFF);
+  if ((o >> 8) != (unsigned long long)smem || blocks < 1) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kPermThreads, smem) != cudaSuccess || b < 1) b = 1;
-    occ_smem[idx] = smem;
-    occ_blocks[idx] = b;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kPermThreads, smem) != cudaSuccess || b < 1) {
+      cudaGetLastError();
+      b = 1;
+    }
+    blocks = std::min(b, 255);
+    occ[idx][dev].store(((unsigned long long)smem << 8) | (unsigned long long)blocks, std::memory_order_relaxed);
   }
-  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)num_sms() * occ_blocks[idx], ntiles);
+  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)num_sms() * blocks, ntiles);
   kern<<<grid, kPermThreads, smem, s>>>(P, in, st, flags);
 }
 
@@ -563,12 +571,9 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
   static const bool longrows_bulk = [] { const char* e = getenv("TB_PERM_LONGROWS"); return e && !strcmp(e, "bulk"); }();
   const bool bulk = eligible && (mode == 1 || (mode == 0 && (int64_t)P.LA * P.es >= 4096 &&
                                                (!P.rows2d || longrows_bulk || P.bulk_rows)));
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(perm_pipe_kernel<Elem, Store, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(perm_pipe_kernel<Elem, Store, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    attr_set = true;
-  }
+  static DeviceOnce attr_bulk, attr_async;
+  smem_limit_once(attr_bulk, perm_pipe_kernel<Elem, Store, true>, 220 * 1024);
+  smem_limit_once(attr_async, perm_pipe_kernel<Elem, Store, false>, 220 * 1024);
   if (smem > 220 * 1024) { set_error("permutation tile too large for shared memory"); return TB_ERR_LIMIT; }
   int per_sm = (int)((224 * 1024) / (smem + 1024));
   if (per_sm < 1) per_sm = 1;

@@ -16,13 +16,13 @@ thread_local char g_err[512] = "";
 int g_sms[64] = {0};
 unsigned int* g_err_word[64] = {nullptr};
 std::mutex g_mu;
+}  // namespace
 
 int current_device() {
   int d = 0;
-  cudaGetDevice(&d);
+  if (cudaGetDevice(&d) != cudaSuccess) { cudaGetLastError(); return 0; }
   return d < 0 || d >= 64 ? 0 : d;
 }
-}  // namespace
 
 thread_local bool g_timing = false;
 thread_local std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timed;

@@ -61,6 +61,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
   return false;
 }
 
+// Warp-collective form of mbar_wait: every lane waits, and the warp gives up
+// together when any lane's wait expired, so that the warp-collective
+// operations after it (tcgen05.ld, __syncwarp, shuffles) are reached by all
+// 32 lanes or by none.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, unsigned int* err, unsigned code = 1u) {
+  const bool ok = mbar_wait(bar, parity, err, code);
+  return __all_sync(0xffffffffu, ok ? 1 : 0) != 0;
+}
+
 // TMA: 3-D tiled load (x = innermost) into shared memory, completion on bar.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
   asm volatile(

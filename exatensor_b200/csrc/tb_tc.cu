@@ -57,13 +57,9 @@ struct Operand {
 template <int BN, bool I8, int EPI>
 int launch_tc(const TcGemmParams& P, cudaStream_t s) {
   constexpr size_t smem = tc_smem_bytes<BN>();
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<BN, I8, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) { set_error("tcgen05 GEMM smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
-    attr = true;
-  }
+  static DeviceOnce attr;
+  const cudaError_t e = smem_limit_once(attr, tc_gemm_kernel<BN, I8, EPI>, (int)smem);
+  if (e != cudaSuccess) { set_error("tcgen05 GEMM smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
   const int tiles = P.mtiles * P.ntiles;
   const int grid = std::max(1, std::min(tiles, num_sms()));
   tc_gemm_kernel<BN, I8, EPI><<<grid, kTcThreads, smem, s>>>(P);
@@ -75,7 +71,10 @@ int launch_tc(const TcGemmParams& P, cudaStream_t s) {
 template <int BN, bool I8, int EPI>
 int launch_tc2(const TcGemmParams& P, cudaStream_t s) {
   constexpr size_t smem = tc2_smem_bytes<BN>();
-  static int max_pairs = 0;
+  // per device: the shared-memory limit and the pairs resident at once
+  static std::atomic<int> max_pairs_of[64];
+  const int dev = current_device();
+  int max_pairs = max_pairs_of[dev].load(std::memory_order_relaxed);
   if (!max_pairs) {
     cudaError_t e = cudaFuncSetAttribute(tc_gemm2_kernel<BN, I8, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -96,6 +95,7 @@ int launch_tc2(const TcGemmParams& P, cudaStream_t s) {
       n = num_sms() / 2;
     }
     max_pairs = n;
+    max_pairs_of[dev].store(n, std::memory_order_relaxed);
   }
   const int tiles = P.mtiles * P.ntiles;
   const int pairs = std::max(1, std::min(tiles, max_pairs));
@@ -248,7 +248,8 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   const size_t offA = 0, offB = al(bytesA), offDm = offB + al(bytesB), offDn = offDm + al(M * 8),
                offLA = offDn + al(Nc * 8), offLB = offLA + al(M * 8), offKA = offLB + al(Nc * 8),
                offKB = offKA + al(K * 8), offRE = offKB + al(K * 8), offCE = offRE + al(M * 4),
-               offRX = offCE + al(Nc * 4), offCX = offRX + al(M * 4), total = offCX + al(Nr * 4);
+               offRX = offCE + al(Nc * 4), offCX = offRX + al(M * 4), offBR = offCX + al(Nr * 4),
+               offBC = offBR + al(M * 4), offNB = offBC + al(Nc * 4), total = offNB + 256;
   unsigned char* ws = nullptr;
   if (int e = scratch_alloc((void**)&ws, total, s)) return e;
   int err = 0;
@@ -264,6 +265,9 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   unsigned* colE = (unsigned*)(ws + offCE);
   int* rowx = (int*)(ws + offRX);
   int* colx = (int*)(ws + offCX);
+  int* badrows = (int*)(ws + offBR);  // rows of A / columns of B holding a NaN or an infinity
+  int* badcols = (int*)(ws + offBC);
+  int* nbad = (int*)(ws + offNB);
   const int64_t ksrc_pad = cplx ? Kpad / 2 : Kpad;  // padded K in source elements
   do {
     if ((err = build_offsets(A.rows, true, dm, s))) break;
@@ -281,8 +285,21 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     GB.lanes_on_k = (B.ks[0].s1 == 1 || B.rows.empty() || B.rows[0].s1 != 1) ? 1 : 0;
     const int tmr = i8 && cplx ? 32 : 64;               // gather tile rows (16-byte elements: 32)
     const int64_t gA = Mpad / tmr, gB = (cplx ? Npad / 2 : Npad) / tmr, gk = ksrc_pad / kGK;
+    // row / column exponents and the lists of rows and columns flagged as
+    // holding a NaN or an infinity (exponent field 2047): the epilogue leaves
+    // their D entries to nonfinite_fixup_kernel
+    if (cudaMemsetAsync(rowE, 0, offRX - offRE, s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
+    if (cudaMemsetAsync(nbad, 0, 2 * sizeof(int), s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
+    auto run_exps = [&]() -> int {
+      exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 4096)), 256, 0, s>>>(rowE, rowx, M, 1,
+                                                                                                 badrows, nbad);
+      TB_CHECK_LAUNCH();
+      exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((Nr + 255) / 256, 4096)), 256, 0, s>>>(
+          colE, colx, Nr, cplx ? 2 : 1, badcols, nbad + 1);
+      TB_CHECK_LAUNCH();
+      return 0;
+    };
     if (i8) {
-      if (cudaMemsetAsync(rowE, 0, offRX - offRE, s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
       const int64_t eA = (M + tmr - 1) / tmr, eB = (Nc + tmr - 1) / tmr, ek = (K + kGK - 1) / kGK;
       if (!cplx) {
         if ((err = run_rowmax<false>(GA, eA, ek, s))) break;
@@ -291,11 +308,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
         if ((err = run_rowmax<true>(GA, eA, ek, s))) break;
         if ((err = run_rowmax<true>(GB, eB, ek, s))) break;
       }
-      exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 4096)), 256, 0, s>>>(rowE, rowx, M, 1);
-      exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((Nr + 255) / 256, 4096)), 256, 0, s>>>(colE, colx, Nr,
-                                                                                                  cplx ? 2 : 1);
-      count_launch();
-      count_launch();
+      if ((err = run_exps())) break;
       if (!cplx) {
         if ((err = run_gather<G_SLICE_R8>(GA, gA, gk, s))) break;
         if ((err = run_gather<G_SLICE_R8>(GB, gB, gk, s))) break;
@@ -311,9 +324,12 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
         if ((err = run_gather<G_SPLIT_C4A>(GA, gA, gk, s))) break;
         if ((err = run_gather<G_SPLIT_C4B>(GB, gB, gk, s))) break;
       }
+      if ((err = run_exps())) break;  // the split gathers flag non-finite rows
     }
     // GEMM parameters
-    static TcGemmParams P;  // large: kept off the stack
+    // per call (about 2 KB), so that host threads contracting on different
+    // streams never share a parameter block
+    TcGemmParams P;
     std::memset(&P, 0, sizeof(P));
     if ((err = make_operand_map(&P.tmA, Ap, i8, Kpad, Mpad, npa, 128))) break;
     if ((err = make_operand_map(&P.tmB, Bp, i8, Kpad, Npad, npb, pair ? BN / 2 : BN))) break;
@@ -336,10 +352,32 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     P.ar = realpha; P.ai = cplx ? ai : 0.0;
     P.br = accumulate ? 1.0 : 0.0; P.bi = 0.0;
     P.err = device_error_word();
+    P.nf_skip = 1;
     const int epi = i8 ? (cplx ? EPI_OZAKI_C : EPI_OZAKI_R) : (cplx ? EPI_BF16_C : EPI_BF16_R);
     const int ts = timed_begin(s);
     err = BN == 256 ? launch_tc_epi<256>(P, epi, pair, s) : launch_tc_epi<128>(P, epi, pair, s);
     timed_end(ts, s);
+    if (err) break;
+    // entries of rows / columns with a NaN or an infinity (returns at once without)
+    NfParams F;
+    F.srcA = A.ptr; F.srcB = B.ptr;
+    F.lmA = lmA; F.lkA = lkA; F.lmB = lmB; F.lkB = lkB;
+    F.dm = dm; F.dn = dn; F.D = d;
+    F.M = M; F.N = Nc; F.K = K;
+    F.rowE = rowE; F.badrows = badrows; F.badcols = badcols; F.nbad = nbad;
+    F.isignA = A.conj ? -1.0 : 1.0; F.isignB = B.conj ? -1.0 : 1.0;
+    F.ar = realpha; F.ai = cplx ? ai : 0.0; F.br = P.br; F.bi = 0.0;
+    const unsigned fgrid = (unsigned)(2 * num_sms());
+    if (dtk == kR8) nonfinite_fixup_kernel<double, false><<<fgrid, 256, 0, s>>>(F);
+    else if (dtk == kC8) nonfinite_fixup_kernel<double, true><<<fgrid, 256, 0, s>>>(F);
+    else if (dtk == kR4) nonfinite_fixup_kernel<float, false><<<fgrid, 256, 0, s>>>(F);
+    else nonfinite_fixup_kernel<float, true><<<fgrid, 256, 0, s>>>(F);
+    count_launch();
+    if (cudaError_t e = cudaGetLastError()) {
+      set_error("non-finite fix-up launch: %s", cudaGetErrorString(e));
+      err = TB_ERR_CUDA;
+      break;
+    }
     if (stats) {
       stats->slices = S;
       stats->passes = (int)passes.size();

@@ -45,7 +45,13 @@ struct __align__(64) TcGemmParams {
   const int* colexp;          // INT8 slices: column scale exponents
   double ar, ai, br, bi;      // alpha, beta
   unsigned int* err;
+  int nf_skip;                // 1: leave entries of flagged rows / columns to the non-finite fix-up
 };
+
+// A row or column whose exponent entry exceeds this holds a NaN or an
+// infinity (exponent field 2047, minus 1021): with nf_skip the epilogue leaves
+// its D entries untouched for the non-finite fix-up kernel.
+constexpr int kNonFiniteExp = 2047 - 1021;
 
 // Epilogue view of one output block: what epilogue_pass reads besides TMEM.
 struct EpiView {
@@ -54,6 +60,7 @@ struct EpiView {
   const int* colexp;
   int N;
   double ar, ai, br, bi;
+  int nf_skip;
 };
 
 struct TcSmemBarriers {
@@ -104,7 +111,9 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
     const int nl = n0 + lane;
     const bool lvalid = nl < P.N;
     const int64_t dn_l = lvalid ? P.dn[CPLX ? (nl >> 1) : nl] : 0;
-    const int ce_l = (OZ && lvalid) ? P.colexp[nl] : 0;
+    const int ce_l = ((OZ || P.nf_skip) && lvalid) ? P.colexp[nl] : 0;
+    // columns left to the non-finite fix-up
+    const unsigned skipc = __ballot_sync(0xffffffffu, P.nf_skip && ce_l >= kNonFiniteExp);
     if (!CPLX) {
       using T = typename std::conditional<OZ, double, float>::type;
       T* D = (T*)P.D;
@@ -118,7 +127,7 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
       for (int j = 0; j < 32; ++j) {
         const int64_t dn = __shfl_sync(0xffffffffu, dn_l, j);
         const int ce = __shfl_sync(0xffffffffu, ce_l, j);
-        if (!mval || n0 + j >= P.N) continue;
+        if (!mval || n0 + j >= P.N || ((skipc >> j) & 1u)) continue;
         T v;
         if (OZ) v = (T)(P.ar * scale2((double)(int)r[j], re + ce - shift));
         else v = (T)P.ar * __uint_as_float(r[j]);
@@ -145,7 +154,7 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
       for (int j = 0; j < 16; ++j) {
         const int64_t dn = __shfl_sync(0xffffffffu, dn_l, 2 * j);
         const int ce = __shfl_sync(0xffffffffu, ce_l, 2 * j);
-        if (!mval || n0 + 2 * j >= P.N) continue;
+        if (!mval || n0 + 2 * j >= P.N || ((skipc >> (2 * j)) & 1u)) continue;
         T xr, xi;
         if (OZ) {
           const int e = re + ce - shift;
@@ -262,13 +271,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
     for (int t = blockIdx.x; t < ntile_total && ok; t += gridDim.x) {
       const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
       const int m = mb * 128 + quad * 32 + lane;
-      const bool mval = m < P.M;
+      const int re = ((EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) || P.nf_skip) && m < P.M ? P.rowexp[m] : 0;
+      const bool mval = m < P.M && !(P.nf_skip && re >= kNonFiniteExp);  // flagged rows: the fix-up's
       const int64_t dmo = mval ? P.dm[m] : 0;
-      const int re = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) && mval ? P.rowexp[m] : 0;
       for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err))) break;
+        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
         tc_fence_after();
         const bool first = (p == 0);
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) ? P.pass_shift[p] : 0;
@@ -414,13 +423,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
     for (int t = pair; t < ntile_total && ok; t += npairs) {
       const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
       const int m = mb * 256 + (int)rank * 128 + quad * 32 + lane;
-      const bool mval = m < P.M;
+      const int re = ((EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) || P.nf_skip) && m < P.M ? P.rowexp[m] : 0;
+      const bool mval = m < P.M && !(P.nf_skip && re >= kNonFiniteExp);  // flagged rows: the fix-up's
       const int64_t dmo = mval ? P.dm[m] : 0;
-      const int re = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) && mval ? P.rowexp[m] : 0;
       for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait(&bars->acc_full[a], aph, P.err))) break;
+        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
         tc_fence_after();
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) ? P.pass_shift[p] : 0;
         epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, nb,

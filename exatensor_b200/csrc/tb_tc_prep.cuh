@@ -122,7 +122,8 @@ struct GatherParams {
   int64_t kpad;        // real row length of the output planes (elements)
   int64_t pstride;     // elements per plane
   void* planes;
-  unsigned* rowE;      // exponent fields (exp modes write, slice modes read)
+  unsigned* rowE;      // per row: largest exponent field (slice modes read it; the
+                       // split modes set it to 2047 for rows with a NaN or an infinity)
   int slices;
   int lanes_on_k;      // 1: consecutive k are contiguous in the source
   double isign;        // -1 conjugates the imaginary part
@@ -247,8 +248,13 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
             }
         } else if constexpr (MODE == G_SPLIT_R4) {
           __nv_bfloat16 h[4], l[4];
+          bool nf = false;
 #pragma unroll
-          for (int t = 0; t < 4; ++t) split_bf16(tile[mm][kq + t], h[t], l[t]);
+          for (int t = 0; t < 4; ++t) {
+            split_bf16(tile[mm][kq + t], h[t], l[t]);
+            nf |= !isfinite(tile[mm][kq + t]);
+          }
+          if (nf && P.rowE && m < P.rows) atomicMax(&P.rowE[m], 2047u);  // row left to the non-finite fix-up
           __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + k;
           __nv_bfloat162 hh[2] = {{h[0], h[1]}, {h[2], h[3]}}, ll[2] = {{l[0], l[1]}, {l[2], l[3]}};
           *reinterpret_cast<uint2*>(base) = *reinterpret_cast<uint2*>(hh);
@@ -256,6 +262,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
         } else {
           // complex FP32: A' rows (re, im); B' rows 2n (re, -im), 2n+1 (im, re)
           __nv_bfloat16 hr[4], lr[4], hi[4], li[4], nhi[4], nli[4];
+          bool nf = false;
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
             const E v = tile[mm][kq + t];
@@ -263,7 +270,9 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
             split_bf16(v.x, hr[t], lr[t]);
             split_bf16(im, hi[t], li[t]);
             split_bf16(-im, nhi[t], nli[t]);
+            nf |= !isfinite(v.x) || !isfinite(v.y);
           }
+          if (nf && P.rowE && m < P.rows) atomicMax(&P.rowE[m], 2047u);  // row left to the non-finite fix-up
           if constexpr (MODE == G_SPLIT_C4A) {
             __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + 2 * k;
             __nv_bfloat162 H[4] = {{hr[0], hi[0]}, {hr[1], hi[1]}, {hr[2], hi[2]}, {hr[3], hi[3]}};
@@ -302,10 +311,104 @@ __global__ void __launch_bounds__(kGThreads, 4) gather_grouped_kernel(const Gath
   gather_body<MODE>(P, jm.y, blockIdx.y, gridDim.y);
 }
 
-// exponents: rowexp[r] = rowE[r / rep] - 1021 (rep = 2 for complex B' rows)
-__global__ void exps_kernel(const unsigned* __restrict__ rowE, int* __restrict__ out, int64_t n, int rep) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int)rowE[i / rep] - 1021;
+// exponents: rowexp[r] = rowE[r / rep] - 1021 (rep = 2 for complex B' rows).
+// With a list, the source rows flagged 2047 (a NaN or an infinity) are also
+// appended to it (in no particular order; *count counts them).
+__global__ void exps_kernel(const unsigned* __restrict__ rowE, int* __restrict__ out, int64_t n, int rep,
+                            int* __restrict__ list = nullptr, int* __restrict__ count = nullptr) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned e = rowE[i / rep];
+    out[i] = (int)e - 1021;
+    if (list && e >= 2047u && i % rep == 0) list[atomicAdd(count, 1)] = (int)(i / rep);
+  }
+}
+
+// ---- non-finite fix-up -----------------------------------------------------------
+// D entries whose row of A or column of B holds a NaN or an infinity are left
+// untouched by the GEMM epilogue (nf_skip) and computed here as plain dot
+// products in FP64 (FP32 data too, rounded once at the end), so that
+// non-finite values propagate the way an IEEE GEMM propagates them: a NaN
+// term, an infinity times zero, or infinities of both signs give NaN; other
+// infinities give an infinity of their sign.  Work: one warp per entry, the
+// entries of the flagged rows (all columns) and then of the flagged columns
+// (the rows that are not flagged).  With nothing flagged every CTA returns at
+// once.
+struct NfParams {
+  const void* srcA;
+  const void* srcB;
+  const int64_t *lmA, *lkA, *lmB, *lkB;  // operand offsets (rows, contracted index)
+  const int64_t *dm, *dn;                 // D offsets of rows of A and columns of B
+  void* D;
+  int64_t M, N, K;                        // rows of A, columns of B (complex: pairs), contracted extent
+  const unsigned* rowE;                   // 2047: the row holds a non-finite value
+  const int* badrows;                     // flagged rows of A, count nbad[0]
+  const int* badcols;                     // flagged columns of B, count nbad[1]
+  const int* nbad;
+  double isignA, isignB;                  // -1: conjugate the operand
+  double ar, ai, br, bi;                  // alpha, beta (beta 0: D is not read)
+};
+
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) nonfinite_fixup_kernel(const __grid_constant__ NfParams P) {
+  const int nbr = P.nbad[0], nbc = P.nbad[1];
+  if (nbr == 0 && nbc == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t total = (int64_t)nbr * P.N + (int64_t)nbc * P.M;
+  for (int64_t e = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); e < total; e += warps) {
+    int64_t m, n;
+    if (e < (int64_t)nbr * P.N) {
+      m = P.badrows[e / P.N];
+      n = e % P.N;
+    } else {
+      const int64_t f = e - (int64_t)nbr * P.N;
+      n = P.badcols[f / P.M];
+      m = f % P.M;
+      if (P.rowE[m] >= 2047u) continue;  // done with the flagged rows
+    }
+    const int64_t a0 = P.lmA[m], b0 = P.lmB[n];
+    double sr = 0.0, si = 0.0;
+    if constexpr (!CPLX) {
+      const R* A = (const R*)P.srcA;
+      const R* B = (const R*)P.srcB;
+      for (int64_t k = lane; k < P.K; k += 32) sr += (double)A[a0 + P.lkA[k]] * (double)B[b0 + P.lkB[k]];
+    } else {
+      using C2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
+      const C2* A = (const C2*)P.srcA;
+      const C2* B = (const C2*)P.srcB;
+      for (int64_t k = lane; k < P.K; k += 32) {
+        const C2 x = A[a0 + P.lkA[k]], y = B[b0 + P.lkB[k]];
+        const double xr = x.x, xi = P.isignA * (double)x.y, yr = y.x, yi = P.isignB * (double)y.y;
+        sr += xr * yr - xi * yi;
+        si += xr * yi + xi * yr;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      if (CPLX) si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane != 0) continue;
+    const int64_t off = P.dm[m] + P.dn[n];
+    if constexpr (!CPLX) {
+      R* D = (R*)P.D;
+      const double v = P.ar * sr;
+      D[off] = (R)(P.br == 0.0 ? v : P.br * (double)D[off] + v);
+    } else {
+      using C2 = typename std::conditional<sizeof(R) == 8, double2, float2>::type;
+      C2* D = (C2*)P.D;
+      double vr = P.ar * sr - P.ai * si, vi = P.ar * si + P.ai * sr;
+      if (P.br != 0.0 || P.bi != 0.0) {
+        const C2 d = D[off];
+        vr += P.br * (double)d.x - P.bi * (double)d.y;
+        vi += P.br * (double)d.y + P.bi * (double)d.x;
+      }
+      C2 w;
+      w.x = (R)vr;
+      w.y = (R)vi;
+      D[off] = w;
+    }
+  }
 }
 
 

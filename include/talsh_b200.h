@@ -280,6 +280,21 @@ typedef struct {
 } tb_contract_stats_t;
 int tb_last_contract_stats(tb_contract_stats_t* stats);
 
+/* Tensor-core throughput probes (diagnostics; no counterpart in the
+ * reference, which has no tensor-core code): the rooflines of the
+ * contraction kernels, measured on this GPU.  Each runs `iters` MMAs per
+ * issuing unit with operands resident on chip (no global memory traffic)
+ * once untimed, then once between CUDA events on `stream`, synchronizes, and
+ * returns the rate in operations per second (2*M*N*K per MMA) and the timed
+ * launch's milliseconds (ms may be NULL).
+ *   TB_PEAK_I8    tcgen05.mma kind::i8, M 128 x N 256 x K 32, one CTA per SM
+ *   TB_PEAK_BF16  tcgen05.mma kind::f16 with BF16 inputs, M 128 x N 256 x K 16
+ *   TB_PEAK_F64   mma.sync m8n8k4 FP64 (DMMA), four chains per warp */
+#define TB_PEAK_I8 1
+#define TB_PEAK_BF16 2
+#define TB_PEAK_F64 3
+int tb_peak_measure(int kind, long long iters, double* ops_per_s, double* ms, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

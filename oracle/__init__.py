@@ -58,6 +58,8 @@ def lib():
         L.orc_init.argtypes = [C.c_int, C.c_int64, C.c_void_p, C.c_double, C.c_double]
         L.orc_norm.argtypes = [C.c_int, C.c_int64, C.c_void_p, C.c_int]
         L.orc_norm.restype = C.c_double
+        L.orc_fill_uniform.argtypes = [C.c_int64, C.c_uint64, C.c_double, C.c_double, C.c_void_p, C.c_int]
+        L.orc_dd_dot_batch.argtypes = [C.c_int, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.orc_contract.argtypes = [ip, C.c_int, C.c_int, ip, C.c_void_p, C.c_int, ip, C.c_void_p,
                                    C.c_int, ip, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int,
                                    C.c_int, C.c_int]
@@ -200,6 +202,21 @@ def contract(cptrn, d, ddims, l, ldims, r, rdims, alpha=1.0, conj_bits=0, accumu
     return d
 
 
+def dd_dot_batch(l: np.ndarray, r: np.ndarray, nthreads=None) -> np.ndarray:
+    """Row-wise dot products of two (n, K) float64 or complex128 arrays with
+    double-double accumulation, rounded once (the FP64 error oracle for
+    sampled elements of large contractions)."""
+    l = np.ascontiguousarray(l)
+    r = np.ascontiguousarray(r)
+    assert l.shape == r.shape and l.ndim == 2 and l.dtype == r.dtype
+    out = np.empty(l.shape[0], dtype=l.dtype)
+    err = lib().orc_dd_dot_batch(_dtk(l), l.shape[0], l.shape[1], _ptr(l), _ptr(r), _ptr(out),
+                                 nthreads or nthreads_default())
+    if err:
+        raise ValueError(f"orc_dd_dot_batch error {err}")
+    return out
+
+
 def blas_available() -> bool:
     for p in OPENBLAS_CANDIDATES:
         if os.path.exists(p) and lib().orc_blas_load(p.encode()) == 0:
@@ -230,6 +247,14 @@ def splitmix64_uniform(n: int, seed: int, lo=-1.0, hi=1.0) -> np.ndarray:
         z = z ^ (z >> np.uint64(31))
     u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
     return lo + (hi - lo) * u
+
+
+def fill_uniform(n: int, seed: int, lo=-1.0, hi=1.0, nthreads=None) -> np.ndarray:
+    """splitmix64_uniform computed by the C oracle on all host threads (the
+    same bits; for the large CPU-baseline operands)."""
+    out = np.empty(n, dtype=np.float64)
+    lib().orc_fill_uniform(n, seed, lo, hi, _ptr(out), nthreads or nthreads_default())
+    return out
 
 
 def rel_frobenius(x: np.ndarray, ref: np.ndarray) -> float:

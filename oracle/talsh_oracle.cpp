@@ -26,6 +26,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <string>
+#include <memory>
 #include <vector>
 #include <algorithm>
 #include <dlfcn.h>
@@ -668,6 +669,9 @@ int orc_blas_load(const char* path) {
   return (g_dgemm && g_sgemm) ? 0 : 2;
 }
 
+int orc_permute_blocked(int dtk, int rank, const int* dims, const int* o2n, const void* in, void* out,
+                        int nthreads);
+
 int orc_contract_blas(const int* cptrn, int dtk, int drank, const int* ddims, void* d, int lrank,
                       const int* ldims, const void* l, int rrank, const int* rdims, const void* r,
                       double ar, double ai, int accumulative, int nthreads) {
@@ -685,9 +689,13 @@ int orc_contract_blas(const int* cptrn, int dtk, int drank, const int* ddims, vo
   for (int i = 0; i < ncd; ++i) K *= rt[i];
   for (int i = ncd; i < lrank; ++i) M *= lt[i];
   for (int i = ncd; i < rrank; ++i) N *= rt[i];
-  std::vector<char> Lt(M * K * es), Rt(K * N * es), Ct(M * N * es);
-  orc_permute(dtk, lrank, ldims, lprm + 1, l, Lt.data(), 0, nthreads);
-  orc_permute(dtk, rrank, rdims, rprm + 1, r, Rt.data(), 0, nthreads);
+  // temporaries are not initialised (like the reference's allocate); the
+  // permutations are the cache-blocked OpenMP transposes of
+  // tensor_block_copy_dlf_r8 (tensor_algebra_cpu.F90:7764-7834)
+  std::unique_ptr<char[]> Ltb(new char[M * K * es]), Rtb(new char[K * N * es]), Ctb(new char[M * N * es]);
+  char *Lt = Ltb.get(), *Rt = Rtb.get(), *Ct = Ctb.get();
+  orc_permute_blocked(dtk, lrank, ldims, lprm + 1, l, Lt, nthreads);
+  orc_permute_blocked(dtk, rrank, rdims, rprm + 1, r, Rt, nthreads);
   // C dims are (L-uncontracted, R-uncontracted); C dim j maps to D dim dprm[j].
   std::vector<int> cdims(drank), c2d(drank);
   for (int j = 0; j < drank; ++j) { cdims[j] = ddims[dprm[j + 1] - 1]; c2d[j] = dprm[j + 1]; }
@@ -697,23 +705,21 @@ int orc_contract_blas(const int* cptrn, int dtk, int drank, const int* ddims, vo
     if (dtr) {
       std::vector<int> d2c(drank);
       for (int j = 0; j < drank; ++j) d2c[c2d[j] - 1] = j + 1;
-      orc_permute(dtk, drank, ddims, d2c.data(), d, Ct.data(), 0, nthreads);
+      orc_permute_blocked(dtk, drank, ddims, d2c.data(), d, Ct, nthreads);
     } else {
-      std::memcpy(Ct.data(), d, M * N * es);
+      std::memcpy(Ct, d, M * N * es);
     }
   }
   int m = (int)M, n = (int)N, k = (int)K;
   if (dtk == R8) {
     double a = cmplx8_to_real8(ar, ai), b = accumulative ? 1.0 : 0.0;
-    g_dgemm("T", "N", &m, &n, &k, &a, (const double*)Lt.data(), &k, (const double*)Rt.data(), &k, &b,
-            (double*)Ct.data(), &m, 1, 1);
+    g_dgemm("T", "N", &m, &n, &k, &a, (const double*)Lt, &k, (const double*)Rt, &k, &b, (double*)Ct, &m, 1, 1);
   } else {
     float a = (float)cmplx8_to_real8(ar, ai), b = accumulative ? 1.0f : 0.0f;
-    g_sgemm("T", "N", &m, &n, &k, &a, (const float*)Lt.data(), &k, (const float*)Rt.data(), &k, &b,
-            (float*)Ct.data(), &m, 1, 1);
+    g_sgemm("T", "N", &m, &n, &k, &a, (const float*)Lt, &k, (const float*)Rt, &k, &b, (float*)Ct, &m, 1, 1);
   }
-  if (dtr) orc_permute(dtk, drank, cdims.data(), c2d.data(), Ct.data(), d, 0, nthreads);
-  else std::memcpy(d, Ct.data(), M * N * es);
+  if (dtr) orc_permute_blocked(dtk, drank, cdims.data(), c2d.data(), Ct, d, nthreads);
+  else std::memcpy(d, Ct, M * N * es);
   return 0;
 }
 
@@ -758,5 +764,52 @@ int orc_permute_blocked(int dtk, int rank, const int* dims, const int* o2n, cons
 }
 
 int orc_elem_size(int dtk) { return elem_size(dtk); }
+
+// Seeded U[lo,hi) doubles in parallel: the splitmix64 stream of
+// splitmix64_uniform (oracle/__init__.py) and tb_fill_uniform, value i from
+// state seed + (i+1) * golden gamma, 53-bit fraction; same bits.
+void orc_fill_uniform(int64_t n, uint64_t seed, double lo, double hi, double* out, int nthreads) {
+  if (nthreads <= 0) nthreads = 1;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t z = seed + (uint64_t)(i + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    out[i] = lo + (hi - lo) * u;
+  }
+}
+
+// Batched FP64 error oracle: out[i] = sum_k l[i*K + k] * r[i*K + k] with
+// double-double accumulation, rounded once (R8: doubles; C8: complex
+// products of interleaved pairs).  Used to check sampled elements of large
+// contractions, one K-long dot product per sampled D element.
+int orc_dd_dot_batch(int dtk, int64_t n, int64_t K, const void* l, const void* r, void* out, int nthreads) {
+  if (dtk != R8 && dtk != C8) return 6;
+  if (nthreads <= 0) nthreads = 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+  for (int64_t i = 0; i < n; ++i) {
+    if (dtk == R8) {
+      const double* x = (const double*)l + i * K;
+      const double* y = (const double*)r + i * K;
+      dd acc{0.0, 0.0};
+      for (int64_t k = 0; k < K; ++k) acc = dd_add(acc, two_prod(x[k], y[k]));
+      ((double*)out)[i] = acc.hi + acc.lo;
+    } else {
+      const double* x = (const double*)l + 2 * i * K;
+      const double* y = (const double*)r + 2 * i * K;
+      dd sr{0, 0}, si{0, 0};
+      for (int64_t k = 0; k < K; ++k) {
+        const double xr = x[2 * k], xi = x[2 * k + 1], yr = y[2 * k], yi = y[2 * k + 1];
+        sr = dd_add(sr, two_prod(xr, yr)); sr = dd_add(sr, two_prod(-xi, yi));
+        si = dd_add(si, two_prod(xr, yi)); si = dd_add(si, two_prod(xi, yr));
+      }
+      ((double*)out)[2 * i] = sr.hi + sr.lo;
+      ((double*)out)[2 * i + 1] = si.hi + si.lo;
+    }
+  }
+  return 0;
+}
 
 }  // extern "C"

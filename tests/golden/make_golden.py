@@ -13,7 +13,7 @@
   :962-963: a pattern line, then "rank dims... rank dims... rank dims...").
   This part reads the reference tree and is run only where it is mounted.
 
-Usage: python tests/golden/make_golden.py [--reference-root DIR]
+Usage: python tests/golden/make_golden.py [--reference-root DIR]   (or TALSH_REFERENCE_ROOT=DIR)
 """
 import argparse
 import json
@@ -139,12 +139,14 @@ def parse_ctm(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--reference-root", default=os.environ.get("TALSH_REFERENCE_ROOT"),
+                    help="root of the ExaTENSOR source tree (or set TALSH_REFERENCE_ROOT); "
+                         "without it only kats.json is written")
     args = ap.parse_args()
     with open(os.path.join(HERE, "kats.json"), "w") as f:
         json.dump(KATS, f, indent=1)
-    ctm = os.path.join(args.reference_root, "TALSH", "tensor_contractions.txt")
-    if os.path.exists(ctm):
+    ctm = os.path.join(args.reference_root, "TALSH", "tensor_contractions.txt") if args.reference_root else None
+    if ctm and os.path.exists(ctm):
         with open(os.path.join(HERE, "ctm_patterns.json"), "w") as f:
             json.dump({"source": "TALSH/tensor_contractions.txt", "entries": parse_ctm(ctm)}, f, indent=1)
     print("wrote fixtures to", HERE)

@@ -57,7 +57,7 @@ def _ref_main(rank, world, port, out):
 
     import bench
     calls = []
-    bench.cpu_contraction_sample = lambda steps=1: calls.append(steps) or None  # no CPU work in this test
+    bench.cpu_contraction_sample = lambda steps=1, **kw: calls.append(steps) or None  # no CPU work in this test
     bench.run_reference(argparse.Namespace(gpus=world, steps=1, warmup=0, workload="ccsd1_r8"))
     out[rank] = len(calls)
 
