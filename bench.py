@@ -284,7 +284,8 @@ def sig(x, n=4):
     return round(x, -int(floor(log10(abs(x)))) + (n - 1))
 
 
-def ccsd_case(X, s, s_obj, name, steps, warmup, nsamp, psteps=None, world=1, on_timed=None, after_timed=None):
+def ccsd_case(X, s, s_obj, name, steps, warmup, nsamp, psteps=None, world=1, on_timed=None, after_timed=None,
+              on_warmup=None):
     """Chosen (METHOD_AUTO: the plan selector) against plain TTGT for one
     CCSD-like workload: device-timed TFLOP/s of both, the chosen D compared with
     the plain D over the WHOLE output tensor, and (R8/C8) both against the
@@ -296,6 +297,8 @@ def ccsd_case(X, s, s_obj, name, steps, warmup, nsamp, psteps=None, world=1, on_
     case = ContractionCase(X, wl, s)
     case.run(X.METHOD_AUTO)  # first call of a shape: the selector may time close candidates
     torch.cuda.synchronize()
+    if on_warmup:
+        on_warmup()  # e.g. the clock sampler, started early so that it is running in the timed region
     X.timing_enable(True)  # CUDA events around the GEMM launches, read after each timed region
 
     def hook():
@@ -453,7 +456,7 @@ def torch_permuted(t, dims, perm, word):
     return x.view(-1)
 
 
-def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True):
+def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True, per_case=False):
     """Every sweep case: 10 back-to-back timed copies after the first call (where
     the library's measured plan choice runs), and a bit-for-bit comparison of
     the result with torch's permute of the same device data.  Per class the
@@ -499,13 +502,15 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True):
            "rank4_48": {"GB/s": round(sum(g for g, _ in r4) / sum(g / r for g, r in r4), 1),
                         "min": round(min(r for _, r in r4), 1)},
            "by_class_agg_min": {k: [round(v[0] / v[1]), round(v[2])] for k, v in stats.items()}}
+    if per_case:
+        out["per_case"] = [[c["cls"], c["dims"], list(c["perm"]), round(r)] for c, r in zip(cases, rates)]
     if with_add:
-        out["add"] = add_sweep(X, stream, stream_obj, hbm_gbs)
+        out["add"] = add_sweep(X, stream, stream_obj, hbm_gbs, per_case=per_case)
     out["timing"] = "10 back-to-back calls per case after the first; bits checked against torch.permute"
     return out
 
 
-def add_sweep(X, stream, stream_obj, hbm_gbs, scale=0.37):
+def add_sweep(X, stream, stream_obj, hbm_gbs, scale=0.37, per_case=False):
     """D += scale * permute(L) over add_cases(): 3 * vol * elem bytes per call;
     one call per case from a fresh D compared bit for bit with torch's
     d + permute(l) * scale (two roundings), then 10 back-to-back timed calls."""
@@ -540,8 +545,11 @@ def add_sweep(X, stream, stream_obj, hbm_gbs, scale=0.37):
         tot_s += ms / 1e3
     l = d0 = d = None
     agg = tot_b / tot_s
-    return {"GB/s": round(agg, 1), "min_GB/s": round(min(rates), 1), "frac_measured_hbm": sig(agg / hbm_gbs, 3),
-            "cases": len(cases), "bit_exact": len(cases) - mism}
+    out = {"GB/s": round(agg, 1), "min_GB/s": round(min(rates), 1), "frac_measured_hbm": sig(agg / hbm_gbs, 3),
+           "cases": len(cases), "bit_exact": len(cases) - mism}
+    if per_case:
+        out["per_case"] = [[c["cls"], c["dims"], list(c["perm"]), round(r)] for c, r in zip(cases, rates)]
+    return out
 
 
 def permute_sweep_repeated(X, stream, stream_obj, reps=3):
@@ -903,14 +911,13 @@ def run_ours(args):
 
     def start():
         cnt["n0"] = X.launch_count()
-        clocks.start()
 
     def stop():
         cnt["clk"] = clocks.stop()
         cnt["launches"] = X.launch_count() - cnt["n0"]
     rec, case, (ms, pms, st, gemm, pgemm) = ccsd_case(
         X, s, s_obj, args.workload, args.steps, args.warmup, nsamp=4096 if rank == 0 else 0,
-        psteps=max(1, args.steps // 2), world=world, on_timed=start, after_timed=stop)
+        psteps=max(1, args.steps // 2), world=world, on_timed=start, after_timed=stop, on_warmup=clocks.start)
     ms_max = max_over_ranks(ms, world)
     pms_max = max_over_ranks(pms, world)
     value = world * case.flops / (ms_max / 1e3) / 1e12
@@ -1024,7 +1031,7 @@ def run_profile(args):
             torch.cuda.empty_cache()
         return
     if args.profile == "sweep":
-        print(json.dumps({"profile": "sweep", **permute_sweep(X, s, s_obj, peaks()[0])}))
+        print(json.dumps({"profile": "sweep", **permute_sweep(X, s, s_obj, peaks()[0], per_case=True)}))
         return
     if args.profile == "peaks":
         print(json.dumps({"profile": "peaks", **measure_peaks(X, s)}))

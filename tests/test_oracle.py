@@ -237,3 +237,19 @@ def test_blas_baseline_matches_oracle():
     O.contract(cptrn, a, [n] * 4, L, [n] * 4, R, [n] * 4, alpha=0.5, mode=1)
     O.contract_blas(cptrn, b, [n] * 4, L, [n] * 4, R, [n] * 4, alpha=0.5)
     assert O.rel_frobenius(b, a) < 1e-14
+
+
+def test_reference_nvtal_library_loads():
+    """The reference's own NV-TAL kernels (oracle/_ref, built from the
+    reference's sources by `make -C oracle ref`) load on the CPU and export the
+    harness's entry points; the GPU parity test calls them."""
+    import ctypes
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                        "libnvtal_ref.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref/libnvtal_ref.so not built (needs the reference sources)")
+    lib = ctypes.CDLL(path)
+    for name in ("ref_init", "ref_copy", "ref_add", "ref_contract", "gpu_tensor_block_copy",
+                 "gpu_tensor_block_add", "gpu_tensor_block_contract_dlf", "get_contr_permutations"):
+        assert hasattr(lib, name), name
