@@ -33,11 +33,17 @@ double real_alpha(double re, double im) {
   return im;
 }
 
-// Store functors for the final C -> D permutation of the TTGT path.
+// Store functors for the final C -> D permutation of the TTGT path.  Those
+// that read D expose load / put (kRMW), so that the permutation kernels issue
+// a batch of D loads before the dependent writes.
 template <typename R>
 struct StoreAxpy {  // d = d + v*a
   R* out; R a;
-  __device__ __forceinline__ void operator()(int64_t o, const R& v) const { out[o] = out[o] + v * a; }
+  static constexpr bool kRMW = true;
+  using Old = R;
+  __device__ __forceinline__ R load(int64_t o) const { return out[o]; }
+  __device__ __forceinline__ void put(int64_t o, const R& v, const R& old) const { out[o] = old + v * a; }
+  __device__ __forceinline__ void operator()(int64_t o, const R& v) const { put(o, v, out[o]); }
 };
 template <typename R>
 struct StoreScaled {  // d = v*a
@@ -47,17 +53,24 @@ struct StoreScaled {  // d = v*a
 template <typename C2, typename R>
 struct StoreAxpyC {  // d = beta*d + alpha*v (complex)
   C2* out; R ar, ai, br, bi;
-  __device__ __forceinline__ void operator()(int64_t o, const C2& v) const {
+  static constexpr bool kRMW = true;
+  using Old = C2;
+  __device__ __forceinline__ C2 load(int64_t o) const {
+    if (br != R(0) || bi != R(0)) return out[o];
+    C2 z; z.x = R(0); z.y = R(0);
+    return z;
+  }
+  __device__ __forceinline__ void put(int64_t o, const C2& v, const C2& d) const {
     C2 r;
     r.x = ar * v.x - ai * v.y;
     r.y = ar * v.y + ai * v.x;
     if (br != R(0) || bi != R(0)) {
-      const C2 d = out[o];
       r.x += br * d.x - bi * d.y;
       r.y += br * d.y + bi * d.x;
     }
     out[o] = r;
   }
+  __device__ __forceinline__ void operator()(int64_t o, const C2& v) const { put(o, v, load(o)); }
 };
 
 // ---- full contraction (dot product) ----------------------------------------

@@ -11,7 +11,7 @@
 namespace tb {
 
 int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin_in,
-                    const int64_t* sout_in, PermParams* pp, int vmin_kb, int vmax_kb) {
+                    const int64_t* sout_in, PermParams* pp, int vmin_kb, int vmax_kb, int min_run) {
   PermParams& P = *pp;
   std::memset(&P, 0, sizeof(P));
   P.es = es;
@@ -34,7 +34,14 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
   for (int i = 0; i < r; ++i) Q[i] = i;
   std::stable_sort(Q.begin(), Q.end(), [&](int x, int y) { return SO[x] < SO[y]; });
   if (SO[Q[0]] != 1) return TB_ERR_NOT_IMPLEMENTED;
-  const int64_t T = std::max<int64_t>(1, 256 / es);  // minimum contiguous run of the load and store blocks
+  // minimum contiguous run of the load and store blocks (elements): 256 bytes
+  // unless the caller (or TB_PERM_MINRUN, a tuning knob) asks for another
+  static const int64_t run_env = [] {
+    const char* e = std::getenv("TB_PERM_MINRUN");
+    const long v = e ? std::atol(e) : 0;
+    return (int64_t)(v >= 32 && v <= 4096 ? v : 256);
+  }();
+  const int64_t T = std::max<int64_t>(1, (min_run > 0 ? min_run : run_env) / es);
   // tile volume bounds (bytes; 16 KB .. 32 KB unless TB_PERM_VMIN_KB /
   // TB_PERM_VMAX_KB say otherwise -- tuning knobs that leave results unchanged)
   auto knob = [](const char* name, long dflt) {
@@ -343,7 +350,7 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
 }
 
 int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p, int vmin_kb,
-                        int vmax_kb) {
+                        int vmax_kb, int min_run) {
   if (rank < 0 || rank > kPlanMaxRank) return TB_ERR_INVALID_ARGS;
   int64_t D[kPlanMaxRank], SI[kPlanMaxRank], SO[kPlanMaxRank], pos[kPlanMaxRank + 1];
   int seen[kPlanMaxRank + 1] = {0};
@@ -359,7 +366,26 @@ int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, Per
   s = 1;
   for (int q = 0; q < rank; ++q) { pos[q] = s; s *= oe[q]; }
   for (int i = 0; i < rank; ++i) SO[i] = pos[cptrn[i] - 1];
-  return build_perm_plan(es, rank, D, SI, SO, p, vmin_kb, vmax_kb);
+  return build_perm_plan(es, rank, D, SI, SO, p, vmin_kb, vmax_kb, min_run);
+}
+
+int perm_glist_vector_bytes(const PermParams& P, int in_align, int nthr) {
+  const int es = P.es;
+  int vb = es;
+  if (P.tma_ok && es < 16 && in_align % 16 == 0) vb = 16;
+  else if (P.vec8 && es < 8 && in_align % 8 == 0) vb = 8;
+  if (((int64_t)P.LA * es) % vb != 0) vb = es;
+  const int64_t nld = (int64_t)P.nA * ((int64_t)P.LA * es / vb);
+  const int64_t cap = (int64_t)kGListEntries * nthr;
+  if (P.V > cap || nld > cap) return 0;
+  int64_t maxl = 0, maxs = 0;
+  for (int c = 0; c < P.nA; ++c) maxl = std::max<int64_t>(maxl, P.ld_base[c]);
+  for (int c = 0; c < P.nB; ++c) maxs = std::max<int64_t>(maxs, P.st_base[c]);
+  const int64_t lim = (int64_t)1 << 31;
+  if (maxl + P.LA >= lim || maxs + P.LB >= lim) return 0;
+  for (int c = 0; c < P.nA; ++c) if (P.ld_base[c] < 0) return 0;
+  for (int c = 0; c < P.nB; ++c) if (P.st_base[c] < 0) return 0;
+  return vb;
 }
 
 int perm2d_list_entries(const PermParams& P, bool rows, int nthr) {

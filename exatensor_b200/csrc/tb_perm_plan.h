@@ -94,17 +94,26 @@ TB_HD void perm_list_entry(int lin, int nq, uint32_t Aq, uint32_t Ap, int32_t Bq
 // Host-side plan builder.  dims/sin/sout describe the input dims (input
 // strides, output strides), first dim fastest in the input.  Returns 0 or a
 // TB_ERR code.  Dims of extent 1 are dropped and mergeable neighbours fused.
-// vmin_kb / vmax_kb bound the tile's bytes (0: the defaults, 16 and 32 KB).
+// vmin_kb / vmax_kb bound the tile's bytes (0: the defaults, 16 and 32 KB);
+// min_run is the minimum contiguous run of the load and store blocks in bytes
+// (0: the default, 256).
 int build_perm_plan(int es, int rank, const int64_t* dims, const int64_t* sin, const int64_t* sout,
-                    PermParams* p, int vmin_kb = 0, int vmax_kb = 0);
+                    PermParams* p, int vmin_kb = 0, int vmax_kb = 0, int min_run = 0);
 // Convenience: plain O2N permutation of a dense tensor (cptrn 1-based).
 int build_perm_plan_o2n(int es, int rank, const int* dims, const int* cptrn, PermParams* p, int vmin_kb = 0,
-                        int vmax_kb = 0);
+                        int vmax_kb = 0, int min_run = 0);
 // Entries per thread of the 2-D kernel's full-tile offset lists for a plan
 // whose vector path is rows (row copies) or column groups (transposes): 8 or
 // 16, or 0 when the lists would not cover a tile, an offset would not fit in
 // 32 bits, or the last column group is ragged (the general code runs then).
 int perm2d_list_entries(const PermParams& P, bool rows, int nthr);
+// General-plan list kernel (perm_glist_kernel): entries per thread of its
+// load and store lists, and the bytes of its load copies for a plan and an
+// input pointer aligned to in_align bytes -- 16, 8 or one element -- or 0 when
+// the plan does not fit the lists (more than kGListEntries * nthr elements or
+// load copies per tile, or tile-relative offsets beyond 32 bits).
+constexpr int kGListEntries = 16;
+int perm_glist_vector_bytes(const PermParams& P, int in_align, int nthr);
 // Bytes of one pipeline stage (a tile in shared memory).
 inline int64_t perm_stage_bytes(const PermParams& P) { return (int64_t)P.nA * P.lap * P.es; }
 

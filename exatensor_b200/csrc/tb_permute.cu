@@ -79,38 +79,53 @@ int run_scatter(int rank, const int* dims, const int* cptrn, const E* in, const 
 
 // Fused permute + add: d = d + v*a with two roundings (no FMA), complex
 // products by the textbook formula, the left operand optionally conjugated.
+// Each functor reads the output it updates: load(o) and put(o, v, old) let the
+// list kernels issue a batch of output loads before the dependent writes.
 template <typename R>
 struct AddScalar {
   R* out; R a;
-  __device__ __forceinline__ void operator()(int64_t o, const R& v) const;
+  static constexpr bool kRMW = true;
+  using Old = R;
+  __device__ __forceinline__ R load(int64_t o) const { return out[o]; }
+  __device__ __forceinline__ void put(int64_t o, const R& v, const R& old) const;
+  __device__ __forceinline__ void operator()(int64_t o, const R& v) const { put(o, v, out[o]); }
 };
-template <> __device__ __forceinline__ void AddScalar<float>::operator()(int64_t o, const float& v) const {
-  out[o] = __fadd_rn(out[o], __fmul_rn(v, a));
+template <> __device__ __forceinline__ void AddScalar<float>::put(int64_t o, const float& v, const float& old) const {
+  out[o] = __fadd_rn(old, __fmul_rn(v, a));
 }
-template <> __device__ __forceinline__ void AddScalar<double>::operator()(int64_t o, const double& v) const {
-  out[o] = __dadd_rn(out[o], __dmul_rn(v, a));
+template <> __device__ __forceinline__ void AddScalar<double>::put(int64_t o, const double& v,
+                                                                   const double& old) const {
+  out[o] = __dadd_rn(old, __dmul_rn(v, a));
 }
 struct AddC4 {
   float2* out; float ar, ai; bool conj;
-  __device__ __forceinline__ void operator()(int64_t o, const float2& v) const {
+  static constexpr bool kRMW = true;
+  using Old = float2;
+  __device__ __forceinline__ float2 load(int64_t o) const { return out[o]; }
+  __device__ __forceinline__ void put(int64_t o, const float2& v, const float2& old) const {
     const float vr = v.x, vi = conj ? -v.y : v.y;
     const float tr = __fsub_rn(__fmul_rn(vr, ar), __fmul_rn(vi, ai));
     const float ti = __fadd_rn(__fmul_rn(vr, ai), __fmul_rn(vi, ar));
-    float2 d = out[o];
+    float2 d = old;
     d.x = __fadd_rn(d.x, tr); d.y = __fadd_rn(d.y, ti);
     out[o] = d;
   }
+  __device__ __forceinline__ void operator()(int64_t o, const float2& v) const { put(o, v, out[o]); }
 };
 struct AddC8 {
   double2* out; double ar, ai; bool conj;
-  __device__ __forceinline__ void operator()(int64_t o, const double2& v) const {
+  static constexpr bool kRMW = true;
+  using Old = double2;
+  __device__ __forceinline__ double2 load(int64_t o) const { return out[o]; }
+  __device__ __forceinline__ void put(int64_t o, const double2& v, const double2& old) const {
     const double vr = v.x, vi = conj ? -v.y : v.y;
     const double tr = __dsub_rn(__dmul_rn(vr, ar), __dmul_rn(vi, ai));
     const double ti = __dadd_rn(__dmul_rn(vr, ai), __dmul_rn(vi, ar));
-    double2 d = out[o];
+    double2 d = old;
     d.x = __dadd_rn(d.x, tr); d.y = __dadd_rn(d.y, ti);
     out[o] = d;
   }
+  __device__ __forceinline__ void operator()(int64_t o, const double2& v) const { put(o, v, out[o]); }
 };
 
 double cmplx8_to_real8(double re, double im) {
@@ -137,9 +152,14 @@ double real_scale_factor(double re, double im) { return cmplx8_to_real8(re, im);
 // into a graph (the default plan runs then), and TB_PERM_TUNE=0 turns it
 // off.  Only copies are timed: their output may be written several times,
 // unlike an accumulation's.
-struct TileBounds { int vmin_kb, vmax_kb; };
-constexpr TileBounds kTileCandidates[] = {{0, 0}, {8, 24}, {24, 48}};
-constexpr int kNumTileCandidates = 3;
+// {8, 16} and {4, 16} with 128-byte minimum runs: small tiles, which general
+// plans (several dimensions in a load or store block) run on the list
+// kernel's registers (at most 4096 elements); with 256-byte runs a 4-byte
+// tile that crosses two multi-dimension blocks cannot be that small.
+struct TileBounds { int vmin_kb, vmax_kb, min_run; };
+constexpr TileBounds kTileCandidates[] = {{0, 0, 0}, {8, 24, 0}, {24, 48, 0}, {8, 16, 0}, {4, 16, 128}};
+constexpr int kNumTileCandidates = 5;
+constexpr int kListCand = 3, kListCandShort = 4;
 constexpr int64_t kTuneMinBytes = (int64_t)32 << 20;
 // A further candidate for long row copies: the default plan in the bulk-copy
 // kernel (measured faster for 4-byte elements, slower for 8-byte ones).
@@ -187,7 +207,7 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
     const int c = pick < 0 ? 0 : pick;
     const TileBounds b = kTileCandidates[c == kBulkRowsCand ? 0 : c];
     PermParams P;
-    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb);
+    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb, b.min_run);
     if (e == 0) {
       if (c == kBulkRowsCand && long_row_copy(P)) P.bulk_rows = 1;
       return launch_perm<E, Store>(P, in, st, s);
@@ -200,7 +220,7 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
   int n = 0, idx[kNumPlanCandidates];
   for (int c = 0; c < kNumTileCandidates; ++c) {
     int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &plans[n], kTileCandidates[c].vmin_kb,
-                                kTileCandidates[c].vmax_kb);
+                                kTileCandidates[c].vmax_kb, kTileCandidates[c].min_run);
     if (e == TB_ERR_NOT_IMPLEMENTED && c == 0) {
       remember_choice(key, 0);
       return run_scatter<E, Store>(rank, dims, cptrn, in, st, s);
@@ -245,12 +265,37 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
 
 // Runs a permutation with the tiled engine, or the scatter kernel when the
 // plan builder declines the layout.
+// Runs a permutation with the tiled engine, or the scatter kernel when the
+// plan builder declines the layout.  Used where output must be written once
+// (the fused add), so nothing is timed: the plan is the one the measured
+// choice keeps for copies of the same shape and element size when there is
+// one, else the default plan -- or, for a general plan (several dimensions in
+// a load or store block) whose default tile is too large for the list
+// kernel's registers, the smaller tile of the {8, 16} KB candidate.
 template <typename E, typename Store>
 int run_permutation(int rank, const int* dims, const int* cptrn, const E* in, const Store& st,
                     cudaStream_t s, bool force_scatter = false) {
   if (!force_scatter) {
+    std::vector<int> key{(int)sizeof(E), rank};
+    key.insert(key.end(), dims, dims + rank);
+    key.insert(key.end(), cptrn, cptrn + rank);
+    int pick = -1;
+    {
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      auto it = g_tune.find(key);
+      if (it != g_tune.end()) pick = it->second;
+    }
+    const TileBounds b = kTileCandidates[(pick < 0 || pick == kBulkRowsCand) ? 0 : pick];
     PermParams P;
-    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P);
+    int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb, b.min_run);
+    for (int c : {kListCand, kListCandShort}) {
+      if (e != 0 || pick >= 0 || P.lin2d || glist_vector_bytes(P, in)) break;
+      PermParams Q;
+      const TileBounds q = kTileCandidates[c];
+      if (build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &Q, q.vmin_kb, q.vmax_kb, q.min_run) == 0 &&
+          glist_vector_bytes(Q, in))
+        P = Q;
+    }
     if (e == 0) return launch_perm<E, Store>(P, in, st, s);
     if (e != TB_ERR_NOT_IMPLEMENTED) return e;
   }

@@ -81,7 +81,7 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)
 // Loads one tile into a stage buffer (see the BULK / !BULK note above).
 // !BULK: each warp copies whole rows (lanes along the row, 16-byte copies
 // when rows are 16-byte aligned, element copies otherwise).
-template <typename Elem, bool BULK>
+template <typename Elem, bool BULK, bool COMMIT = true>
 __device__ __forceinline__ void perm_issue(const PermParams& P, const PermSmem& T, const Elem* in, Elem* stage,
                                            unsigned long long* bar, int64_t tile) {
   const TileOrigin o = tile_origin(P, tile);
@@ -109,8 +109,9 @@ __device__ __forceinline__ void perm_issue(const PermParams& P, const PermSmem& 
   } else {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kW = kPermThreads / 32, kU = 4;  // copies per lane per unit
-    const bool vec = P.tma_ok && sizeof(Elem) < 16;
-    const bool vec8 = !vec && P.vec8 && sizeof(Elem) < 8;
+    // vector copies need rows that are whole vectors (the plan) on an aligned tensor
+    const bool vec = P.tma_ok && sizeof(Elem) < 16 && (uintptr_t)in % 16 == 0;
+    const bool vec8 = !vec && P.vec8 && sizeof(Elem) < 8 && (uintptr_t)in % 8 == 0;
     constexpr int VW = sizeof(Elem) < 16 ? 16 / sizeof(Elem) : 1;
     constexpr int VW8 = sizeof(Elem) < 8 ? 8 / sizeof(Elem) : 1;
     const int w = vec ? VW : (vec8 ? VW8 : 1);         // elements per copy
@@ -139,7 +140,7 @@ __device__ __forceinline__ void perm_issue(const PermParams& P, const PermSmem& 
                        : "memory");
       }
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    if (COMMIT) asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
 }
 
@@ -288,8 +289,9 @@ __device__ __forceinline__ void perm2d_issue(const PermParams& P, const Elem* in
   if (!o.full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb) rows = min(rows, o.rem_b);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int kW = kPermThreads / 32;
-  const bool vec = P.tma_ok && sizeof(Elem) < 16;
-  const bool vec8 = !vec && P.vec8 && sizeof(Elem) < 8;
+  // vector copies need rows that are whole vectors (the plan) on an aligned tensor
+  const bool vec = P.tma_ok && sizeof(Elem) < 16 && (uintptr_t)in % 16 == 0;
+  const bool vec8 = !vec && P.vec8 && sizeof(Elem) < 8 && (uintptr_t)in % 8 == 0;
   constexpr int VW = sizeof(Elem) < 16 ? 16 / sizeof(Elem) : 1;
   constexpr int VW8 = sizeof(Elem) < 8 ? 8 / sizeof(Elem) : 1;
   const int w = vec ? VW : (vec8 ? VW8 : 1);
@@ -398,6 +400,19 @@ struct has_vec_store : std::false_type {};
 template <class S>
 struct has_vec_store<S, std::void_t<decltype(S::kVecStore)>> : std::true_type {};
 
+// Store functors that read the output they update (the fused add): they
+// expose load(o) -> Old and put(o, v, old), so that the list kernels can
+// issue a batch of output loads before any of the writes that depend on them
+// (one element at a time, each load's latency would serialise the stores).
+template <class S, class = void>
+struct is_rmw_store : std::false_type {};
+template <class S>
+struct is_rmw_store<S, std::void_t<decltype(S::kRMW)>> : std::true_type {};
+template <class S, class E, bool = is_rmw_store<S>::value>
+struct rmw_old { using type = E; };
+template <class S, class E>
+struct rmw_old<S, E, true> { using type = typename S::Old; };
+
 constexpr int kHdrRing = kStages + 1;  // tile headers: issued, in flight, stored, being written
 
 // VB: vector bytes of the vector paths (0: scalar general code only).
@@ -461,7 +476,44 @@ perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in,
   auto store = [&](int k) {
     const TileOrigin o = org[k % kHdrRing];
     const Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
-    if (lists && o.full) {
+    bool done = false;
+    if constexpr (is_rmw_store<Store>::value) {
+     if (lists && o.full) {
+      // read-modify-write stores in batches of kRmwBatch list entries: the
+      // output loads of a batch are all issued before its writes
+      done = true;
+      Store s2 = st;
+      s2.out += o.out_base;
+      const unsigned char* sb = reinterpret_cast<const unsigned char*>(stage);
+      const int32_t cs = ROWS ? 1 : (int32_t)P.chunk_sout;
+      constexpr int kRmwBatch = 4;
+      using Old = typename rmw_old<Store, Elem>::type;
+#pragma unroll
+      for (int i0 = 0; i0 < NL; i0 += kRmwBatch) {
+        Old old[kRmwBatch][VW];
+#pragma unroll
+        for (int g = 0; g < kRmwBatch; ++g) {
+          const int i = i0 + g;
+          if (i < NL && i < stl.n) {
+#pragma unroll
+            for (int t = 0; t < VW; ++t) old[g][t] = s2.load(stl.b[i] + t * cs);
+          }
+        }
+#pragma unroll
+        for (int g = 0; g < kRmwBatch; ++g) {
+          const int i = i0 + g;
+          if (i < NL && i < stl.n) {
+            union { V q; Elem v[VW]; } u;
+            u.q = *reinterpret_cast<const V*>(sb + stl.a[i]);
+#pragma unroll
+            for (int t = 0; t < VW; ++t) s2.put(stl.b[i] + t * cs, u.v[t], old[g][t]);
+          }
+        }
+      }
+     }
+    }
+    if (done) {
+    } else if (lists && o.full) {
       Store s2 = st;
       s2.out += o.out_base;
       const unsigned char* sb = reinterpret_cast<const unsigned char*>(stage);
@@ -509,6 +561,155 @@ perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in,
     store(k);
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// General plans on per-thread offset lists (perm_glist_kernel).  A plan of
+// any shape -- several dimensions in the load or the store block, chunk
+// tables -- moves every full tile with the same tile-relative offsets, so each
+// thread computes its copies once, from the plan's tables: up to kGListN
+// vector loads (VB bytes of a load row: 16, 8 or one element) and up to
+// kGListN element stores, kept in registers.  Full tiles then run as unrolled
+// base-plus-offset copies: a cp.async per load entry, a shared-memory read
+// and a global store per store entry.  Store functors that read the output
+// (the fused add) load a whole tile's worth of a thread's outputs before
+// writing any.  Tiles at the tensor's edges (partial tiles) take the
+// table-driven code of the pipelined kernel.  The host launches this kernel
+// only for plans whose tile has at most kGListN * 256 elements and load
+// vectors, and whose tile-relative offsets fit in 32 bits (glist_ok).
+constexpr int kGListN = kGListEntries;
+
+template <typename Elem, typename Store, int VB>
+__global__ void __launch_bounds__(kPermThreads, 2)
+perm_glist_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st) {
+  constexpr int es = (int)sizeof(Elem);
+  constexpr int VW = VB / es;  // elements per load copy
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PermSmem& T = *reinterpret_cast<PermSmem*>(smem_raw);
+  Elem* bufs = reinterpret_cast<Elem*>(smem_raw + ((sizeof(PermSmem) + 127) & ~size_t(127)));
+  __shared__ TileOrigin org[kHdrRing];
+  const size_t stage_elems = (size_t)P.nA * P.lap;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < P.nA; i += kPermThreads) { T.ld_base[i] = P.ld_base[i]; T.ld_dpb[i] = P.ld_dpb[i]; }
+  for (int i = tid; i < P.nB; i += kPermThreads) {
+    T.st_base[i] = P.st_base[i]; T.st_ebase[i] = P.st_ebase[i]; T.st_dpa[i] = P.st_dpa[i];
+  }
+  for (int i = tid; i < P.ejf_n; i += kPermThreads) T.ejf[i] = P.ejf[i];
+  const int64_t first = blockIdx.x, step = gridDim.x;
+  const int mine = first < P.ntiles ? (int)((P.ntiles - 1 - first) / step + 1) : 0;
+  if (tid == 0)
+    for (int k = 0; k < kStages && k < mine; ++k) org[k] = tile_origin(P, first + k * step);
+  __syncthreads();
+  // this thread's full-tile copies: load vector v = (row c, vector x), store
+  // element e = (store chunk c', position j) with consecutive e along a chunk
+  const int nvec = P.LA / VW;
+  const int nld_all = P.nA * nvec;
+  const int nld = tid < nld_all ? min(kGListN, (nld_all - 1 - tid) / kPermThreads + 1) : 0;
+  const int nst = tid < P.V ? min(kGListN, (P.V - 1 - tid) / kPermThreads + 1) : 0;
+  uint32_t la[kGListN], sa[kGListN];
+  int32_t lb[kGListN], sb[kGListN];
+#pragma unroll
+  for (int i = 0; i < kGListN; ++i) {
+    int v = tid + i * kPermThreads;
+    if (v >= nld_all) v = 0;
+    const int c = v / nvec, x = v - c * nvec;
+    la[i] = (uint32_t)((c * P.lap + x * VW) * es);
+    lb[i] = (int32_t)(T.ld_base[c] + x * VW);
+    int e = tid + i * kPermThreads;
+    if (e >= P.V) e = 0;
+    const int cc = e / P.LB, j = e - cc * P.LB;
+    const int q = j / P.prodB;
+    sa[i] = (uint32_t)((T.st_ebase[cc] + T.ejf[j - q * P.prodB] + q * P.ej_pb_stride) * es);
+    sb[i] = (int32_t)(T.st_base[cc] + j);
+  }
+  StoreLanes SL;
+  store_lanes_init(P, SL);
+
+  auto issue = [&](int k) {
+    const TileOrigin o = org[k % kHdrRing];
+    Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
+    if (o.full) {
+      const Elem* src = in + o.in_base;
+      const uint32_t sbase = smem_addr(stage);
+#pragma unroll
+      for (int i = 0; i < kGListN; ++i) {
+        if (i < nld) {
+          if (VB == 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + la[i]), "l"(src + lb[i])
+                         : "memory");
+          else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sbase + la[i]), "l"(src + lb[i]),
+                         "n"(VB)
+                         : "memory");
+        }
+      }
+    } else {
+      perm_issue<Elem, false, false>(P, T, in, stage, nullptr, first + (int64_t)k * step);
+    }
+  };
+  auto store = [&](int k) {
+    const TileOrigin o = org[k % kHdrRing];
+    const Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
+    if (!o.full) {
+      perm_store<Elem, Store>(P, T, SL, stage, first + (int64_t)k * step, st);
+      return;
+    }
+    Store s2 = st;
+    s2.out += o.out_base;
+    const unsigned char* sbase = reinterpret_cast<const unsigned char*>(stage);
+    if constexpr (is_rmw_store<Store>::value) {
+      constexpr int kBatch = 8;  // output loads in flight per thread before their writes
+#pragma unroll
+      for (int h = 0; h < kGListN; h += kBatch) {
+        typename Store::Old old[kBatch];
+#pragma unroll
+        for (int g = 0; g < kBatch; ++g)
+          if (h + g < nst) old[g] = s2.load(sb[h + g]);
+#pragma unroll
+        for (int g = 0; g < kBatch; ++g)
+          if (h + g < nst) s2.put(sb[h + g], *reinterpret_cast<const Elem*>(sbase + sa[h + g]), old[g]);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < kGListN; ++i)
+        if (i < nst) s2(sb[i], *reinterpret_cast<const Elem*>(sbase + sa[i]));
+    }
+  };
+
+  for (int k = 0; k < kStages - 1; ++k) {
+    if (k < mine) issue(k);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int k = 0; k < mine; ++k) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+    __syncthreads();
+    const int nk = k + kStages - 1;
+    if (nk < mine) issue(nk);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // the header slot of tile k + kStages last held tile k - 1, whose store
+    // finished before the barrier above; it is read after the next barrier
+    if (tid == 0 && k + kStages < mine) org[(k + kStages) % kHdrRing] = tile_origin(P, first + (int64_t)(k + kStages) * step);
+    store(k);
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Load vector bytes of the list kernel for a plan and input pointer, or 0
+// when the plan does not fit its lists.
+template <typename Elem>
+inline int glist_vector_bytes(const PermParams& P, const Elem* in) {
+  const uintptr_t a = (uintptr_t)in;
+  return perm_glist_vector_bytes(P, a % 16 == 0 ? 16 : (a % 8 == 0 ? 8 : (int)sizeof(Elem)), kPermThreads);
+}
+
+template <typename Elem, typename Store, int VB>
+void launch_glist(const PermParams& P, const Elem* in, const Store& st, size_t smem, cudaStream_t s) {
+  static DeviceOnce attr;
+  smem_limit_once(attr, perm_glist_kernel<Elem, Store, VB>, 220 * 1024);
+  int per_sm = (int)((224 * 1024) / (smem + 1024));
+  per_sm = std::max(1, std::min(per_sm, 2));  // launch bound: 2 CTAs of 256 threads per SM (register lists)
+  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)num_sms() * per_sm, P.ntiles);
+  perm_glist_kernel<Elem, Store, VB><<<grid, kPermThreads, smem, s>>>(P, in, st);
 }
 
 // Whether a store functor writes vectors of vbytes to an aligned output
@@ -566,6 +767,9 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
     return 0;
   }();
   const bool eligible = P.tma_ok && ((uintptr_t)in % 16 == 0);
+  // TB_PERM_GLIST=0: general plans through the table-driven kernel (tuning
+  // and diagnostic switch; results are identical)
+  static const bool glist_on = [] { const char* e = getenv("TB_PERM_GLIST"); return !(e && e[0] == '0'); }();
   // long rows move as bulk copies, except row copies (rows2d), whose 2-D
   // kernel stores whole vectors (TB_PERM_LONGROWS=bulk: those too)
   static const bool longrows_bulk = [] { const char* e = getenv("TB_PERM_LONGROWS"); return e && !strcmp(e, "bulk"); }();
@@ -596,9 +800,18 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
       else if (rows) launch_2d<Elem, Store, V8, true>(N, P.ntiles, smem2, s, P, in, st, flags);
       else if (P.vbytes == 16) launch_2d<Elem, Store, 16, false>(N, P.ntiles, smem2, s, P, in, st, flags);
       else launch_2d<Elem, Store, V8, false>(N, P.ntiles, smem2, s, P, in, st, flags);
+    } else if (const int gvb = (mode == 0 && glist_on) ? glist_vector_bytes(P, in) : 0) {
+      if (gvb == 16) launch_glist<Elem, Store, (sizeof(Elem) < 16 ? 16 : sizeof(Elem))>(P, in, st, smem, s);
+      else if (gvb == 8) launch_glist<Elem, Store, (sizeof(Elem) < 8 ? 8 : sizeof(Elem))>(P, in, st, smem, s);
+      else launch_glist<Elem, Store, sizeof(Elem)>(P, in, st, smem, s);
     } else {
       launch_2d<Elem, Store, 0, false>(0, P.ntiles, smem2, s, P, in, st, 0);
     }
+  } else if (!bulk && mode == 0 && glist_on && glist_vector_bytes(P, in)) {
+    const int gvb = glist_vector_bytes(P, in);
+    if (gvb == 16) launch_glist<Elem, Store, (sizeof(Elem) < 16 ? 16 : sizeof(Elem))>(P, in, st, smem, s);
+    else if (gvb == 8) launch_glist<Elem, Store, (sizeof(Elem) < 8 ? 8 : sizeof(Elem))>(P, in, st, smem, s);
+    else launch_glist<Elem, Store, sizeof(Elem)>(P, in, st, smem, s);
   } else if (bulk)
     perm_pipe_kernel<Elem, Store, true><<<(unsigned)grid, kPermThreads, smem, s>>>(P, in, st, device_error_word());
   else

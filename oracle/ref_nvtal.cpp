@@ -2,8 +2,8 @@
 // own NV-TAL device path (ExaTENSOR TALSH/tensor_algebra_gpu_nvidia.cu with
 // TALSH/tensor_algebra_gpu.cpp, mem_manager.cpp and timer.cpp), which
 // oracle/Makefile compiles from the reference's sources, unchanged, into
-// oracle/_ref/libnvtal_ref.so (cuBLAS off: -DNO_BLAS, so contractions run the
-// reference's own gpu_matrix_multiply_tn__ kernel).  The tests call these
+// oracle/_ref/libnvtal_ref.so in the reference's default configuration (its
+// contractions call cuBLAS GEMMs, :6899-7024).  The tests call these
 // functions to compare this library's results with the reference's GPU kernels
 // on the same inputs:
 //   ref_copy      gpu_tensor_block_copy        (TALSH/tensor_algebra_gpu_nvidia.cu:4806)

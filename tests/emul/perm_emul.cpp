@@ -79,6 +79,12 @@ int main(int argc, char** argv) {
     };
     if (NLIST) { check_list(gl, "load"); check_list(gs, P.rows2d ? "row store" : "column store"); }
   }
+  // General-plan list kernel (perm_glist_kernel): replayed for every plan that
+  // fits its lists (16-byte-aligned input), whichever kernel the launcher
+  // picks for it -- full tiles through the lists, partial tiles through the
+  // table-driven store below.
+  const int GVB = perm_glist_vector_bytes(P, 16, 256);
+  std::vector<long long> out4(GVB ? vol : 0, -1);
   const int V = P.V, LA = P.LA, LB = P.LB;
   const long long bufn = (long long)P.nA * P.lap;
   std::vector<long long> buf(bufn, -1);
@@ -170,8 +176,44 @@ int main(int argc, char** argv) {
               if (buf[ee] < 0) fail("store reads unloaded smem", ee, tile);
               if (out[dst] != -1) fail("double write", dst, tile);
               out[dst] = buf[ee];
+              if (GVB && !full) out4[dst] = buf[ee];  // the list kernel's partial tiles
             }
           }
+        }
+    }
+    if (GVB && full) {
+      const int VW = GVB / es, nvec = LA / VW, nld_all = P.nA * nvec;
+      if ((long long)LA % VW) fail("glist rows not whole vectors", LA, VW);
+      if (P.V > kGListEntries * 256 || nld_all > kGListEntries * 256) fail("glist lists too short", P.V, nld_all);
+      std::vector<long long> gbuf(bufn, -1);
+      for (int tid = 0; tid < 256; ++tid)
+        for (int i = 0; i < kGListEntries; ++i) {
+          const int v = tid + i * 256;
+          if (v >= nld_all) break;
+          const int c = v / nvec, x = v - c * nvec;
+          const long long a = ((long long)c * P.lap + (long long)x * VW) * es;  // shared-memory bytes
+          const long long b = P.ld_base[c] + (long long)x * VW;                  // tile-relative element
+          if (a % GVB) fail("glist load smem misaligned", a, tid);
+          if (((in_base + b) * es) % GVB) fail("glist load source misaligned", in_base + b, tid);
+          if ((long long)x * VW + VW > P.lap || a / es + VW > bufn) fail("glist load smem oob", a, tid);
+          if (b >= ((long long)1 << 31)) fail("glist load offset beyond 32 bits", b, tid);
+          if (in_base + b < 0 || in_base + b + VW > vol) fail("glist load leaves the tensor", in_base + b, tid);
+          for (int t = 0; t < VW; ++t) gbuf[a / es + t] = in_base + b + t;
+        }
+      for (int tid = 0; tid < 256; ++tid)
+        for (int i = 0; i < kGListEntries; ++i) {
+          const int e = tid + i * 256;
+          if (e >= V) break;
+          const int cc = e / LB, j = e - cc * LB, q = j / P.prodB;
+          const long long pos = (long long)P.st_ebase[cc] + P.ejf[j - q * P.prodB] + (long long)q * P.ej_pb_stride;
+          const long long rel = P.st_base[cc] + j;
+          if (pos < 0 || pos >= bufn) fail("glist store smem oob", pos, tid);
+          if (rel >= ((long long)1 << 31)) fail("glist store offset beyond 32 bits", rel, tid);
+          const long long dst = out_base + rel;
+          if (dst < 0 || dst >= vol) fail("glist store oob", dst, tid);
+          if (gbuf[pos] < 0) fail("glist store reads unloaded smem", pos, tid);
+          if (out4[dst] != -1) fail("glist double write", dst, tid);
+          out4[dst] = gbuf[pos];
         }
     }
     // two-dimensional kernel replay (perm2d_kernel): rows, chunks and
@@ -266,8 +308,9 @@ int main(int argc, char** argv) {
     if (out[o] != ref[o]) fail("wrong value at", o, out[o]);
     if (P.lin2d && out2[o] != ref[o]) fail("2d wrong value at", o, out2[o]);
     if (vecpath && out3[o] != ref[o]) fail("walk wrong value at", o, out3[o]);
+    if (GVB && out4[o] != ref[o]) fail("glist wrong value at", o, out4[o]);
   }
-  printf("OK %lld %d %d %d tma=%d lin2d=%d vec2d=%d rows2d=%d lists=%d\n", (long long)P.ntiles, V, LA, LB, P.tma_ok,
-         P.lin2d, P.vec2d, P.rows2d, NLIST);
+  printf("OK %lld %d %d %d tma=%d lin2d=%d vec2d=%d rows2d=%d lists=%d glist=%d\n", (long long)P.ntiles, V, LA, LB,
+         P.tma_ok, P.lin2d, P.vec2d, P.rows2d, NLIST, GVB);
   return 0;
 }

@@ -10,7 +10,8 @@ oracle/_ref/libnvtal_ref.so and driven through the harness oracle/ref_nvtal.cpp
     conjugation) and adds (scale 1, 0.37 and complex, conjugation) must be
     bit-identical to the reference kernels' results;
   * contractions (TTGT and the tensor-core method) agree with the reference's
-    in-house GEMM path within the relative Frobenius bounds of the methods
+    TTGT path (its permutation kernels and cuBLAS GEMMs, the reference's default
+    build) within the relative Frobenius bounds of the methods
     (1e-13 / 1e-12 for R8/C8, 2e-5 / 1e-4 for R4/C4): the summation orders
     differ, so the bits do not;
   * the seeded 40^4 single-block contraction (seed 0, alpha 0.5, D = 0) agrees

@@ -83,10 +83,11 @@ def test_two_dimensional_vector_paths(emul, es):
             run(emul, es, dims, perm)
 
 
-@pytest.mark.parametrize("vmin,vmax", [(8, 24), (24, 48)])
-def test_measured_choice_tile_bounds(emul, vmin, vmax):
-    # the other tile-size bounds that large copies may be timed with and run
-    env = dict(os.environ, TB_PERM_VMIN_KB=str(vmin), TB_PERM_VMAX_KB=str(vmax))
+@pytest.mark.parametrize("vmin,vmax,minrun", [(8, 24, 256), (24, 48, 256), (8, 16, 256), (4, 16, 128)])
+def test_measured_choice_tile_bounds(emul, vmin, vmax, minrun):
+    # the other tile-size bounds (and minimum runs) that large copies may be
+    # timed with and run; the small ones are the list kernel's candidates
+    env = dict(os.environ, TB_PERM_VMIN_KB=str(vmin), TB_PERM_VMAX_KB=str(vmax), TB_PERM_MINRUN=str(minrun))
     for es in (4, 8, 16):
         for perm in itertools.permutations([1, 2, 3, 4]):
             run(emul, es, [40, 40, 40, 40] if es != 16 else [20, 20, 20, 20], perm, env)
@@ -95,7 +96,7 @@ def test_measured_choice_tile_bounds(emul, vmin, vmax):
         for dims in ([90, 90, 30, 30], [66, 70, 18, 22], [100, 37, 45, 12]):
             for perm in ([1, 3, 2, 4], [2, 1, 3, 4], [2, 4, 1, 3], [3, 4, 1, 2], [4, 3, 2, 1]):
                 run(emul, es, dims, perm, env)
-    rng = random.Random(77 + vmin)
+    rng = random.Random(77 + vmin + minrun)
     for _ in range(60):
         rank = rng.randint(2, 6)
         dims = [rng.randint(2, 40) for _ in range(rank)]
@@ -154,3 +155,20 @@ def test_offset_lists_decline_offsets_beyond_32_bits(plan_info):
     out = subprocess.run([plan_info, "8", "3", "76", "76", "1000000", "2", "1", "3"], capture_output=True, text=True,
                          check=True).stdout.split()
     assert int(out[3]) == 8, out
+
+
+@pytest.mark.parametrize("minrun", [256, 128])
+def test_sweep_shapes_general_plans(emul, minrun):
+    """The permutation sweep's rank-5/6 and skewed shapes at reduced extents
+    (the planner's structure, not the volume, decides the kernel), with the
+    list kernel's small-tile candidates: lists, tables and partial tiles."""
+    env = dict(os.environ, TB_PERM_VMIN_KB="4", TB_PERM_VMAX_KB="16", TB_PERM_MINRUN=str(minrun))
+    rng = random.Random(5 + minrun)
+    shapes = [[9, 9, 9, 9, 9], [6, 6, 6, 6, 6, 6], [5, 7, 6, 5, 6, 7], [3, 60, 60], [60, 60, 2], [5, 24, 24, 24],
+              [24, 24, 24, 7], [2, 10, 10, 10, 10, 10], [10, 10, 10, 10, 10, 4]]
+    for dims in shapes:
+        for _ in range(6):
+            perm = list(range(1, len(dims) + 1))
+            rng.shuffle(perm)
+            for es in (4, 8):
+                run(emul, es, dims, perm, env)
