@@ -125,7 +125,11 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
       t[a + 1] = best;
     }
   }
-  // 4. extend the tile to Vmin elements: whole small dims first, then the partial dims
+  // 4. extend the tile to Vmin elements: whole small dims first, then the
+  // partial dims, then a divisor of a dim outside both blocks (so that no tile
+  // is partial in it: when the load and store blocks cover the same dims, the
+  // tile would otherwise stay as small as they are, e.g. 18 x 18 of an 18^6
+  // tensor)
   for (int guard = 0; guard < 4 * r + 8; ++guard) {
     int64_t V = vol_of();
     if (V >= Vmin) break;
@@ -140,6 +144,11 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
         const int64_t f = std::min(cdiv(D[d], t[d]), cdiv(Vmin, V));
         if (f > 1) { const int64_t nt = even(D[d], t[d] * f); if (nt > t[d]) { t[d] = nt; grown = true; } }
       }
+    }
+    for (int i = 0; i < r && !grown; ++i) {
+      if (t[i] != 1 || D[i] <= 1 || i <= a || inB[i]) continue;
+      for (int64_t x = std::min(D[i] - 1, Vmax / V); x >= 2; --x)
+        if (D[i] % x == 0) { t[i] = x; grown = true; break; }
     }
     if (!grown) break;
   }
@@ -274,8 +283,9 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     bool ok = bulk_rows && (tot * es) % 16 == 0 && (prodA * t[a] * es) % 16 == 0;
     for (int i = a + 1; i < r; ++i) if ((SI[i] * es) % 16 != 0) ok = false;
     P.tma_ok = ok ? 1 : 0;
-    // the same for 8-byte copies of 4-byte elements
-    bool ok8 = rows8 && (tot * es) % 8 == 0 && (prodA * t[a] * es) % 8 == 0;
+    // the same for 8-byte copies of 4-byte elements (also when the rows are
+    // whole 16-byte units but the row starts are only 8-byte aligned)
+    bool ok8 = !ok && (rows8 || bulk_rows) && es < 8 && (tot * es) % 8 == 0 && (prodA * t[a] * es) % 8 == 0;
     for (int i = a + 1; i < r; ++i) if ((SI[i] * es) % 8 != 0) ok8 = false;
     P.vec8 = ok8 ? 1 : 0;
   }

@@ -254,6 +254,8 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
     }
     if (k == 0) { ms0 = best_ms = ms; best = 0; }
     else if (ms < best_ms) { best_ms = ms; best = k; }
+    static const bool trace = [] { const char* e = getenv("TB_PERM_TRACE"); return e && e[0] == '1'; }();
+    if (trace) fprintf(stderr, "perm candidate %d: %.4f ms\n", idx[k], ms);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

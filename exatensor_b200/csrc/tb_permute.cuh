@@ -579,15 +579,16 @@ perm2d_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in,
 // vectors, and whose tile-relative offsets fit in 32 bits (glist_ok).
 constexpr int kGListN = kGListEntries;
 
-template <typename Elem, typename Store, int VB>
+template <typename Elem, typename Store, int VB, int ST>
 __global__ void __launch_bounds__(kPermThreads, 2)
 perm_glist_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st) {
   constexpr int es = (int)sizeof(Elem);
   constexpr int VW = VB / es;  // elements per load copy
+  constexpr int kRing = ST + 1;  // tile headers: issued, in flight, stored, being written
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PermSmem& T = *reinterpret_cast<PermSmem*>(smem_raw);
   Elem* bufs = reinterpret_cast<Elem*>(smem_raw + ((sizeof(PermSmem) + 127) & ~size_t(127)));
-  __shared__ TileOrigin org[kHdrRing];
+  __shared__ TileOrigin org[kRing];
   const size_t stage_elems = (size_t)P.nA * P.lap;
   const int tid = threadIdx.x;
   for (int i = tid; i < P.nA; i += kPermThreads) { T.ld_base[i] = P.ld_base[i]; T.ld_dpb[i] = P.ld_dpb[i]; }
@@ -598,7 +599,7 @@ perm_glist_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__
   const int64_t first = blockIdx.x, step = gridDim.x;
   const int mine = first < P.ntiles ? (int)((P.ntiles - 1 - first) / step + 1) : 0;
   if (tid == 0)
-    for (int k = 0; k < kStages && k < mine; ++k) org[k] = tile_origin(P, first + k * step);
+    for (int k = 0; k < ST && k < mine; ++k) org[k] = tile_origin(P, first + k * step);
   __syncthreads();
   // this thread's full-tile copies: load vector v = (row c, vector x), store
   // element e = (store chunk c', position j) with consecutive e along a chunk
@@ -626,8 +627,8 @@ perm_glist_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__
   store_lanes_init(P, SL);
 
   auto issue = [&](int k) {
-    const TileOrigin o = org[k % kHdrRing];
-    Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
+    const TileOrigin o = org[k % kRing];
+    Elem* stage = bufs + (size_t)(k % ST) * stage_elems;
     if (o.full) {
       const Elem* src = in + o.in_base;
       const uint32_t sbase = smem_addr(stage);
@@ -648,8 +649,8 @@ perm_glist_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__
     }
   };
   auto store = [&](int k) {
-    const TileOrigin o = org[k % kHdrRing];
-    const Elem* stage = bufs + (size_t)(k % kStages) * stage_elems;
+    const TileOrigin o = org[k % kRing];
+    const Elem* stage = bufs + (size_t)(k % ST) * stage_elems;
     if (!o.full) {
       perm_store<Elem, Store>(P, T, SL, stage, first + (int64_t)k * step, st);
       return;
@@ -676,19 +677,19 @@ perm_glist_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__
     }
   };
 
-  for (int k = 0; k < kStages - 1; ++k) {
+  for (int k = 0; k < ST - 1; ++k) {
     if (k < mine) issue(k);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
   for (int k = 0; k < mine; ++k) {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(ST - 2) : "memory");
     __syncthreads();
-    const int nk = k + kStages - 1;
+    const int nk = k + ST - 1;
     if (nk < mine) issue(nk);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    // the header slot of tile k + kStages last held tile k - 1, whose store
+    // the header slot of tile k + ST last held tile k - 1, whose store
     // finished before the barrier above; it is read after the next barrier
-    if (tid == 0 && k + kStages < mine) org[(k + kStages) % kHdrRing] = tile_origin(P, first + (int64_t)(k + kStages) * step);
+    if (tid == 0 && k + ST < mine) org[(k + ST) % kRing] = tile_origin(P, first + (int64_t)(k + ST) * step);
     store(k);
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -702,14 +703,84 @@ inline int glist_vector_bytes(const PermParams& P, const Elem* in) {
   return perm_glist_vector_bytes(P, a % 16 == 0 ? 16 : (a % 8 == 0 ? 8 : (int)sizeof(Elem)), kPermThreads);
 }
 
+// Pipeline depth of the list kernel: small tiles keep six in flight (two
+// CTAs per SM still fit), larger ones three.
+constexpr int kGListDeep = 6;
+
 template <typename Elem, typename Store, int VB>
-void launch_glist(const PermParams& P, const Elem* in, const Store& st, size_t smem, cudaStream_t s) {
-  static DeviceOnce attr;
-  smem_limit_once(attr, perm_glist_kernel<Elem, Store, VB>, 220 * 1024);
+void launch_glist(const PermParams& P, const Elem* in, const Store& st, cudaStream_t s) {
+  static DeviceOnce attr3, attr6;
+  const size_t tables = ((sizeof(PermSmem) + 127) & ~size_t(127)) + 128;
+  const size_t stage = (size_t)perm_stage_bytes(P);
+  const bool deep = tables + kGListDeep * stage <= 110 * 1024;
+  const size_t smem = tables + (deep ? kGListDeep : kStages) * stage;
   int per_sm = (int)((224 * 1024) / (smem + 1024));
   per_sm = std::max(1, std::min(per_sm, 2));  // launch bound: 2 CTAs of 256 threads per SM (register lists)
   const unsigned grid = (unsigned)std::min<int64_t>((int64_t)num_sms() * per_sm, P.ntiles);
-  perm_glist_kernel<Elem, Store, VB><<<grid, kPermThreads, smem, s>>>(P, in, st);
+  if (deep) {
+    smem_limit_once(attr6, perm_glist_kernel<Elem, Store, VB, kGListDeep>, 220 * 1024);
+    perm_glist_kernel<Elem, Store, VB, kGListDeep><<<grid, kPermThreads, smem, s>>>(P, in, st);
+  } else {
+    smem_limit_once(attr3, perm_glist_kernel<Elem, Store, VB, kStages>, 220 * 1024);
+    perm_glist_kernel<Elem, Store, VB, kStages><<<grid, kPermThreads, smem, s>>>(P, in, st);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row copies without shared memory (perm_rowcopy_kernel): plans whose store
+// chunks are the load rows themselves (the fastest dimension stays fastest,
+// as rows2d) but whose rows are not whole vectors (rows2d needs 8- or 16-byte
+// rows) need no transposition at all, so each row moves directly from global
+// to global memory: one warp per (tile, row), lanes along the row, kRowBatch
+// loads in flight per lane before their stores (with the output loads of
+// functors that read the output).
+constexpr int kRowBatch = 8;
+
+template <typename Elem, typename Store>
+__global__ void __launch_bounds__(kPermThreads)
+perm_rowcopy_kernel(const __grid_constant__ PermParams P, const Elem* __restrict__ in, Store st) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t units = P.ntiles * P.nA;
+  for (int64_t u = warp; u < units; u += nwarps) {
+    const int64_t tile = u / P.nA;
+    const int c = (int)(u - tile * P.nA);
+    const TileOrigin o = tile_origin(P, tile);
+    if (!o.full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb && c >= o.rem_b) continue;
+    int len = P.LA;
+    if (!o.full && P.pa >= 0) len = P.prodA * (P.pb == P.pa ? min(o.rem_a, o.rem_b) : o.rem_a);
+    const Elem* src = in + o.in_base + (int64_t)c * P.row_sin;
+    const int64_t ob = o.out_base + (int64_t)c * P.chunk_sout;
+    for (int j0 = 0; j0 < len; j0 += 32 * kRowBatch) {
+      Elem v[kRowBatch];
+      typename rmw_old<Store, Elem>::type old[kRowBatch];
+#pragma unroll
+      for (int t = 0; t < kRowBatch; ++t) {
+        const int j = j0 + t * 32 + lane;
+        if (j < len) v[t] = src[j];
+      }
+      if constexpr (is_rmw_store<Store>::value) {
+#pragma unroll
+        for (int t = 0; t < kRowBatch; ++t) {
+          const int j = j0 + t * 32 + lane;
+          if (j < len) old[t] = st.load(ob + j);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < kRowBatch; ++t) {
+        const int j = j0 + t * 32 + lane;
+        if (j >= len) continue;
+        if constexpr (is_rmw_store<Store>::value) st.put(ob + j, v[t], old[t]);
+        else st(ob + j, v[t]);
+      }
+    }
+  }
+}
+
+// Row-copy-shaped plans (load row c is store chunk c, same run).
+inline bool row_copy_shape(const PermParams& P) {
+  return P.lin2d && P.nA == P.nB && P.LA == P.LB && P.ej_pb_stride == 1 && (P.chunk_eb == P.lap || P.nA == 1);
 }
 
 // Whether a store functor writes vectors of vbytes to an aligned output
@@ -779,6 +850,20 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
   smem_limit_once(attr_bulk, perm_pipe_kernel<Elem, Store, true>, 220 * 1024);
   smem_limit_once(attr_async, perm_pipe_kernel<Elem, Store, false>, 220 * 1024);
   if (smem > 220 * 1024) { set_error("permutation tile too large for shared memory"); return TB_ERR_LIMIT; }
+  // TB_PERM_TRACE=1: one line per launch on stderr (plan shape and kernel; diagnostics)
+  static const bool trace = [] { const char* e = getenv("TB_PERM_TRACE"); return e && e[0] == '1'; }();
+  if (trace) {
+    const int gvb = glist_vector_bytes(P, in);
+    fprintf(stderr, "perm es=%d rank=%d V=%d LA=%d nA=%d LB=%d nB=%d prodB=%d lin2d=%d vec2d=%d rows2d=%d tma=%d "
+                    "vec8=%d tiles=%lld kernel=%s\n",
+            P.es, P.rank, P.V, P.LA, P.nA, P.LB, P.nB, P.prodB, P.lin2d, P.vec2d, P.rows2d, P.tma_ok, P.vec8,
+            (long long)P.ntiles,
+            bulk ? "bulk" : (P.lin2d && mode != 3 && (P.vec2d || P.rows2d) && P.vbytes && (uintptr_t)in % P.vbytes == 0)
+                                ? "2d-vector"
+                                : (P.lin2d && mode == 0 && glist_on && row_copy_shape(P)) ? "rowcopy"
+                                : (mode == 0 && glist_on && gvb) ? (gvb == 16 ? "glist16" : gvb == 8 ? "glist8" : "glist1")
+                                : P.lin2d && mode != 3 ? "2d-scalar" : "tables");
+  }
   int per_sm = (int)((224 * 1024) / (smem + 1024));
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 2048 / kPermThreads) per_sm = 2048 / kPermThreads;
@@ -800,18 +885,21 @@ int launch_perm(const PermParams& P, const Elem* in, const Store& st, cudaStream
       else if (rows) launch_2d<Elem, Store, V8, true>(N, P.ntiles, smem2, s, P, in, st, flags);
       else if (P.vbytes == 16) launch_2d<Elem, Store, 16, false>(N, P.ntiles, smem2, s, P, in, st, flags);
       else launch_2d<Elem, Store, V8, false>(N, P.ntiles, smem2, s, P, in, st, flags);
+    } else if (mode == 0 && glist_on && row_copy_shape(P)) {
+      const unsigned grid = (unsigned)std::min<int64_t>((int64_t)num_sms() * 8, (P.ntiles * P.nA + 7) / 8);
+      perm_rowcopy_kernel<Elem, Store><<<std::max(1u, grid), kPermThreads, 0, s>>>(P, in, st);
     } else if (const int gvb = (mode == 0 && glist_on) ? glist_vector_bytes(P, in) : 0) {
-      if (gvb == 16) launch_glist<Elem, Store, (sizeof(Elem) < 16 ? 16 : sizeof(Elem))>(P, in, st, smem, s);
-      else if (gvb == 8) launch_glist<Elem, Store, (sizeof(Elem) < 8 ? 8 : sizeof(Elem))>(P, in, st, smem, s);
-      else launch_glist<Elem, Store, sizeof(Elem)>(P, in, st, smem, s);
+      if (gvb == 16) launch_glist<Elem, Store, (sizeof(Elem) < 16 ? 16 : sizeof(Elem))>(P, in, st, s);
+      else if (gvb == 8) launch_glist<Elem, Store, (sizeof(Elem) < 8 ? 8 : sizeof(Elem))>(P, in, st, s);
+      else launch_glist<Elem, Store, sizeof(Elem)>(P, in, st, s);
     } else {
       launch_2d<Elem, Store, 0, false>(0, P.ntiles, smem2, s, P, in, st, 0);
     }
   } else if (!bulk && mode == 0 && glist_on && glist_vector_bytes(P, in)) {
     const int gvb = glist_vector_bytes(P, in);
-    if (gvb == 16) launch_glist<Elem, Store, (sizeof(Elem) < 16 ? 16 : sizeof(Elem))>(P, in, st, smem, s);
-    else if (gvb == 8) launch_glist<Elem, Store, (sizeof(Elem) < 8 ? 8 : sizeof(Elem))>(P, in, st, smem, s);
-    else launch_glist<Elem, Store, sizeof(Elem)>(P, in, st, smem, s);
+    if (gvb == 16) launch_glist<Elem, Store, (sizeof(Elem) < 16 ? 16 : sizeof(Elem))>(P, in, st, s);
+    else if (gvb == 8) launch_glist<Elem, Store, (sizeof(Elem) < 8 ? 8 : sizeof(Elem))>(P, in, st, s);
+    else launch_glist<Elem, Store, sizeof(Elem)>(P, in, st, s);
   } else if (bulk)
     perm_pipe_kernel<Elem, Store, true><<<(unsigned)grid, kPermThreads, smem, s>>>(P, in, st, device_error_word());
   else

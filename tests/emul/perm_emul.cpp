@@ -85,6 +85,11 @@ int main(int argc, char** argv) {
   // table-driven store below.
   const int GVB = perm_glist_vector_bytes(P, 16, 256);
   std::vector<long long> out4(GVB ? vol : 0, -1);
+  // Row-copy kernel (perm_rowcopy_kernel): plans whose store chunk c is load
+  // row c move each row global to global; replayed for every such plan.
+  const bool ROWCOPY = P.lin2d && P.nA == P.nB && P.LA == P.LB && P.ej_pb_stride == 1 &&
+                       (P.chunk_eb == P.lap || P.nA == 1);
+  std::vector<long long> out5(ROWCOPY ? vol : 0, -1);
   const int V = P.V, LA = P.LA, LB = P.LB;
   const long long bufn = (long long)P.nA * P.lap;
   std::vector<long long> buf(bufn, -1);
@@ -216,6 +221,21 @@ int main(int argc, char** argv) {
           out4[dst] = gbuf[pos];
         }
     }
+    if (ROWCOPY) {
+      for (int c = 0; c < P.nA; ++c) {
+        if (!full && P.pb >= 0 && P.pb != P.pa && P.row_is_pb && c >= rem_b) continue;
+        long long len = P.LA;
+        if (!full && P.pa >= 0) len = (long long)P.prodA * (P.pb == P.pa ? std::min(rem_a, rem_b) : rem_a);
+        for (long long j = 0; j < len; ++j) {
+          const long long src = in_base + (long long)c * P.row_sin + j;
+          const long long dst = out_base + (long long)c * P.chunk_sout + j;
+          if (src < 0 || src >= vol) fail("rowcopy load oob", src, tile);
+          if (dst < 0 || dst >= vol) fail("rowcopy store oob", dst, tile);
+          if (out5[dst] != -1) fail("rowcopy double write", dst, tile);
+          out5[dst] = src;
+        }
+      }
+    }
     // two-dimensional kernel replay (perm2d_kernel): rows, chunks and
     // positions by formula instead of the chunk tables
     if (P.vec2d) {
@@ -309,8 +329,9 @@ int main(int argc, char** argv) {
     if (P.lin2d && out2[o] != ref[o]) fail("2d wrong value at", o, out2[o]);
     if (vecpath && out3[o] != ref[o]) fail("walk wrong value at", o, out3[o]);
     if (GVB && out4[o] != ref[o]) fail("glist wrong value at", o, out4[o]);
+    if (ROWCOPY && out5[o] != ref[o]) fail("rowcopy wrong value at", o, out5[o]);
   }
-  printf("OK %lld %d %d %d tma=%d lin2d=%d vec2d=%d rows2d=%d lists=%d glist=%d\n", (long long)P.ntiles, V, LA, LB,
-         P.tma_ok, P.lin2d, P.vec2d, P.rows2d, NLIST, GVB);
+  printf("OK %lld %d %d %d tma=%d vec8=%d lin2d=%d vec2d=%d rows2d=%d lists=%d glist=%d rowcopy=%d\n",
+         (long long)P.ntiles, V, LA, LB, P.tma_ok, P.vec8, P.lin2d, P.vec2d, P.rows2d, NLIST, GVB, (int)ROWCOPY);
   return 0;
 }
