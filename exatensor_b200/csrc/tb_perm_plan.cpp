@@ -356,6 +356,8 @@ int build_perm_plan(int es, int rank, const int64_t* dims_in, const int64_t* sin
     if (ext > 1) { P.gdim[g] = i; P.gext[g] = ext; P.gdiv[g].init((uint64_t)ext); ++g; nt *= ext; }
   }
   P.ngd = g; P.ntiles = nt;
+  P.gd32 = nt < ((int64_t)1 << 31) ? 1 : 0;
+  for (int k = 0; k < g; ++k) magic32((uint32_t)std::min<int64_t>(P.gext[k], (int64_t)1 << 31), &P.gmag[k], &P.gsh[k]);
   return 0;
 }
 

@@ -41,6 +41,11 @@ struct PermParams {
   int gdim[kPlanMaxRank];        // reduced dim of each grid dim
   int64_t gext[kPlanMaxRank];    // tile positions along each grid dim
   FastDiv gdiv[kPlanMaxRank];    // divisors for gext
+  // 32-bit magic divisors for gext, valid while ntiles < 2^31 (gd32 = 1): a
+  // tile's origin then costs one 32x32->64 multiply and a shift per grid dim
+  int gd32;
+  uint32_t gmag[kPlanMaxRank];
+  int gsh[kPlanMaxRank];
   uint32_t la_magic; int la_shift;   // 32-bit fast division by LA
   uint32_t lb_magic; int lb_shift;   // by LB
   uint32_t pb_magic; int pb_shift;   // by prodB

@@ -61,7 +61,7 @@ __device__ __forceinline__ TileOrigin tile_origin(const PermParams& P, int64_t t
   TileOrigin o{0, 0, 1 << 30, 1 << 30, true};
   uint64_t r = (uint64_t)tile;
   for (int g = 0; g < P.ngd; ++g) {
-    const uint64_t q = P.gdiv[g].div(r);
+    const uint64_t q = P.gd32 ? (uint64_t)fdiv32((uint32_t)r, P.gmag[g], P.gsh[g]) : P.gdiv[g].div(r);
     const int64_t x = (int64_t)(r - q * (uint64_t)P.gext[g]);
     r = q;
     const int d = P.gdim[g];

@@ -104,6 +104,10 @@ int main(int argc, char** argv) {
     for (int g = 0; g < P.ngd; ++g) {
       unsigned long long q = P.gdiv[g].div(r);
       if (q != r / (unsigned long long)P.gext[g]) fail("fastdiv", r, P.gext[g]);
+      if (P.gd32) {
+        if (r >= (1ull << 31)) fail("gd32 with a tile index past 2^31", r, tile);
+        if (fdiv32((uint32_t)r, P.gmag[g], P.gsh[g]) != q) fail("fdiv32 grid", r, P.gext[g]);
+      }
       long long x = (long long)(r - q * P.gext[g]);
       r = q;
       int d = P.gdim[g];
