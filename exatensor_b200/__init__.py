@@ -37,13 +37,14 @@ class TBError(RuntimeError):
 class Plan(C.Structure):
     """tb_plan_t: contraction plan (method, INT8 slices, N tile, split-BF16 terms, M tile)."""
     _fields_ = [("method", C.c_int), ("slices", C.c_int), ("tile_n", C.c_int), ("bf16_terms", C.c_int),
-                ("tile_m", C.c_int), ("reserved", C.c_int * 3)]
+                ("tile_m", C.c_int), ("moduli", C.c_int), ("reserved", C.c_int * 2)]
 
 
 class ContractStats(C.Structure):
     _fields_ = [("method", C.c_int), ("slices", C.c_int), ("passes", C.c_int), ("gemm_launches", C.c_int),
                 ("m", C.c_longlong), ("n", C.c_longlong), ("k", C.c_longlong), ("flops", C.c_double),
-                ("products", C.c_int), ("tile_n", C.c_int), ("tile_m", C.c_int)]
+                ("products", C.c_int), ("tile_n", C.c_int), ("tile_m", C.c_int), ("moduli", C.c_int),
+                ("residue_bits", C.c_int)]
 
 
 class BlockTask(C.Structure):
@@ -181,9 +182,12 @@ def fill_uniform(dtk, volume, d_ptr, seed, lo=-1.0, hi=1.0, stream=None):
     _check(lib().tb_fill_uniform(dtk, volume, C.c_void_p(d_ptr), seed, lo, hi, _stream(stream)))
 
 
-def make_plan(method=METHOD_AUTO, slices=0, tile_n=0, bf16_terms=0, tile_m=0) -> Plan:
+def make_plan(method=METHOD_AUTO, slices=0, tile_n=0, bf16_terms=0, tile_m=0, moduli=0) -> Plan:
+    """moduli (R8/C8 on the tensor cores): 0 = modular residues where possible,
+    8..15 = that many moduli, -1 = INT8 slices; slices > 0 also selects slices."""
     p = Plan()
     p.method, p.slices, p.tile_n, p.bf16_terms, p.tile_m = method, slices, tile_n, bf16_terms, tile_m
+    p.moduli = moduli
     return p
 
 

@@ -108,6 +108,7 @@ template <int BN>
 int launch_tc_epi(const TcGemmParams& P, int epi, bool pair, cudaStream_t s) {
   if (pair) {
     switch (epi) {
+      case EPI_RESID: return launch_tc2<BN, true, EPI_RESID>(P, s);
       case EPI_OZAKI_R: return launch_tc2<BN, true, EPI_OZAKI_R>(P, s);
       case EPI_OZAKI_C: return launch_tc2<BN, true, EPI_OZAKI_C>(P, s);
       case EPI_BF16_R: return launch_tc2<BN, false, EPI_BF16_R>(P, s);
@@ -115,11 +116,84 @@ int launch_tc_epi(const TcGemmParams& P, int epi, bool pair, cudaStream_t s) {
     }
   }
   switch (epi) {
+    case EPI_RESID: return launch_tc<BN, true, EPI_RESID>(P, s);
     case EPI_OZAKI_R: return launch_tc<BN, true, EPI_OZAKI_R>(P, s);
     case EPI_OZAKI_C: return launch_tc<BN, true, EPI_OZAKI_C>(P, s);
     case EPI_BF16_R: return launch_tc<BN, false, EPI_BF16_R>(P, s);
     default: return launch_tc<BN, false, EPI_BF16_C>(P, s);
   }
+}
+
+// ---- Ozaki scheme II: modular residues -----------------------------------------
+// Pairwise coprime moduli <= 256, largest first (their residues in the
+// symmetric range are signed 8-bit).  With n of them, M = prod m_i and the
+// operands scaled to integers |X| <= 2^p, an exact INT32 GEMM per modulus and
+// the Chinese remainder theorem give the exact integer product as long as
+// M > 2 Kr 2^(2p) (Kr: the real contraction length).
+constexpr int kModuliTable[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193};
+constexpr int kMinModuli = 8;
+constexpr int kResidueBitsTarget = 46;  // operand bits kept by the default choice (INT8 slices keep 47)
+
+using u128 = unsigned __int128;
+
+u128 moduli_product(int n) {
+  u128 M = 1;
+  for (int i = 0; i < n; ++i) M *= (u128)kModuliTable[i];
+  return M;
+}
+
+// The largest p with M > 2 Kr 2^(2p) for n moduli (checked in exact integer arithmetic).
+int residue_bits(int n, int64_t Kr) {
+  const u128 M = moduli_product(n);
+  int p = 0;
+  while (p < 60 && (M >> (2 * (p + 1))) > (u128)(2 * Kr)) ++p;
+  return p;
+}
+
+struct ResiduePlan {
+  ResidueSpec rs;
+  int p;
+  CrtParams crt;  // constants only; pointers and sizes are filled by the caller
+};
+
+// Moduli count and constants for a contraction of real length Kr: `want` > 0
+// asks for that many moduli, else the fewest with p >= kResidueBitsTarget.
+// Returns false when no allowed count reaches kResidueBitsTarget bits.
+bool plan_residues(int64_t Kr, int want, ResiduePlan* out) {
+  int n = want;
+  if (n <= 0) {
+    for (n = kMinModuli; n <= kMaxModuli && residue_bits(n, Kr) < kResidueBitsTarget; ++n) {}
+    if (n > kMaxModuli) return false;
+  }
+  if (n < kMinModuli || n > kMaxModuli) return false;
+  const int p = residue_bits(n, Kr);
+  if (p < 20 || p > 52) return false;
+  ResiduePlan& R = *out;
+  std::memset(&R, 0, sizeof(R));
+  R.p = p;
+  R.rs.n = n;
+  R.rs.pscale = std::ldexp(1.0, p + 1);
+  const u128 M = moduli_product(n);
+  R.crt.n = n;
+  R.crt.M_lo = (uint64_t)M;
+  R.crt.M_hi = (uint64_t)(M >> 64);
+  R.crt.Md = (double)(uint64_t)(M >> 64) * 18446744073709551616.0 + (double)(uint64_t)M;
+  R.crt.shift = 2 * (p + 1);
+  for (int i = 0; i < n; ++i) {
+    const int m = kModuliTable[i];
+    R.rs.mod[i] = m;
+    R.rs.inv[i] = 1.0 / (double)m;
+    const u128 Mi = M / (u128)m;
+    const int mi_mod = (int)(Mi % (u128)m);
+    int y = 0;
+    for (int c = 1; c < m; ++c)
+      if ((mi_mod * c) % m == 1) { y = c; break; }
+    R.crt.mod[i] = m;
+    R.crt.y[i] = y;
+    R.crt.mi_lo[i] = (uint64_t)Mi;
+    R.crt.mi_hi[i] = (uint64_t)(Mi >> 64);
+  }
+  return true;
 }
 
 }  // namespace
@@ -175,7 +249,23 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   std::vector<int> shifts;
   const int kblocks = (int)(Kpad * (i8 ? 1 : 2) / 128);  // 128-byte K blocks
   int S = 0, npa = 2, npb = 2;
-  if (i8) {
+  // R8/C8: modular residues (one exact INT8 GEMM per modulus, fewer than the
+  // slice pairs) unless the plan asks for INT8 slices, or the contraction is
+  // longer than one exact INT32 pass (1023 K blocks) or needs more moduli
+  ResiduePlan RP;
+  const bool resid = i8 && !(plan && (plan->slices > 0 || plan->moduli < 0)) && kblocks <= 1023 &&
+                     plan_residues(Kr, plan ? plan->moduli : 0, &RP);
+  if (i8 && plan && plan->moduli > 0 && !resid) {
+    set_error("modular residues: %d moduli do not fit this contraction (K = %lld)", plan->moduli, (long long)Kr);
+    return TB_ERR_INVALID_ARGS;
+  }
+  if (resid) {
+    for (int i = 0; i < RP.rs.n; ++i) {
+      passes.push_back({{i, i, 0, kblocks}});
+      shifts.push_back(RP.rs.mod[i]);  // the epilogue's modulus
+    }
+    npa = npb = RP.rs.n;
+  } else if (i8) {
     S = (plan && plan->slices > 0) ? plan->slices : kDefaultSlices;
     if (S < 2 || S > kMaxSlices) { set_error("slice count %d outside 2..%d", S, kMaxSlices); return TB_ERR_INVALID_ARGS; }
     // |slice| <= 128, so one K block (128 products) adds at most 128^3.
@@ -249,7 +339,8 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
                offLA = offDn + al(Nc * 8), offLB = offLA + al(M * 8), offKA = offLB + al(Nc * 8),
                offKB = offKA + al(K * 8), offRE = offKB + al(K * 8), offCE = offRE + al(M * 4),
                offRX = offCE + al(Nc * 4), offCX = offRX + al(M * 4), offBR = offCX + al(Nr * 4),
-               offBC = offBR + al(M * 4), offNB = offBC + al(Nc * 4), total = offNB + 256;
+               offBC = offBR + al(M * 4), offNB = offBC + al(Nc * 4), offRES = offNB + 256,
+               total = offRES + (resid ? al((size_t)RP.rs.n * Npad * Mpad) : 0);
   unsigned char* ws = nullptr;
   if (int e = scratch_alloc((void**)&ws, total, s)) return e;
   int err = 0;
@@ -280,9 +371,11 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     GA.src = A.ptr; GA.lm = lmA; GA.lk = lkA; GA.rows = M; GA.K = K; GA.kpad = Kpad; GA.pstride = Mpad * Kpad;
     GA.planes = Ap; GA.rowE = rowE; GA.slices = S; GA.isign = A.conj ? -1.0 : 1.0;
     GA.lanes_on_k = (A.ks[0].s1 == 1 || A.rows.empty() || A.rows[0].s1 != 1) ? 1 : 0;
+    if (resid) GA.rs = RP.rs;
     GB.src = B.ptr; GB.lm = lmB; GB.lk = lkB; GB.rows = Nc; GB.K = K; GB.kpad = Kpad; GB.pstride = Npad * Kpad;
     GB.planes = Bp; GB.rowE = colE; GB.slices = S; GB.isign = B.conj ? -1.0 : 1.0;
     GB.lanes_on_k = (B.ks[0].s1 == 1 || B.rows.empty() || B.rows[0].s1 != 1) ? 1 : 0;
+    if (resid) GB.rs = RP.rs;
     const int tmr = i8 && cplx ? 32 : 64;               // gather tile rows (16-byte elements: 32)
     const int64_t gA = Mpad / tmr, gB = (cplx ? Npad / 2 : Npad) / tmr, gk = ksrc_pad / kGK;
     // row / column exponents and the lists of rows and columns flagged as
@@ -309,7 +402,13 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
         if ((err = run_rowmax<true>(GB, eB, ek, s))) break;
       }
       if ((err = run_exps())) break;
-      if (!cplx) {
+      if (resid && !cplx) {
+        if ((err = run_gather<G_RESID_R8>(GA, gA, gk, s))) break;
+        if ((err = run_gather<G_RESID_R8>(GB, gB, gk, s))) break;
+      } else if (resid) {
+        if ((err = run_gather<G_RESID_C8A>(GA, gA, gk, s))) break;
+        if ((err = run_gather<G_RESID_C8B>(GB, gB, gk, s))) break;
+      } else if (!cplx) {
         if ((err = run_gather<G_SLICE_R8>(GA, gA, gk, s))) break;
         if ((err = run_gather<G_SLICE_R8>(GB, gB, gk, s))) break;
       } else {
@@ -352,12 +451,38 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     P.ar = realpha; P.ai = cplx ? ai : 0.0;
     P.br = accumulate ? 1.0 : 0.0; P.bi = 0.0;
     P.err = device_error_word();
-    P.nf_skip = 1;
-    const int epi = i8 ? (cplx ? EPI_OZAKI_C : EPI_OZAKI_R) : (cplx ? EPI_BF16_C : EPI_BF16_R);
+    P.nf_skip = resid ? 0 : 1;  // residues: crt_kernel leaves the flagged entries to the fix-up
+    if (resid) {
+      P.res = (uint8_t*)(ws + offRES);
+      P.res_ld = Mpad;
+      P.res_plane = Npad * Mpad;
+    }
+    const int epi = resid ? EPI_RESID : i8 ? (cplx ? EPI_OZAKI_C : EPI_OZAKI_R) : (cplx ? EPI_BF16_C : EPI_BF16_R);
     const int ts = timed_begin(s);
     err = BN == 256 ? launch_tc_epi<256>(P, epi, pair, s) : launch_tc_epi<128>(P, epi, pair, s);
     timed_end(ts, s);
     if (err) break;
+    if (resid) {
+      // Chinese remainder reconstruction of the exact products into D
+      CrtParams C = RP.crt;
+      C.res = (const uint8_t*)(ws + offRES);
+      C.res_ld = Mpad;
+      C.res_plane = Npad * Mpad;
+      C.rows = M;
+      C.cols = Nc;
+      C.dm = dm; C.dn = dn; C.D = d;
+      C.rowexp = rowx; C.colexp = colx;
+      C.ar = realpha; C.ai = cplx ? ai : 0.0; C.br = P.br; C.bi = 0.0;
+      const dim3 cg((unsigned)std::min<int64_t>(64, (M + 255) / 256), (unsigned)std::min<int64_t>(Nc, 4096));
+      if (cplx) crt_kernel<true><<<cg, 256, 0, s>>>(C);
+      else crt_kernel<false><<<cg, 256, 0, s>>>(C);
+      count_launch();
+      if (cudaError_t e = cudaGetLastError()) {
+        set_error("residue reconstruction launch: %s", cudaGetErrorString(e));
+        err = TB_ERR_CUDA;
+        break;
+      }
+    }
     // entries of rows / columns with a NaN or an infinity (returns at once without)
     NfParams F;
     F.srcA = A.ptr; F.srcB = B.ptr;
@@ -386,6 +511,8 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       stats->tile_m = TM;
       stats->gemm_launches = 1;
       stats->m = M; stats->n = Nr; stats->k = Kr;
+      stats->moduli = resid ? RP.rs.n : 0;
+      stats->residue_bits = resid ? RP.p : 0;
     }
   } while (false);
   scratch_free(ws, s);

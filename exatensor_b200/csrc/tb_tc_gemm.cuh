@@ -25,7 +25,11 @@ constexpr int kStagesTC = 4;
 constexpr int kMaxProducts = 64;  // entries (plane pair and K range) over all passes
 constexpr int kTcThreads = 192;
 
-enum TcEpilogue { EPI_OZAKI_R = 0, EPI_OZAKI_C = 1, EPI_BF16_R = 2, EPI_BF16_C = 3 };
+// EPI_RESID: modular residues (Ozaki scheme II) -- each pass is one modulus
+// (pass_shift holds it) and the epilogue stores acc mod m as one byte per
+// element into residue plane `pass` (layout [pass][column][row], rows fastest);
+// crt_kernel later rebuilds D from all planes.
+enum TcEpilogue { EPI_OZAKI_R = 0, EPI_OZAKI_C = 1, EPI_BF16_R = 2, EPI_BF16_C = 3, EPI_RESID = 4 };
 
 struct __align__(64) TcGemmParams {
   CUtensorMap tmA;            // 3-D: (K elements, rows, planes)
@@ -46,6 +50,8 @@ struct __align__(64) TcGemmParams {
   double ar, ai, br, bi;      // alpha, beta
   unsigned int* err;
   int nf_skip;                // 1: leave entries of flagged rows / columns to the non-finite fix-up
+  uint8_t* res;               // EPI_RESID: residue planes
+  int64_t res_ld, res_plane;  // EPI_RESID: column stride and plane stride (bytes)
 };
 
 // A row or column whose exponent entry exceeds this holds a NaN or an
@@ -107,6 +113,23 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
     uint32_t r[32];
     tmem_ld32(tcol + (uint32_t)(c * 32), r);
     const int n0 = nb * BN + c * 32;
+    if constexpr (EPI == EPI_RESID) {
+      // residues of the exact INT32 sums: shift is the modulus, and the
+      // caller passes this pass's plane through P.res / res_plane
+      if constexpr (std::is_same<EP, TcGemmParams>::value) {
+        if (mval) {
+          uint8_t* col = P.res + dmo;  // dmo: this pass's plane offset + row
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            if (n0 + j >= P.N) break;
+            int v = (int)r[j] % shift;
+            if (v < 0) v += shift;
+            col[(int64_t)(n0 + j) * P.res_ld] = (uint8_t)v;
+          }
+        }
+      }
+      continue;
+    }
     // lane j: metadata of column n0 + j (complex: of column pair (n0 + j) / 2)
     const int nl = n0 + lane;
     const bool lvalid = nl < P.N;
@@ -280,9 +303,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
         if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
         tc_fence_after();
         const bool first = (p == 0);
-        const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) ? P.pass_shift[p] : 0;
-        epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, nb, first,
-                               shift);
+        const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C || EPI == EPI_RESID) ? P.pass_shift[p] : 0;
+        const int64_t dmp = EPI == EPI_RESID ? (int64_t)p * P.res_plane + m : dmo;
+        epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN),
+                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, first, shift);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&bars->acc_empty[a]);
@@ -431,9 +455,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
         const uint32_t aph = (acc_it >> 1) & 1;
         if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
         tc_fence_after();
-        const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) ? P.pass_shift[p] : 0;
-        epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, nb,
-                               p == 0, shift);
+        const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C || EPI == EPI_RESID) ? P.pass_shift[p] : 0;
+        const int64_t dmp = EPI == EPI_RESID ? (int64_t)p * P.res_plane + m : dmo;
+        epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN),
+                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, p == 0, shift);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive_cluster(acc_empty0 + (uint32_t)(a * sizeof(uint64_t)));

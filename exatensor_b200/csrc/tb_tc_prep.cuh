@@ -112,7 +112,20 @@ constexpr int kMaxSlicesDev = 7;
 template <typename E> constexpr int gather_rows() { return sizeof(E) == 16 ? 32 : 64; }  // 32-34 KB tiles
 constexpr int kGK = 64;
 
-enum GatherMode { G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A, G_SPLIT_C4B };
+enum GatherMode { G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A, G_SPLIT_C4B,
+                  G_RESID_R8, G_RESID_C8A, G_RESID_C8B };
+
+// Ozaki scheme II operands: each scaled value x in (-1/2, 1/2) becomes the
+// integer X = floor(x 2^(p+1)) (|X| <= 2^p, exact in FP64), stored as its
+// residues modulo the pairwise coprime moduli m_i <= 256 in the symmetric
+// range (signed 8 bits), one plane per modulus.
+constexpr int kMaxModuli = 15;
+struct ResidueSpec {
+  int n;                    // moduli
+  double pscale;            // 2^(p+1)
+  int mod[kMaxModuli];
+  double inv[kMaxModuli];   // 1 / m_i
+};
 
 struct GatherParams {
   const void* src;
@@ -127,7 +140,25 @@ struct GatherParams {
   int slices;
   int lanes_on_k;      // 1: consecutive k are contiguous in the source
   double isign;        // -1 conjugates the imaginary part
+  ResidueSpec rs;      // residue modes: the moduli
 };
+
+// Residues of four integer-valued doubles modulo m (symmetric range), packed
+// little-endian: q = rint(X / m) from the reciprocal (off by at most one),
+// r = X - q m exact by one FMA, then moved into [-(m/2), (m-1)/2].
+__device__ __forceinline__ uint32_t residue4(const double (&X)[4], int m, double inv) {
+  const int hi = (m - 1) / 2, lo = -(m / 2);
+  uint32_t w = 0;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const double q = rint(X[t] * inv);
+    int r = (int)fma(-q, (double)m, X[t]);
+    if (r > hi) r -= m;
+    if (r < lo) r += m;
+    w |= (uint32_t)(uint8_t)(int8_t)r << (8 * t);
+  }
+  return w;
+}
 
 // Slices of x in (-1/2, 1/2): balanced signed base-256 digits of the fixed-point
 // value X = floor(x * 2^55) = sum_i d_i 2^(48-8i), d_i in [-128, 127] for
@@ -151,7 +182,8 @@ __device__ __forceinline__ uint32_t slice4(long long y0, long long y1, long long
 
 template <int MODE>
 __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowtile, int ky, int kstep) {
-  constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
+  constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B ||
+                        MODE == G_RESID_C8A || MODE == G_RESID_C8B;
   constexpr bool F32 = MODE == G_SPLIT_R4 || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
   using R = typename std::conditional<F32, float, double>::type;
   using E = typename std::conditional<CPLX, typename std::conditional<F32, float2, double2>::type, R>::type;
@@ -198,7 +230,57 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
       for (int idx = tid; idx < TM * (TK / 4); idx += kGThreads) {
         const int mm = idx / (TK / 4), kq = (idx % (TK / 4)) * 4;
         const int64_t m = m0 + mm, k = k0 + kq;
-        if constexpr (MODE == G_SLICE_R8) {
+        if constexpr (MODE == G_RESID_R8) {
+          const int se = sm_se[mm];
+          double X[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) X[t] = floor(scale2(tile[mm][kq + t], se) * P.rs.pscale);
+          int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
+#pragma unroll 1
+          for (int i = 0; i < P.rs.n; ++i)
+            *reinterpret_cast<uint32_t*>(base + i * P.pstride) = residue4(X, P.rs.mod[i], P.rs.inv[i]);
+        } else if constexpr (MODE == G_RESID_C8A) {
+          // A' row m: (re, im) interleaved along K
+          const int se = sm_se[mm];
+          double R[4], I[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const E v = tile[mm][kq + t];
+            R[t] = floor(scale2(v.x, se) * P.rs.pscale);
+            I[t] = floor(scale2(P.isign * v.y, se) * P.rs.pscale);
+          }
+          double xa[4] = {R[0], I[0], R[1], I[1]}, xb[4] = {R[2], I[2], R[3], I[3]};
+          int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
+#pragma unroll 1
+          for (int i = 0; i < P.rs.n; ++i) {
+            const int md = P.rs.mod[i];
+            const double inv = P.rs.inv[i];
+            *reinterpret_cast<uint2*>(base + i * P.pstride) = make_uint2(residue4(xa, md, inv), residue4(xb, md, inv));
+          }
+        } else if constexpr (MODE == G_RESID_C8B) {
+          // B' rows 2n = (re, -im), 2n+1 = (im, re) interleaved along K
+          const int se = sm_se[mm];
+          double R[4], I[4], NI[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const E v = tile[mm][kq + t];
+            const double im = scale2(P.isign * v.y, se);
+            R[t] = floor(scale2(v.x, se) * P.rs.pscale);
+            I[t] = floor(im * P.rs.pscale);
+            NI[t] = floor(-im * P.rs.pscale);
+          }
+          double r0a[4] = {R[0], NI[0], R[1], NI[1]}, r0b[4] = {R[2], NI[2], R[3], NI[3]};
+          double r1a[4] = {I[0], R[0], I[1], R[1]}, r1b[4] = {I[2], R[2], I[3], R[3]};
+          int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
+          int8_t* b1 = b0 + P.kpad;
+#pragma unroll 1
+          for (int i = 0; i < P.rs.n; ++i) {
+            const int md = P.rs.mod[i];
+            const double inv = P.rs.inv[i];
+            *reinterpret_cast<uint2*>(b0 + i * P.pstride) = make_uint2(residue4(r0a, md, inv), residue4(r0b, md, inv));
+            *reinterpret_cast<uint2*>(b1 + i * P.pstride) = make_uint2(residue4(r1a, md, inv), residue4(r1b, md, inv));
+          }
+        } else if constexpr (MODE == G_SLICE_R8) {
           const int se = sm_se[mm];
           long long X[4];
 #pragma unroll
@@ -416,6 +498,89 @@ __global__ void __launch_bounds__(256) nonfinite_fixup_kernel(const __grid_const
 // shared-memory staging: each thread keeps the running maximum of the rows it
 // touches in registers over all K tiles of its CTA, and the CTA merges them once
 // at the end.  Thread -> (row, k) mapping as in gather_kernel.
+// ---- Ozaki scheme II reconstruction (Chinese remainder theorem) ------------------
+// With M = prod m_i, M_i = M / m_i and y_i = M_i^-1 mod m_i, the exact integer
+// dot product is C = sum_i t_i M_i mod M, t_i = (r_i y_i) mod m_i, taken in the
+// symmetric range (|C| < M / 2 by the choice of p).  Each t_i M_i < M, so the
+// sum stays below n M < 2^123 in 128 bits.  C is converted to FP64 (about one
+// rounding), scaled by 2^(e_m + f_n - 2(p+1)) exactly, and D = beta D +
+// alpha C through the offset tables.  Rows and columns flagged as holding a
+// NaN or an infinity are left to the fix-up kernel.  Grid: x over rows (D's
+// fastest), y over columns.
+struct CrtParams {
+  const uint8_t* res;          // residue planes [i][column][row], bytes
+  int64_t res_ld, res_plane;
+  int n;
+  int mod[kMaxModuli], y[kMaxModuli];
+  uint64_t mi_lo[kMaxModuli], mi_hi[kMaxModuli];
+  uint64_t M_lo, M_hi;
+  double Md;                   // M as a double
+  int64_t rows, cols;          // rows of A; columns of B (complex: column pairs)
+  const int64_t* dm;
+  const int64_t* dn;
+  void* D;
+  const int* rowexp;
+  const int* colexp;
+  int shift;                   // 2 (p + 1)
+  double ar, ai, br, bi;
+};
+
+__device__ __forceinline__ double u128_to_double(unsigned __int128 x) {
+  return (double)(uint64_t)(x >> 64) * 18446744073709551616.0 + (double)(uint64_t)x;
+}
+
+__device__ __forceinline__ double crt_value(const CrtParams& P, int64_t col, int64_t m) {
+  const uint8_t* rp = P.res + col * P.res_ld + m;
+  unsigned __int128 S = 0;
+#pragma unroll 1
+  for (int i = 0; i < P.n; ++i) {
+    const int t = ((int)rp[i * P.res_plane] * P.y[i]) % P.mod[i];
+    S += (unsigned __int128)(uint64_t)t * (((unsigned __int128)P.mi_hi[i] << 64) | P.mi_lo[i]);
+  }
+  const unsigned __int128 M = ((unsigned __int128)P.M_hi << 64) | P.M_lo;
+  // S < n M: subtract q M, q = floor(S / M) estimated in FP64 (within one), then
+  // at most a few exact corrections
+  uint64_t q = (uint64_t)(u128_to_double(S) / P.Md);
+  if (q > 0) --q;
+  S -= (unsigned __int128)q * M;
+  for (int it = 0; it < 4 && S >= M; ++it) S -= M;
+  const bool neg = S > (M >> 1);
+  const double v = u128_to_double(neg ? M - S : S);
+  return neg ? -v : v;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
+  for (int64_t n = blockIdx.y; n < P.cols; n += gridDim.y) {
+    const int ce = P.colexp[CPLX ? 2 * n : n];
+    if (ce >= kNonFiniteExp) continue;  // flagged column: the fix-up's
+    const int64_t dno = P.dn[n];
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < P.rows; m += (int64_t)gridDim.x * blockDim.x) {
+      const int re = P.rowexp[m];
+      if (re >= kNonFiniteExp) continue;  // flagged row: the fix-up's
+      const int e = re + ce - P.shift;
+      const int64_t o = P.dm[m] + dno;
+      if constexpr (!CPLX) {
+        double* D = (double*)P.D;
+        const double v = P.ar * scale2(crt_value(P, n, m), e);
+        D[o] = P.br == 0.0 ? v : fma(P.br, D[o], v);
+      } else {
+        double2* D = (double2*)P.D;
+        const double xr = scale2(crt_value(P, 2 * n, m), e), xi = scale2(crt_value(P, 2 * n + 1, m), e);
+        double2 v;
+        v.x = P.ar * xr - P.ai * xi;
+        v.y = P.ar * xi + P.ai * xr;
+        if (P.br != 0.0 || P.bi != 0.0) {
+          const double2 d = D[o];
+          v.x += P.br * d.x - P.bi * d.y;
+          v.y += P.br * d.y + P.bi * d.x;
+        }
+        D[o] = v;
+      }
+    }
+  }
+}
+
 template <bool CPLX>
 __device__ __forceinline__ void rowmax_body(const GatherParams& P, int64_t rowtile, int ky, int kstep) {
   using E = typename std::conditional<CPLX, double2, double>::type;

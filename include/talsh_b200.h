@@ -37,7 +37,8 @@ extern "C" {
 /* Contraction methods. */
 #define TB_METHOD_AUTO 0      /* plan selector decides */
 #define TB_METHOD_TTGT 1      /* plain: permute, GEMM in the tensor's own type, permute back */
-#define TB_METHOD_FUSED 2     /* tensor cores: fused gather/epilogue, split-BF16 or INT8 slices */
+#define TB_METHOD_FUSED 2     /* tensor cores: fused gather/epilogue; split-BF16 (R4/C4), modular
+                                 residues or INT8 slices (R8/C8) */
 
 /* Contraction plan (all-zero = automatic). */
 typedef struct {
@@ -46,7 +47,11 @@ typedef struct {
   int tile_n;      /* tensor-core N tile: 0 (default), 128 or 256 */
   int bf16_terms;  /* split-BF16 products for R4/C4 fused: 0 (default = 3) */
   int tile_m;      /* tensor-core M tile: 0 (default), 128 (one SM) or 256 (an SM pair) */
-  int reserved[3];
+  int moduli;      /* R8/C8 fused: 0 (default) = modular residues (Ozaki scheme II) where the
+                      contraction allows, with the fewest moduli that keep 46 bits per operand;
+                      8..15 = that many moduli; -1 = INT8 slices (Ozaki scheme I) instead.
+                      A positive `slices` also selects INT8 slices. */
+  int reserved[2];
 } tb_plan_t;
 
 /* Last error message of the calling thread ("" if none). */
@@ -277,6 +282,8 @@ typedef struct {
                         terms); its tensor-core work is products * flops */
   int tile_n;        /* tensor-core N tile of the executed plan */
   int tile_m;        /* tensor-core M tile: 128 (one SM) or 256 (an SM pair, cta_group::2) */
+  int moduli;        /* R8/C8 fused with modular residues: moduli (one INT8 GEMM each); 0 otherwise */
+  int residue_bits;  /* ... and the bits p kept per operand (|X| <= 2^p) */
 } tb_contract_stats_t;
 int tb_last_contract_stats(tb_contract_stats_t* stats);
 

@@ -34,9 +34,40 @@ def fused(xt, dev, pattern, ext, dtk, alpha=1.0, accumulative=True, plan=None, s
 
 
 def test_fused_r8_square(xt, dev):
+    # the default for R8 on the tensor cores: modular residues (Ozaki scheme II)
     err, st = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 256, "j": 256, "k": 256}, O.R8)
     assert err <= TOL[O.R8], err
-    assert st.slices == 6 and st.passes >= 6 and st.products == 21
+    assert st.moduli >= 8 and st.residue_bits >= 46 and st.products == st.moduli and st.passes == st.moduli
+    # INT8 slices (Ozaki scheme I) on request
+    err, st = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", {"i": 256, "j": 256, "k": 256}, O.R8,
+                    plan=xt.make_plan(XB.METHOD_FUSED, moduli=-1))
+    assert err <= TOL[O.R8], err
+    assert st.moduli == 0 and st.slices == 6 and st.passes >= 6 and st.products == 21
+
+
+@pytest.mark.parametrize("dtk", [O.R8, O.C8])
+@pytest.mark.parametrize("moduli", [10, 12, 14, 15])
+def test_residue_moduli_counts(xt, dev, dtk, moduli):
+    """More moduli keep more bits per operand (p, with prod m_i > 2 K 2^(2p));
+    the error falls with p: it stays within 2^(5-p) relative Frobenius
+    (uniform data, K = 512) for every count."""
+    ext = {"i": 192, "j": 160, "k": 512}
+    err, st = fused(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", ext, dtk, alpha=0.75,
+                    plan=xt.make_plan(XB.METHOD_FUSED, moduli=moduli))
+    assert st.moduli == moduli and st.products == moduli
+    assert err <= 2.0 ** (5 - st.residue_bits), (moduli, st.residue_bits, err)
+    if moduli >= 14:
+        assert err <= TOL[dtk], err
+
+
+def test_residues_and_slices_agree(xt, dev):
+    """Both FP64 schemes on the same contraction: within their bounds of each other."""
+    ext = {"a": 24, "b": 20, "c": 16, "d": 12, "i": 10, "j": 9}
+    pat = "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)"
+    e1, s1 = fused(xt, dev, pat, ext, O.R8, plan=xt.make_plan(XB.METHOD_FUSED), seed=9)
+    e2, s2 = fused(xt, dev, pat, ext, O.R8, plan=xt.make_plan(XB.METHOD_FUSED, slices=6), seed=9)
+    assert s1.moduli > 0 and s2.moduli == 0
+    assert e1 <= TOL[O.R8] and e2 <= TOL[O.R8]
 
 
 @pytest.mark.parametrize("dtk", [O.R8, O.R4, O.C8, O.C4])
