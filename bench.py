@@ -326,7 +326,8 @@ def ccsd_case(X, s, s_obj, name, steps, warmup, nsamp, psteps=None, world=1, on_
     rel = full_rel(case.D, dplain, fp32=wl["dtk"] in (4, 14))
     case.dchosen = case.D.clone()
     del dplain
-    rec = {"chosen": {"method": {1: "ttgt", 2: "fused"}.get(st.method, st.method), "slices": st.slices,
+    rec = {"chosen": {"method": {1: "ttgt", 2: "fused"}.get(st.method, st.method), "moduli": st.moduli,
+                      "slices": st.slices,
                       "tile_n": st.tile_n, "tile_m": st.tile_m, "ms": sig(ms), "TFLOP/s": sig(case.flops / ms / 1e9)},
            "plain": {"ms": sig(pms), "TFLOP/s": sig(case.flops / pms / 1e9)},
            "chosen_over_plain": sig(pms / ms, 3),
@@ -929,7 +930,9 @@ def run_ours(args):
         per_launch_ms = gemm_ms / max(1, gemm_n)
         i8 = wl["dtk"] in (8, 18)
         if chosen_method == "fused":
-            kern = "tc_gemm_kernel: tcgen05 INT8-slice GEMM" if i8 else "tc_gemm_kernel: tcgen05 split-BF16 GEMM"
+            kern = ("tc_gemm_kernel: tcgen05 INT8 GEMM, " + (f"{st.moduli} modular residues" if st.moduli
+                                                                else f"{st.slices} slices")) if i8 else \
+                "tc_gemm_kernel: tcgen05 split-BF16 GEMM"
             hw_ops = case.flops * max(1, st.products)  # each slice pair / BF16 term is a full GEMM
             peak = pk["i8_tops_sustained"] if i8 else bf16_tflops
             peak_note = ("measured: tb_peak_measure INT8 tcgen05, sustained (the GEMM runs back to back for the "
@@ -985,7 +988,8 @@ def run_ours(args):
             "vs_baseline": None, "dtype": {4: "f32", 8: "f64", 14: "c64", 18: "c128"}[wl["dtk"]], "data": DATA,
             "config": config_of(args.workload),
             "permute": perm, "configs": configs, "c1": c1, "block_sparse": bsc, "selector": sel, "peaks": pk,
-            "plan": {"method": chosen_method, "slices": st.slices, "passes": st.passes, "products": st.products,
+            "plan": {"method": chosen_method, "moduli": st.moduli, "residue_bits": st.residue_bits,
+                     "slices": st.slices, "passes": st.passes, "products": st.products,
                      "tile_n": st.tile_n, "tile_m": st.tile_m, "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": cnt.get("clk"),
             "gpu_launches": cnt.get("launches"),
@@ -1073,7 +1077,8 @@ def run_profile(args):
     X.device_check(s)
     st = X.last_contract_stats()
     print(json.dumps({"profile": args.profile, "workload": args.workload, "v": wl["v"], "o": wl["o"],
-                      "method": st.method, "slices": st.slices, "products": st.products, "tile_n": st.tile_n,
+                      "method": st.method, "moduli": st.moduli, "slices": st.slices, "products": st.products,
+                      "tile_n": st.tile_n,
                       "tile_m": st.tile_m,
                       "ms_per_step": round(ms / args.steps, 3),
                       "TFLOP/s": round(case.flops * args.steps / (ms / 1e3) / 1e12, 3)}))

@@ -166,8 +166,9 @@ bool plan_residues(int64_t Kr, int want, ResiduePlan* out) {
     if (n > kMaxModuli) return false;
   }
   if (n < kMinModuli || n > kMaxModuli) return false;
-  const int p = residue_bits(n, Kr);
-  if (p < 20 || p > 52) return false;
+  // at most 52 bits: X = floor(x 2^(p+1)) must be exact in FP64
+  const int p = std::min(residue_bits(n, Kr), 52);
+  if (p < 20) return false;
   ResiduePlan& R = *out;
   std::memset(&R, 0, sizeof(R));
   R.p = p;
