@@ -180,10 +180,17 @@ bool plan_residues(int64_t Kr, int want, ResiduePlan* out) {
   R.crt.M_hi = (uint64_t)(M >> 64);
   R.crt.Md = (double)(uint64_t)(M >> 64) * 18446744073709551616.0 + (double)(uint64_t)M;
   R.crt.shift = 2 * (p + 1);
+  R.rs.ndig = p <= 47 ? 3 : 4;
   for (int i = 0; i < n; ++i) {
     const int m = kModuliTable[i];
     R.rs.mod[i] = m;
-    R.rs.inv[i] = 1.0 / (double)m;
+    R.rs.modf[i] = (float)m;
+    R.rs.invf[i] = 1.0f / (float)m;
+    for (int j = 0; j < 4; ++j) {  // 2^(16 j) mod m, symmetric range
+      int c = (int)(((u128)1 << (16 * j)) % (u128)m);
+      if (c > (m - 1) / 2) c -= m;
+      R.rs.cdig[i][j] = (float)c;
+    }
     const u128 Mi = M / (u128)m;
     const int mi_mod = (int)(Mi % (u128)m);
     int y = 0;
@@ -474,9 +481,13 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       C.dm = dm; C.dn = dn; C.D = d;
       C.rowexp = rowx; C.colexp = colx;
       C.ar = realpha; C.ai = cplx ? ai : 0.0; C.br = P.br; C.bi = 0.0;
-      const dim3 cg((unsigned)std::min<int64_t>(64, (M + 255) / 256), (unsigned)std::min<int64_t>(Nc, 4096));
-      if (cplx) crt_kernel<true><<<cg, 256, 0, s>>>(C);
-      else crt_kernel<false><<<cg, 256, 0, s>>>(C);
+      static DeviceOnce crt_attr_r, crt_attr_c;
+      const cudaError_t ea = cplx ? smem_limit_once(crt_attr_c, crt_kernel<true>, kCrtTableBytes)
+                                  : smem_limit_once(crt_attr_r, crt_kernel<false>, kCrtTableBytes);
+      if (ea != cudaSuccess) { set_error("residue reconstruction smem attribute: %s", cudaGetErrorString(ea)); err = TB_ERR_CUDA; break; }
+      const unsigned cg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(Nc, 3 * num_sms()));
+      if (cplx) crt_kernel<true><<<cg, 256, kCrtTableBytes, s>>>(C);
+      else crt_kernel<false><<<cg, 256, kCrtTableBytes, s>>>(C);
       count_launch();
       if (cudaError_t e = cudaGetLastError()) {
         set_error("residue reconstruction launch: %s", cudaGetErrorString(e));

@@ -123,8 +123,11 @@ constexpr int kMaxModuli = 15;
 struct ResidueSpec {
   int n;                    // moduli
   double pscale;            // 2^(p+1)
+  int ndig;                 // balanced 16-bit digits of X: 3 (p <= 47) or 4
   int mod[kMaxModuli];
-  double inv[kMaxModuli];   // 1 / m_i
+  float modf[kMaxModuli];   // m_i
+  float invf[kMaxModuli];   // 1 / m_i (FP32)
+  float cdig[kMaxModuli][4];  // 2^(16 j) mod m_i, symmetric range
 };
 
 struct GatherParams {
@@ -143,21 +146,52 @@ struct GatherParams {
   ResidueSpec rs;      // residue modes: the moduli
 };
 
-// Residues of four integer-valued doubles modulo m (symmetric range), packed
-// little-endian: q = rint(X / m) from the reciprocal (off by at most one),
-// r = X - q m exact by one FMA, then moved into [-(m/2), (m-1)/2].
-__device__ __forceinline__ uint32_t residue4(const double (&X)[4], int m, double inv) {
-  const int hi = (m - 1) / 2, lo = -(m / 2);
-  uint32_t w = 0;
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const double q = rint(X[t] * inv);
-    int r = (int)fma(-q, (double)m, X[t]);
-    if (r > hi) r -= m;
-    if (r < lo) r += m;
-    w |= (uint32_t)(uint8_t)(int8_t)r << (8 * t);
+// Residues of integers |X| <= 2^p (p <= 63) held exactly as doubles.  X is
+// split once into balanced 16-bit digits D_j (|D_j| <= 2^15; three digits
+// when p <= 47), so that for every modulus the residue is
+//   raw = sum_j D_j c_j   (c_j = 2^(16 j) mod m in the symmetric range),
+// exact in FP32 (|raw| <= 4 * 2^15 * 128 = 2^24), then r = raw - m rint(raw / m)
+// in [-m/2, m/2] -- exact, the quotient rounded by the 1.5 * 2^23 trick (right
+// since raw / m is never within 1/(2m) of a half integer for odd m, and the
+// product's error is far below that).  The low byte of r, read off the bit
+// pattern of r + 1.5 * 2^23, is r in signed 8 bits (for m = 256, r = 128 gives
+// -128, the same residue).
+struct Digits16 { float d[4]; };
+
+// ndig = 3: the top digit is x2 itself (|x2| <= 2^15 + 1 for p <= 47);
+// ndig = 4: x2 is split once more (|x3| <= 2^(p-48) + 1).
+__device__ __forceinline__ Digits16 digits16(double X, int ndig) {
+  Digits16 g;
+  const double x1 = rint(X * (1.0 / 65536.0));
+  g.d[0] = (float)fma(-x1, 65536.0, X);
+  const double x2 = rint(x1 * (1.0 / 65536.0));
+  g.d[1] = (float)fma(-x2, 65536.0, x1);
+  if (ndig > 3) {
+    const double x3 = rint(x2 * (1.0 / 65536.0));
+    g.d[2] = (float)fma(-x3, 65536.0, x2);
+    g.d[3] = (float)x3;
+  } else {
+    g.d[2] = (float)x2;
+    g.d[3] = 0.f;
   }
-  return w;
+  return g;
+}
+
+__device__ __forceinline__ uint32_t residue_byte(const Digits16& g, const ResidueSpec& S, int i) {
+  constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+  float raw = g.d[0] * S.cdig[i][0];
+  raw = fmaf(g.d[1], S.cdig[i][1], raw);
+  raw = fmaf(g.d[2], S.cdig[i][2], raw);
+  if (S.ndig > 3) raw = fmaf(g.d[3], S.cdig[i][3], raw);
+  const float q = fmaf(raw, S.invf[i], kMagic) - kMagic;
+  const float r = fmaf(-q, S.modf[i], raw);
+  return (uint32_t)__float_as_int(r + kMagic) & 0xFFu;
+}
+
+// Residue i of four values, packed little-endian.
+__device__ __forceinline__ uint32_t residue4(const Digits16 (&g)[4], const ResidueSpec& S, int i) {
+  return residue_byte(g[0], S, i) | (residue_byte(g[1], S, i) << 8) | (residue_byte(g[2], S, i) << 16) |
+         (residue_byte(g[3], S, i) << 24);
 }
 
 // Slices of x in (-1/2, 1/2): balanced signed base-256 digits of the fixed-point
@@ -232,53 +266,48 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
         const int64_t m = m0 + mm, k = k0 + kq;
         if constexpr (MODE == G_RESID_R8) {
           const int se = sm_se[mm];
-          double X[4];
+          Digits16 g[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) X[t] = floor(scale2(tile[mm][kq + t], se) * P.rs.pscale);
+          for (int t = 0; t < 4; ++t) g[t] = digits16(floor(scale2(tile[mm][kq + t], se) * P.rs.pscale), P.rs.ndig);
           int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
 #pragma unroll 1
-          for (int i = 0; i < P.rs.n; ++i)
-            *reinterpret_cast<uint32_t*>(base + i * P.pstride) = residue4(X, P.rs.mod[i], P.rs.inv[i]);
+          for (int i = 0; i < P.rs.n; ++i) *reinterpret_cast<uint32_t*>(base + i * P.pstride) = residue4(g, P.rs, i);
         } else if constexpr (MODE == G_RESID_C8A) {
           // A' row m: (re, im) interleaved along K
           const int se = sm_se[mm];
-          double R[4], I[4];
+          Digits16 ga[4], gb[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
-            R[t] = floor(scale2(v.x, se) * P.rs.pscale);
-            I[t] = floor(scale2(P.isign * v.y, se) * P.rs.pscale);
+          for (int t = 0; t < 2; ++t) {
+            const E v0 = tile[mm][kq + t], v1 = tile[mm][kq + 2 + t];
+            ga[2 * t] = digits16(floor(scale2(v0.x, se) * P.rs.pscale), P.rs.ndig);
+            ga[2 * t + 1] = digits16(floor(scale2(P.isign * v0.y, se) * P.rs.pscale), P.rs.ndig);
+            gb[2 * t] = digits16(floor(scale2(v1.x, se) * P.rs.pscale), P.rs.ndig);
+            gb[2 * t + 1] = digits16(floor(scale2(P.isign * v1.y, se) * P.rs.pscale), P.rs.ndig);
           }
-          double xa[4] = {R[0], I[0], R[1], I[1]}, xb[4] = {R[2], I[2], R[3], I[3]};
           int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
 #pragma unroll 1
-          for (int i = 0; i < P.rs.n; ++i) {
-            const int md = P.rs.mod[i];
-            const double inv = P.rs.inv[i];
-            *reinterpret_cast<uint2*>(base + i * P.pstride) = make_uint2(residue4(xa, md, inv), residue4(xb, md, inv));
-          }
+          for (int i = 0; i < P.rs.n; ++i)
+            *reinterpret_cast<uint2*>(base + i * P.pstride) = make_uint2(residue4(ga, P.rs, i), residue4(gb, P.rs, i));
         } else if constexpr (MODE == G_RESID_C8B) {
           // B' rows 2n = (re, -im), 2n+1 = (im, re) interleaved along K
           const int se = sm_se[mm];
-          double R[4], I[4], NI[4];
+          Digits16 R[4], I[4], NI[4];
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
             const E v = tile[mm][kq + t];
             const double im = scale2(P.isign * v.y, se);
-            R[t] = floor(scale2(v.x, se) * P.rs.pscale);
-            I[t] = floor(im * P.rs.pscale);
-            NI[t] = floor(-im * P.rs.pscale);
+            R[t] = digits16(floor(scale2(v.x, se) * P.rs.pscale), P.rs.ndig);
+            I[t] = digits16(floor(im * P.rs.pscale), P.rs.ndig);
+            NI[t] = digits16(floor(-im * P.rs.pscale), P.rs.ndig);
           }
-          double r0a[4] = {R[0], NI[0], R[1], NI[1]}, r0b[4] = {R[2], NI[2], R[3], NI[3]};
-          double r1a[4] = {I[0], R[0], I[1], R[1]}, r1b[4] = {I[2], R[2], I[3], R[3]};
+          const Digits16 r0a[4] = {R[0], NI[0], R[1], NI[1]}, r0b[4] = {R[2], NI[2], R[3], NI[3]};
+          const Digits16 r1a[4] = {I[0], R[0], I[1], R[1]}, r1b[4] = {I[2], R[2], I[3], R[3]};
           int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
           int8_t* b1 = b0 + P.kpad;
 #pragma unroll 1
           for (int i = 0; i < P.rs.n; ++i) {
-            const int md = P.rs.mod[i];
-            const double inv = P.rs.inv[i];
-            *reinterpret_cast<uint2*>(b0 + i * P.pstride) = make_uint2(residue4(r0a, md, inv), residue4(r0b, md, inv));
-            *reinterpret_cast<uint2*>(b1 + i * P.pstride) = make_uint2(residue4(r1a, md, inv), residue4(r1b, md, inv));
+            *reinterpret_cast<uint2*>(b0 + i * P.pstride) = make_uint2(residue4(r0a, P.rs, i), residue4(r0b, P.rs, i));
+            *reinterpret_cast<uint2*>(b1 + i * P.pstride) = make_uint2(residue4(r1a, P.rs, i), residue4(r1b, P.rs, i));
           }
         } else if constexpr (MODE == G_SLICE_R8) {
           const int se = sm_se[mm];
@@ -505,8 +534,8 @@ __global__ void __launch_bounds__(256) nonfinite_fixup_kernel(const __grid_const
 // sum stays below n M < 2^123 in 128 bits.  C is converted to FP64 (about one
 // rounding), scaled by 2^(e_m + f_n - 2(p+1)) exactly, and D = beta D +
 // alpha C through the offset tables.  Rows and columns flagged as holding a
-// NaN or an infinity are left to the fix-up kernel.  Grid: x over rows (D's
-// fastest), y over columns.
+// NaN or an infinity are left to the fix-up kernel.  Persistent CTAs take
+// whole columns, threads along the rows (D's fastest).
 struct CrtParams {
   const uint8_t* res;          // residue planes [i][column][row], bytes
   int64_t res_ld, res_plane;
@@ -529,14 +558,22 @@ __device__ __forceinline__ double u128_to_double(unsigned __int128 x) {
   return (double)(uint64_t)(x >> 64) * 18446744073709551616.0 + (double)(uint64_t)x;
 }
 
-__device__ __forceinline__ double crt_value(const CrtParams& P, int64_t col, int64_t m) {
+// The table of crt_kernel: entry i * 256 + r = ((r y_i) mod m_i) M_i (r < m_i),
+// built by each CTA in shared memory, so that a residue costs one lookup and a
+// 128-bit addition.
+constexpr int kCrtTableBytes = kMaxModuli * 256 * 16;
+struct alignas(16) CrtEntry { uint64_t lo, hi; };
+
+__device__ __forceinline__ double crt_value(const CrtParams& P, const CrtEntry* tab, int64_t col, int64_t m) {
   const uint8_t* rp = P.res + col * P.res_ld + m;
-  unsigned __int128 S = 0;
+  uint64_t lo = 0, hi = 0;
 #pragma unroll 1
   for (int i = 0; i < P.n; ++i) {
-    const int t = ((int)rp[i * P.res_plane] * P.y[i]) % P.mod[i];
-    S += (unsigned __int128)(uint64_t)t * (((unsigned __int128)P.mi_hi[i] << 64) | P.mi_lo[i]);
+    const CrtEntry t = tab[i * 256 + rp[i * P.res_plane]];
+    lo += t.lo;
+    hi += t.hi + (lo < t.lo ? 1u : 0u);
   }
+  unsigned __int128 S = ((unsigned __int128)hi << 64) | lo;
   const unsigned __int128 M = ((unsigned __int128)P.M_hi << 64) | P.M_lo;
   // S < n M: subtract q M, q = floor(S / M) estimated in FP64 (within one), then
   // at most a few exact corrections
@@ -551,22 +588,36 @@ __device__ __forceinline__ double crt_value(const CrtParams& P, int64_t col, int
 
 template <bool CPLX>
 __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
-  for (int64_t n = blockIdx.y; n < P.cols; n += gridDim.y) {
+  extern __shared__ __align__(16) unsigned char crt_smem[];
+  CrtEntry* tab = reinterpret_cast<CrtEntry*>(crt_smem);
+  for (int e = threadIdx.x; e < P.n * 256; e += blockDim.x) {
+    const int i = e >> 8, r = e & 255;
+    CrtEntry t{0, 0};
+    if (r < P.mod[i]) {
+      const uint64_t c = (uint64_t)((r * P.y[i]) % P.mod[i]);
+      const unsigned __int128 v = (unsigned __int128)c * (((unsigned __int128)P.mi_hi[i] << 64) | P.mi_lo[i]);
+      t.lo = (uint64_t)v;
+      t.hi = (uint64_t)(v >> 64);
+    }
+    tab[e] = t;
+  }
+  __syncthreads();
+  for (int64_t n = blockIdx.x; n < P.cols; n += gridDim.x) {
     const int ce = P.colexp[CPLX ? 2 * n : n];
     if (ce >= kNonFiniteExp) continue;  // flagged column: the fix-up's
     const int64_t dno = P.dn[n];
-    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < P.rows; m += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t m = threadIdx.x; m < P.rows; m += blockDim.x) {
       const int re = P.rowexp[m];
       if (re >= kNonFiniteExp) continue;  // flagged row: the fix-up's
       const int e = re + ce - P.shift;
       const int64_t o = P.dm[m] + dno;
       if constexpr (!CPLX) {
         double* D = (double*)P.D;
-        const double v = P.ar * scale2(crt_value(P, n, m), e);
+        const double v = P.ar * scale2(crt_value(P, tab, n, m), e);
         D[o] = P.br == 0.0 ? v : fma(P.br, D[o], v);
       } else {
         double2* D = (double2*)P.D;
-        const double xr = scale2(crt_value(P, 2 * n, m), e), xi = scale2(crt_value(P, 2 * n + 1, m), e);
+        const double xr = scale2(crt_value(P, tab, 2 * n, m), e), xi = scale2(crt_value(P, tab, 2 * n + 1, m), e);
         double2 v;
         v.x = P.ar * xr - P.ai * xi;
         v.y = P.ar * xi + P.ai * xr;
