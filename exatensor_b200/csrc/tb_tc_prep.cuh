@@ -223,7 +223,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
   using E = typename std::conditional<CPLX, typename std::conditional<F32, float2, double2>::type, R>::type;
   constexpr int TM = gather_rows<E>(), TK = kGK;
   __shared__ E tile[TM][TK + 1];
-  __shared__ int64_t sm_lm[TM], sm_lk[TK];
+  __shared__ int64_t sm_lm[TM];
   __shared__ int sm_se[TM];  // slice modes: the row's scale exponent
   const int64_t m0 = rowtile * TM;
   const int tid = threadIdx.x;
@@ -233,32 +233,36 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
   }
   const E* src = (const E*)P.src;
   const int64_t ntiles = (P.kpad / (CPLX ? 2 : 1)) / TK;  // conversion also writes the padding
+  // The next tile's values are loaded into registers while the current one is
+  // converted (the loads' latency overlaps the conversion arithmetic); the
+  // K offsets of the next tile are read by the threads that load them.
+  constexpr int IT = TM * TK / kGThreads;
+  E v[IT];
+  auto load_tile = [&](int64_t k0) {
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int idx = tid + it * kGThreads;
+      const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+      if constexpr (CPLX) { v[it].x = 0; v[it].y = 0; } else { v[it] = 0; }
+      const int64_t k = k0 + kk;
+      if (sm_lm[mm] >= 0 && k < P.K) v[it] = src[sm_lm[mm] + P.lk[k]];
+    }
+  };
+  __syncthreads();  // sm_lm ready
+  if (ky < ntiles) load_tile((int64_t)ky * TK);
   for (int64_t kt = ky; kt < ntiles; kt += kstep) {
     const int64_t k0 = kt * TK;
     __syncthreads();  // previous tile consumed
-    if (tid < TK) sm_lk[tid] = (k0 + tid < P.K) ? P.lk[k0 + tid] : -1;
-    __syncthreads();
-    {
-      // all loads of the tile first (independent, so they overlap), then the stores
-      constexpr int IT = TM * TK / kGThreads;
-      E v[IT];
 #pragma unroll
-      for (int it = 0; it < IT; ++it) {
-        const int idx = tid + it * kGThreads;
-        const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-        const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-        if constexpr (CPLX) { v[it].x = 0; v[it].y = 0; } else { v[it] = 0; }
-        if (sm_lm[mm] >= 0 && sm_lk[kk] >= 0) v[it] = src[sm_lm[mm] + sm_lk[kk]];
-      }
-#pragma unroll
-      for (int it = 0; it < IT; ++it) {
-        const int idx = tid + it * kGThreads;
-        const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-        const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-        tile[mm][kk] = v[it];
-      }
+    for (int it = 0; it < IT; ++it) {
+      const int idx = tid + it * kGThreads;
+      const int mm = P.lanes_on_k ? idx / TK : idx % TM;
+      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
+      tile[mm][kk] = v[it];
     }
     __syncthreads();
+    if (kt + kstep < ntiles) load_tile((kt + kstep) * TK);
     {
       // convert: thread -> (row mm, 4 consecutive k)
       for (int idx = tid; idx < TM * (TK / 4); idx += kGThreads) {
@@ -409,13 +413,13 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kGThreads, 4) gather_kernel(const __grid_constant__ GatherParams P) {
+__global__ void __launch_bounds__(kGThreads, 3) gather_kernel(const __grid_constant__ GatherParams P) {
   gather_body<MODE>(P, blockIdx.x, blockIdx.y, gridDim.y);
 }
 
 // Grouped form: CTA x works on row tile map[x].y of job map[x].x.
 template <int MODE>
-__global__ void __launch_bounds__(kGThreads, 4) gather_grouped_kernel(const GatherParams* __restrict__ jobs,
+__global__ void __launch_bounds__(kGThreads, 3) gather_grouped_kernel(const GatherParams* __restrict__ jobs,
                                                                    const int2* __restrict__ map) {
   const int2 jm = map[blockIdx.x];
   const GatherParams P = jobs[jm.x];
@@ -566,10 +570,15 @@ struct alignas(16) CrtEntry { uint64_t lo, hi; };
 
 __device__ __forceinline__ double crt_value(const CrtParams& P, const CrtEntry* tab, int64_t col, int64_t m) {
   const uint8_t* rp = P.res + col * P.res_ld + m;
+  // all residue loads first (independent), then the table lookups
+  int r[kMaxModuli];
+#pragma unroll
+  for (int i = 0; i < kMaxModuli; ++i) r[i] = i < P.n ? rp[i * P.res_plane] : 0;
   uint64_t lo = 0, hi = 0;
-#pragma unroll 1
-  for (int i = 0; i < P.n; ++i) {
-    const CrtEntry t = tab[i * 256 + rp[i * P.res_plane]];
+#pragma unroll
+  for (int i = 0; i < kMaxModuli; ++i) {
+    if (i >= P.n) break;
+    const CrtEntry t = tab[i * 256 + r[i]];
     lo += t.lo;
     hi += t.hi + (lo < t.lo ? 1u : 0u);
   }
