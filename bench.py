@@ -46,9 +46,10 @@ WORKLOADS = {
     "ccsd2_r4": dict(pattern="D(a,i,b,j)+=W(a,k,c,i)*T(c,b,k,j)", v=192, o=48, dtk=4),
 }
 VIRT = set("abcd")
-# dram__bytes_read.sum + dram__bytes_write.sum of tc_gemm_kernel on the v=96 case
-# (4.90 GB + 0.96 GB) times the 16x larger work of v=192 with the same tile shape
-TC_GEMM_TRAFFIC = 16 * (4.902736e9 + 0.963089e9)
+# dram__bytes_read.sum + dram__bytes_write.sum of tc_gemm_kernel (14 modular
+# residues) on the v=96 case (2.74 GB + 0.30 GB) times the 16x larger work of
+# v=192 with the same tile shape
+TC_GEMM_TRAFFIC = 16 * (2.741619e9 + 0.298076e9)
 
 
 def shapes(pattern, v, o):
