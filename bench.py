@@ -47,9 +47,10 @@ WORKLOADS = {
 }
 VIRT = set("abcd")
 # dram__bytes_read.sum + dram__bytes_write.sum of tc_gemm_kernel (14 modular
-# residues) on the v=96 case (2.74 GB + 0.30 GB) times the 16x larger work of
-# v=192 with the same tile shape
-TC_GEMM_TRAFFIC = 16 * (2.741619e9 + 0.298076e9)
+# residues, moduli outermost, dynamic work units, B planes kept in L2) on the
+# v=96 case (1.68 GB + 0.27 GB) times the 16x larger work of v=192 with the
+# same tile shape
+TC_GEMM_TRAFFIC = 16 * (1.683749e9 + 0.273529e9)
 
 
 def shapes(pattern, v, o):

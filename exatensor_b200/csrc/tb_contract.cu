@@ -17,7 +17,10 @@
 #include "tb_pattern.h"
 #include "tb_permute.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -361,26 +364,47 @@ int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* 
         }
       }
       if (tune) {
-        // time each candidate in the mask once with alpha = 0, beta = 1 (D unchanged)
-        float best = 1e30f;
+        // time each candidate in the mask with alpha = 0, beta = 1 (D unchanged):
+        // one untimed run each (first-use costs), then two timed rounds that
+        // visit the candidates in turn, keeping each one's faster time, so that
+        // clock drift under the power cap does not favour the one timed first
+        static const bool trace = [] { const char* e = getenv("TB_SELECT_TRACE"); return e && e[0] == '1'; }();
+        constexpr int kRounds = 2;
+        float t[kNumCandidates];
+        bool ok[kNumCandidates];
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         for (int c = 0; c < kNumCandidates; ++c) {
+          t[c] = 1e30f;
+          ok[c] = false;
           if (!(tune & (1u << c))) continue;
           tb_plan_t cp = candidate(c);
-          // one untimed run (first-use costs), then the timed one
-          int ce = run_method(Z, dtk, ddims, d, ldims, l, rdims, r, 0.0, 0.0, 1, lconj, rconj, &cp, s);
-          cudaEventRecord(e0, s);
-          if (!ce) ce = run_method(Z, dtk, ddims, d, ldims, l, rdims, r, 0.0, 0.0, 1, lconj, rconj, &cp, s);
-          cudaEventRecord(e1, s);
-          float ms = 0.f;
-          if (!ce && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
-              ms < best) {
-            best = ms;
-            idx = c;
-          }
+          ok[c] = run_method(Z, dtk, ddims, d, ldims, l, rdims, r, 0.0, 0.0, 1, lconj, rconj, &cp, s) == 0;
           cudaGetLastError();
+        }
+        for (int round = 0; round < kRounds; ++round)
+          for (int c = 0; c < kNumCandidates; ++c) {
+            if (!ok[c]) continue;
+            tb_plan_t cp = candidate(c);
+            cudaEventRecord(e0, s);
+            const int ce = run_method(Z, dtk, ddims, d, ldims, l, rdims, r, 0.0, 0.0, 1, lconj, rconj, &cp, s);
+            cudaEventRecord(e1, s);
+            float ms = 0.f;
+            if (!ce && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+              t[c] = std::min(t[c], ms);
+            else
+              ok[c] = false;
+            cudaGetLastError();
+          }
+        float best = 1e30f;
+        for (int c = 0; c < kNumCandidates; ++c)
+          if (ok[c] && t[c] < best) { best = t[c]; idx = c; }
+        if (trace) {
+          std::fprintf(stderr, "tb_select: M=%lld N=%lld K=%lld", (long long)Z.M, (long long)Z.N, (long long)Z.K);
+          for (int c = 0; c < kNumCandidates; ++c)
+            if (tune & (1u << c)) std::fprintf(stderr, " cand%d=%.3fms", c, ok[c] ? t[c] : -1.f);
+          std::fprintf(stderr, " -> %d\n", idx);
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -60,8 +61,7 @@ int launch_tc(const TcGemmParams& P, cudaStream_t s) {
   static DeviceOnce attr;
   const cudaError_t e = smem_limit_once(attr, tc_gemm_kernel<BN, I8, EPI>, (int)smem);
   if (e != cudaSuccess) { set_error("tcgen05 GEMM smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
-  const int tiles = P.mtiles * P.ntiles;
-  const int grid = std::max(1, std::min(tiles, num_sms()));
+  const int grid = std::max(1, std::min(gemm_units<EPI>(P), num_sms()));
   tc_gemm_kernel<BN, I8, EPI><<<grid, kTcThreads, smem, s>>>(P);
   TB_CHECK_LAUNCH();
   return 0;
@@ -97,8 +97,7 @@ int launch_tc2(const TcGemmParams& P, cudaStream_t s) {
     max_pairs = n;
     max_pairs_of[dev].store(n, std::memory_order_relaxed);
   }
-  const int tiles = P.mtiles * P.ntiles;
-  const int pairs = std::max(1, std::min(tiles, max_pairs));
+  const int pairs = std::max(1, std::min(gemm_units<EPI>(P), max_pairs));
   tc_gemm2_kernel<BN, I8, EPI><<<2 * pairs, kTcThreads, smem, s>>>(P);
   TB_CHECK_LAUNCH();
   return 0;
@@ -131,6 +130,12 @@ int launch_tc_epi(const TcGemmParams& P, int epi, bool pair, cudaStream_t s) {
 // the Chinese remainder theorem give the exact integer product as long as
 // M > 2 Kr 2^(2p) (Kr: the real contraction length).
 constexpr int kModuliTable[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193};
+constexpr bool moduli_table_matches() {
+  for (int i = 0; i < kMaxModuli; ++i)
+    if (kModuliTable[i] != residue_modulus(i)) return false;
+  return true;
+}
+static_assert(moduli_table_matches(), "the gathers' compile-time moduli must be the plan's table");
 constexpr int kMinModuli = 8;
 constexpr int kResidueBitsTarget = 46;  // operand bits kept by the default choice (INT8 slices keep 47)
 
@@ -183,14 +188,6 @@ bool plan_residues(int64_t Kr, int want, ResiduePlan* out) {
   R.rs.ndig = p <= 47 ? 3 : 4;
   for (int i = 0; i < n; ++i) {
     const int m = kModuliTable[i];
-    R.rs.mod[i] = m;
-    R.rs.modf[i] = (float)m;
-    R.rs.invf[i] = 1.0f / (float)m;
-    for (int j = 0; j < 4; ++j) {  // 2^(16 j) mod m, symmetric range
-      int c = (int)(((u128)1 << (16 * j)) % (u128)m);
-      if (c > (m - 1) / 2) c -= m;
-      R.rs.cdig[i][j] = (float)c;
-    }
     const u128 Mi = M / (u128)m;
     const int mi_mod = (int)(Mi % (u128)m);
     int y = 0;
@@ -270,7 +267,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   if (resid) {
     for (int i = 0; i < RP.rs.n; ++i) {
       passes.push_back({{i, i, 0, kblocks}});
-      shifts.push_back(RP.rs.mod[i]);  // the epilogue's modulus
+      shifts.push_back(RP.crt.mod[i]);  // the epilogue's modulus
     }
     npa = npb = RP.rs.n;
   } else if (i8) {
@@ -390,7 +387,8 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     // holding a NaN or an infinity (exponent field 2047): the epilogue leaves
     // their D entries to nonfinite_fixup_kernel
     if (cudaMemsetAsync(rowE, 0, offRX - offRE, s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
-    if (cudaMemsetAsync(nbad, 0, 2 * sizeof(int), s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
+    // nbad[0..1]: flagged row / column counts; nbad[2]: the GEMM's work-unit counter
+    if (cudaMemsetAsync(nbad, 0, 4 * sizeof(int), s) != cudaSuccess) { err = TB_ERR_CUDA; break; }
     auto run_exps = [&]() -> int {
       exps_kernel<<<std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 4096)), 256, 0, s>>>(rowE, rowx, M, 1,
                                                                                                  badrows, nbad);
@@ -465,6 +463,16 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       P.res_ld = Mpad;
       P.res_plane = Npad * Mpad;
     }
+    // Work units: dynamic (a counter) unless TB_TC_SCHED=0.  L2 policy: with
+    // residues every unit reads one modulus's planes, and all m-tiles re-read
+    // that modulus's B plane -- when it fits in about three quarters of L2, B
+    // is kept (evict-last) and A streamed (evict-first).  TB_TC_L2HINT=0 / 1
+    // turns the policy off / on regardless.
+    static const int sched_env = [] { const char* e = getenv("TB_TC_SCHED"); return e ? atoi(e) : 1; }();
+    static const int hint_env = [] { const char* e = getenv("TB_TC_L2HINT"); return e ? atoi(e) : -1; }();
+    P.sched = sched_env ? (unsigned*)(nbad + 2) : nullptr;
+    const size_t bplane = (size_t)Npad * Kpad * oes;
+    P.l2hint = hint_env >= 0 ? (hint_env ? 1 : 0) : (resid && bplane <= (size_t)96 << 20 ? 1 : 0);
     const int epi = resid ? EPI_RESID : i8 ? (cplx ? EPI_OZAKI_C : EPI_OZAKI_R) : (cplx ? EPI_BF16_C : EPI_BF16_R);
     const int ts = timed_begin(s);
     err = BN == 256 ? launch_tc_epi<256>(P, epi, pair, s) : launch_tc_epi<128>(P, epi, pair, s);

@@ -52,7 +52,31 @@ struct __align__(64) TcGemmParams {
   int nf_skip;                // 1: leave entries of flagged rows / columns to the non-finite fix-up
   uint8_t* res;               // EPI_RESID: residue planes
   int64_t res_ld, res_plane;  // EPI_RESID: column stride and plane stride (bytes)
+  unsigned int* sched;        // single-SM kernel: zeroed work-unit counter (dynamic
+                              // scheduling), or null for a static round robin
+  int l2hint;                 // 1: A tiles are loaded evict-first and B tiles
+                              // evict-last (B planes are re-read by every m-tile)
 };
+
+// Work units of the GEMMs.  EPI_RESID: one (pass, tile) per unit with the
+// passes outermost -- every pass is one modulus with its own output plane,
+// so all CTAs work on one modulus at a time and its B plane can stay in L2.
+// Other epilogues: one tile with all its passes (they accumulate into D in
+// order).
+template <int EPI>
+__host__ __device__ __forceinline__ int gemm_units(const TcGemmParams& P) {
+  return EPI == EPI_RESID ? P.npass * P.mtiles * P.ntiles : P.mtiles * P.ntiles;
+}
+struct GemmUnit { int t, p0, p1; };
+template <int EPI>
+__device__ __forceinline__ GemmUnit gemm_unit(const TcGemmParams& P, int u) {
+  const int nt = P.mtiles * P.ntiles;
+  if (EPI == EPI_RESID) {
+    const int p = u / nt;
+    return {u - p * nt, p, p + 1};
+  }
+  return {u, 0, P.npass};
+}
 
 // A row or column whose exponent entry exceeds this holds a NaN or an
 // infinity (exponent field 2047, minus 1021): with nf_skip the epilogue leaves
@@ -69,11 +93,20 @@ struct EpiView {
   int nf_skip;
 };
 
+// Ring through which the producer hands work units to the MMA and epilogue
+// warps (one arrival from the MMA thread and one from each epilogue warp
+// frees an entry).
+constexpr int kUnitRing = 4;
+constexpr int kUnitConsumers = 5;
+
 struct TcSmemBarriers {
   uint64_t full[kStagesTC];
   uint64_t empty[kStagesTC];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
+  uint64_t unit_full[kUnitRing];
+  uint64_t unit_empty[kUnitRing];
+  int unit[kUnitRing];
   uint32_t tmem_base;
 };
 
@@ -212,12 +245,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
   unsigned char* smB = base + (size_t)kStagesTC * 128 * 128;    // [stages][BN rows][128 B]
   TcSmemBarriers* bars = (TcSmemBarriers*)(smB + (size_t)kStagesTC * BN * 128);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ntile_total = P.mtiles * P.ntiles;
-  const int nprod = P.pass_first[P.npass];
+  const int nunits = gemm_units<EPI>(P);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStagesTC; ++s) { mbar_init(&bars->full[s], 1); mbar_init(&bars->empty[s], 1); }
     for (int a = 0; a < 2; ++a) { mbar_init(&bars->acc_full[a], 1); mbar_init(&bars->acc_empty[a], 4); }
+    for (int r = 0; r < kUnitRing; ++r) {
+      mbar_init(&bars->unit_full[r], 1);
+      mbar_init(&bars->unit_empty[r], kUnitConsumers);
+    }
     fence_barrier_init();
     prefetch_tmap(&P.tmA);
     prefetch_tmap(&P.tmB);
@@ -232,23 +268,55 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
   const uint32_t tmem = bars->tmem_base;
   bool ok = true;
 
+  // Next work unit from the ring (-1: no more).  Every consumer takes every
+  // unit, in order, and frees the entry after reading it.
+  auto take_unit = [&](uint32_t j, bool warp_wide) -> int {
+    const int r = (int)(j % kUnitRing);
+    const uint32_t ph = (j / kUnitRing) & 1;
+    const bool got =
+        warp_wide ? mbar_wait_warp(&bars->unit_full[r], ph, P.err) : mbar_wait(&bars->unit_full[r], ph, P.err);
+    if (!got) { ok = false; return -1; }
+    const int u = *(volatile int*)&bars->unit[r];
+    if (warp_wide) {
+      __syncwarp();  // every lane has read the entry before the warp frees it
+      if (lane == 0) mbar_arrive(&bars->unit_empty[r]);
+    } else {
+      mbar_arrive(&bars->unit_empty[r]);
+    }
+    return u;
+  };
+
   if (warp == 0) {
-    // ---------------- TMA producer ----------------
+    // ---------------- TMA producer and scheduler ----------------
     if (lane == 0) {
+      uint64_t pol_a = 0, pol_b = 0;
+      if (P.l2hint) { pol_a = l2_policy_evict_first(); pol_b = l2_policy_evict_last(); }
       uint32_t it = 0;
       const uint32_t bytes = 128 * 128 + BN * 128;
-      for (int t = blockIdx.x; t < ntile_total && ok; t += gridDim.x) {
-        const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
-        for (int q = 0; q < nprod && ok; ++q) {
+      for (uint32_t j = 0; ok; ++j) {
+        int u = P.sched ? (int)atomicAdd(P.sched, 1u) : (int)(blockIdx.x + j * gridDim.x);
+        if (u >= nunits) u = -1;
+        const int r = (int)(j % kUnitRing);
+        if (!(ok = mbar_wait(&bars->unit_empty[r], ((j / kUnitRing) & 1) ^ 1, P.err))) break;
+        *(volatile int*)&bars->unit[r] = u;
+        mbar_arrive(&bars->unit_full[r]);
+        if (u < 0) break;
+        const GemmUnit w = gemm_unit<EPI>(P, u);
+        const int mb = w.t / P.ntiles, nb = w.t - mb * P.ntiles;
+        for (int q = P.pass_first[w.p0]; q < P.pass_first[w.p1] && ok; ++q) {
           for (int kb = P.prod_kb0[q]; kb < P.prod_kb1[q]; ++kb, ++it) {
             const int s = it % kStagesTC;
             const uint32_t ph = (it / kStagesTC) & 1;
             if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err))) break;
             mbar_expect_tx(&bars->full[s], bytes);
-            tma_load_3d(smA + (size_t)s * 128 * 128, &P.tmA, kb * (I8 ? 128 : 64), mb * 128, P.prod_a[q],
-                        &bars->full[s]);
-            tma_load_3d(smB + (size_t)s * BN * 128, &P.tmB, kb * (I8 ? 128 : 64), nb * BN, P.prod_b[q],
-                        &bars->full[s]);
+            const int kx = kb * (I8 ? 128 : 64);
+            if (P.l2hint) {
+              tma_load_3d_hint(smA + (size_t)s * 128 * 128, &P.tmA, kx, mb * 128, P.prod_a[q], &bars->full[s], pol_a);
+              tma_load_3d_hint(smB + (size_t)s * BN * 128, &P.tmB, kx, nb * BN, P.prod_b[q], &bars->full[s], pol_b);
+            } else {
+              tma_load_3d(smA + (size_t)s * 128 * 128, &P.tmA, kx, mb * 128, P.prod_a[q], &bars->full[s]);
+              tma_load_3d(smB + (size_t)s * BN * 128, &P.tmB, kx, nb * BN, P.prod_b[q], &bars->full[s]);
+            }
           }
         }
       }
@@ -258,8 +326,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
     if (lane == 0) {
       constexpr uint32_t kIdesc = idesc(I8, BN);
       uint32_t it = 0, acc_it = 0;
-      for (int t = blockIdx.x; t < ntile_total && ok; t += gridDim.x) {
-        for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
+      for (uint32_t j = 0; ok; ++j) {
+        const int u = take_unit(j, false);
+        if (u < 0) break;
+        const GemmUnit w = gemm_unit<EPI>(P, u);
+        for (int p = w.p0; p < w.p1 && ok; ++p, ++acc_it) {
           const int a = acc_it & 1;
           const uint32_t aph = (acc_it >> 1) & 1;
           if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err))) break;
@@ -291,13 +362,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
     // ---------------- epilogue (warps 2..5) ----------------
     const int quad = warp & 3;  // TMEM lanes 32*quad .. 32*quad+31
     uint32_t acc_it = 0;
-    for (int t = blockIdx.x; t < ntile_total && ok; t += gridDim.x) {
-      const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
+    for (uint32_t j = 0; ok; ++j) {
+      const int u = take_unit(j, true);
+      if (u < 0) break;
+      const GemmUnit w = gemm_unit<EPI>(P, u);
+      const int mb = w.t / P.ntiles, nb = w.t - mb * P.ntiles;
       const int m = mb * 128 + quad * 32 + lane;
       const int re = ((EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) || P.nf_skip) && m < P.M ? P.rowexp[m] : 0;
       const bool mval = m < P.M && !(P.nf_skip && re >= kNonFiniteExp);  // flagged rows: the fix-up's
       const int64_t dmo = mval ? P.dm[m] : 0;
-      for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
+      for (int p = w.p0; p < w.p1 && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
         if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
@@ -363,8 +437,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_ctarank();
   const int pair = (int)(blockIdx.x >> 1), npairs = (int)(gridDim.x >> 1);
-  const int ntile_total = P.mtiles * P.ntiles;  // mtiles counts 256-row tiles here
-  const int nprod = P.pass_first[P.npass];
+  const int nunits = gemm_units<EPI>(P);  // mtiles counts 256-row tiles here
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) { mbar_init(&bars->full[s], 1); mbar_init(&bars->empty[s], 1); }
@@ -388,9 +461,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       const uint32_t full0 = mapa_shared(smem_u32(&bars->full[0]), 0);  // CTA 0's full barriers
       uint32_t it = 0;
-      for (int t = pair; t < ntile_total && ok; t += npairs) {
-        const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
-        for (int q = 0; q < nprod && ok; ++q) {
+      for (int u = pair; u < nunits && ok; u += npairs) {
+        const GemmUnit w = gemm_unit<EPI>(P, u);
+        const int mb = w.t / P.ntiles, nb = w.t - mb * P.ntiles;
+        for (int q = P.pass_first[w.p0]; q < P.pass_first[w.p1] && ok; ++q) {
           for (int kb = P.prod_kb0[q]; kb < P.prod_kb1[q]; ++kb, ++it) {
             const int s = (int)(it % ST);
             const uint32_t ph = (it / ST) & 1;
@@ -410,8 +484,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
     if (rank == 0 && lane == 0) {
       constexpr uint32_t kIdesc = idesc(I8, BN, 256);
       uint32_t it = 0, acc_it = 0;
-      for (int t = pair; t < ntile_total && ok; t += npairs) {
-        for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
+      for (int u = pair; u < nunits && ok; u += npairs) {
+        const GemmUnit w = gemm_unit<EPI>(P, u);
+        for (int p = w.p0; p < w.p1 && ok; ++p, ++acc_it) {
           const int a = acc_it & 1;
           const uint32_t aph = (acc_it >> 1) & 1;
           if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err))) break;
@@ -444,13 +519,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
     const int quad = warp & 3;
     const uint32_t acc_empty0 = mapa_shared(smem_u32(&bars->acc_empty[0]), 0);
     uint32_t acc_it = 0;
-    for (int t = pair; t < ntile_total && ok; t += npairs) {
-      const int mb = t / P.ntiles, nb = t - mb * P.ntiles;
+    for (int u = pair; u < nunits && ok; u += npairs) {
+      const GemmUnit w = gemm_unit<EPI>(P, u);
+      const int mb = w.t / P.ntiles, nb = w.t - mb * P.ntiles;
       const int m = mb * 256 + (int)rank * 128 + quad * 32 + lane;
       const int re = ((EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C) || P.nf_skip) && m < P.M ? P.rowexp[m] : 0;
       const bool mval = m < P.M && !(P.nf_skip && re >= kNonFiniteExp);  // flagged rows: the fix-up's
       const int64_t dmo = mval ? P.dm[m] : 0;
-      for (int p = 0; p < P.npass && ok; ++p, ++acc_it) {
+      for (int p = w.p0; p < w.p1 && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
         if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;

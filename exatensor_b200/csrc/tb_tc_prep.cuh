@@ -118,16 +118,31 @@ enum GatherMode { G_SLICE_R8, G_SLICE_C8A, G_SLICE_C8B, G_SPLIT_R4, G_SPLIT_C4A,
 // Ozaki scheme II operands: each scaled value x in (-1/2, 1/2) becomes the
 // integer X = floor(x 2^(p+1)) (|X| <= 2^p, exact in FP64), stored as its
 // residues modulo the pairwise coprime moduli m_i <= 256 in the symmetric
-// range (signed 8 bits), one plane per modulus.
+// range (signed 8 bits), one plane per modulus.  The moduli are the first n
+// entries of one fixed table, so the gathers see them as compile-time
+// constants.
 constexpr int kMaxModuli = 15;
+TB_HD constexpr int residue_modulus(int i) {
+  return i == 0 ? 256 : i == 1 ? 255 : i == 2 ? 253 : i == 3 ? 251 : i == 4 ? 247 : i == 5 ? 241 : i == 6 ? 239
+       : i == 7 ? 233 : i == 8 ? 229 : i == 9 ? 227 : i == 10 ? 223 : i == 11 ? 211 : i == 12 ? 199 : i == 13 ? 197
+       : 193;
+}
+// 2^e mod m
+TB_HD constexpr int pow2_mod(int e, int m) {
+  int r = 1 % m;
+  for (int i = 0; i < e; ++i) r = (2 * r) % m;
+  return r;
+}
+// c_ij = 2^(16 j) mod m_i in the symmetric range [-(m-1)/2, m/2]
+TB_HD constexpr int residue_cdig(int i, int j) {
+  const int m = residue_modulus(i), c = pow2_mod(16 * j, m);
+  return c > (m - 1) / 2 ? c - m : c;
+}
+
 struct ResidueSpec {
-  int n;                    // moduli
+  int n;                    // moduli: residue_modulus(0 .. n-1)
   double pscale;            // 2^(p+1)
   int ndig;                 // balanced 16-bit digits of X: 3 (p <= 47) or 4
-  int mod[kMaxModuli];
-  float modf[kMaxModuli];   // m_i
-  float invf[kMaxModuli];   // 1 / m_i (FP32)
-  float cdig[kMaxModuli][4];  // 2^(16 j) mod m_i, symmetric range
 };
 
 struct GatherParams {
@@ -149,24 +164,25 @@ struct GatherParams {
 // Residues of integers |X| <= 2^p (p <= 63) held exactly as doubles.  X is
 // split once into balanced 16-bit digits D_j (|D_j| <= 2^15; three digits
 // when p <= 47), so that for every modulus the residue is
-//   raw = sum_j D_j c_j   (c_j = 2^(16 j) mod m in the symmetric range),
+//   raw = sum_j D_j c_j   (c_j = 2^(16 j) mod m in the symmetric range, c_0 = 1),
 // exact in FP32 (|raw| <= 4 * 2^15 * 128 = 2^24), then r = raw - m rint(raw / m)
 // in [-m/2, m/2] -- exact, the quotient rounded by the 1.5 * 2^23 trick (right
 // since raw / m is never within 1/(2m) of a half integer for odd m, and the
 // product's error is far below that).  The low byte of r, read off the bit
 // pattern of r + 1.5 * 2^23, is r in signed 8 bits (for m = 256, r = 128 gives
-// -128, the same residue).
+// -128, the same residue).  For m = 256 the residue is D_0's low byte.
 struct Digits16 { float d[4]; };
 
-// ndig = 3: the top digit is x2 itself (|x2| <= 2^15 + 1 for p <= 47);
-// ndig = 4: x2 is split once more (|x3| <= 2^(p-48) + 1).
-__device__ __forceinline__ Digits16 digits16(double X, int ndig) {
+// NDIG = 3: the top digit is x2 itself (|x2| <= 2^15 + 1 for p <= 47);
+// NDIG = 4: x2 is split once more (|x3| <= 2^(p-48) + 1).
+template <int NDIG>
+__device__ __forceinline__ Digits16 digits16(double X) {
   Digits16 g;
   const double x1 = rint(X * (1.0 / 65536.0));
   g.d[0] = (float)fma(-x1, 65536.0, X);
   const double x2 = rint(x1 * (1.0 / 65536.0));
   g.d[1] = (float)fma(-x2, 65536.0, x1);
-  if (ndig > 3) {
+  if constexpr (NDIG > 3) {
     const double x3 = rint(x2 * (1.0 / 65536.0));
     g.d[2] = (float)fma(-x3, 65536.0, x2);
     g.d[3] = (float)x3;
@@ -177,21 +193,47 @@ __device__ __forceinline__ Digits16 digits16(double X, int ndig) {
   return g;
 }
 
-__device__ __forceinline__ uint32_t residue_byte(const Digits16& g, const ResidueSpec& S, int i) {
+// r + 1.5 * 2^23 for modulus I: the low byte of its bit pattern is the residue
+template <int NDIG, int I>
+__device__ __forceinline__ float residue_shifted(const Digits16& g) {
   constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
-  float raw = g.d[0] * S.cdig[i][0];
-  raw = fmaf(g.d[1], S.cdig[i][1], raw);
-  raw = fmaf(g.d[2], S.cdig[i][2], raw);
-  if (S.ndig > 3) raw = fmaf(g.d[3], S.cdig[i][3], raw);
-  const float q = fmaf(raw, S.invf[i], kMagic) - kMagic;
-  const float r = fmaf(-q, S.modf[i], raw);
-  return (uint32_t)__float_as_int(r + kMagic) & 0xFFu;
+  constexpr int m = residue_modulus(I);
+  if constexpr (m == 256) {
+    return g.d[0] + kMagic;
+  } else {
+    constexpr float mf = (float)m, inv = 1.0f / (float)m;
+    constexpr float c1 = (float)residue_cdig(I, 1), c2 = (float)residue_cdig(I, 2), c3 = (float)residue_cdig(I, 3);
+    float raw = fmaf(g.d[1], c1, g.d[0]);
+    raw = fmaf(g.d[2], c2, raw);
+    if constexpr (NDIG > 3) raw = fmaf(g.d[3], c3, raw);
+    const float q = fmaf(raw, inv, kMagic) - kMagic;
+    return fmaf(-q, mf, raw) + kMagic;
+  }
 }
 
-// Residue i of four values, packed little-endian.
-__device__ __forceinline__ uint32_t residue4(const Digits16 (&g)[4], const ResidueSpec& S, int i) {
-  return residue_byte(g[0], S, i) | (residue_byte(g[1], S, i) << 8) | (residue_byte(g[2], S, i) << 16) |
-         (residue_byte(g[3], S, i) << 24);
+// low bytes of four words, packed little-endian
+__device__ __forceinline__ uint32_t pack_low_bytes(float a, float b, float c, float d) {
+  const uint32_t lo = __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x0040);
+  const uint32_t hi = __byte_perm(__float_as_uint(c), __float_as_uint(d), 0x0040);
+  return __byte_perm(lo, hi, 0x5410);
+}
+
+// Residue I of four values, packed little-endian.
+template <int NDIG, int I>
+__device__ __forceinline__ uint32_t residue4(const Digits16 (&g)[4]) {
+  return pack_low_bytes(residue_shifted<NDIG, I>(g[0]), residue_shifted<NDIG, I>(g[1]),
+                        residue_shifted<NDIG, I>(g[2]), residue_shifted<NDIG, I>(g[3]));
+}
+
+// f(integral_constant<int, I>) for I = I0 .. min(n, N) - 1 (n uniform)
+template <int I, int N, class F>
+__device__ __forceinline__ void for_moduli(int n, F&& f) {
+  if constexpr (I < N) {
+    if (I < n) {
+      f(std::integral_constant<int, I>{});
+      for_moduli<I + 1, N>(n, f);
+    }
+  }
 }
 
 // Slices of x in (-1/2, 1/2): balanced signed base-256 digits of the fixed-point
@@ -214,7 +256,7 @@ __device__ __forceinline__ uint32_t slice4(long long y0, long long y1, long long
          flip;
 }
 
-template <int MODE>
+template <int MODE, int NDIG = 3>
 __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowtile, int ky, int kstep) {
   constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B ||
                         MODE == G_RESID_C8A || MODE == G_RESID_C8B;
@@ -272,10 +314,12 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           const int se = sm_se[mm];
           Digits16 g[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) g[t] = digits16(floor(scale2(tile[mm][kq + t], se) * P.rs.pscale), P.rs.ndig);
+          for (int t = 0; t < 4; ++t) g[t] = digits16<NDIG>(floor(scale2(tile[mm][kq + t], se) * P.rs.pscale));
           int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
-#pragma unroll 1
-          for (int i = 0; i < P.rs.n; ++i) *reinterpret_cast<uint32_t*>(base + i * P.pstride) = residue4(g, P.rs, i);
+          for_moduli<0, kMaxModuli>(P.rs.n, [&](auto ic) {
+            constexpr int I = decltype(ic)::value;
+            *reinterpret_cast<uint32_t*>(base + I * P.pstride) = residue4<NDIG, I>(g);
+          });
         } else if constexpr (MODE == G_RESID_C8A) {
           // A' row m: (re, im) interleaved along K
           const int se = sm_se[mm];
@@ -283,15 +327,16 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
 #pragma unroll
           for (int t = 0; t < 2; ++t) {
             const E v0 = tile[mm][kq + t], v1 = tile[mm][kq + 2 + t];
-            ga[2 * t] = digits16(floor(scale2(v0.x, se) * P.rs.pscale), P.rs.ndig);
-            ga[2 * t + 1] = digits16(floor(scale2(P.isign * v0.y, se) * P.rs.pscale), P.rs.ndig);
-            gb[2 * t] = digits16(floor(scale2(v1.x, se) * P.rs.pscale), P.rs.ndig);
-            gb[2 * t + 1] = digits16(floor(scale2(P.isign * v1.y, se) * P.rs.pscale), P.rs.ndig);
+            ga[2 * t] = digits16<NDIG>(floor(scale2(v0.x, se) * P.rs.pscale));
+            ga[2 * t + 1] = digits16<NDIG>(floor(scale2(P.isign * v0.y, se) * P.rs.pscale));
+            gb[2 * t] = digits16<NDIG>(floor(scale2(v1.x, se) * P.rs.pscale));
+            gb[2 * t + 1] = digits16<NDIG>(floor(scale2(P.isign * v1.y, se) * P.rs.pscale));
           }
           int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
-#pragma unroll 1
-          for (int i = 0; i < P.rs.n; ++i)
-            *reinterpret_cast<uint2*>(base + i * P.pstride) = make_uint2(residue4(ga, P.rs, i), residue4(gb, P.rs, i));
+          for_moduli<0, kMaxModuli>(P.rs.n, [&](auto ic) {
+            constexpr int I = decltype(ic)::value;
+            *reinterpret_cast<uint2*>(base + I * P.pstride) = make_uint2(residue4<NDIG, I>(ga), residue4<NDIG, I>(gb));
+          });
         } else if constexpr (MODE == G_RESID_C8B) {
           // B' rows 2n = (re, -im), 2n+1 = (im, re) interleaved along K
           const int se = sm_se[mm];
@@ -300,19 +345,21 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           for (int t = 0; t < 4; ++t) {
             const E v = tile[mm][kq + t];
             const double im = scale2(P.isign * v.y, se);
-            R[t] = digits16(floor(scale2(v.x, se) * P.rs.pscale), P.rs.ndig);
-            I[t] = digits16(floor(im * P.rs.pscale), P.rs.ndig);
-            NI[t] = digits16(floor(-im * P.rs.pscale), P.rs.ndig);
+            R[t] = digits16<NDIG>(floor(scale2(v.x, se) * P.rs.pscale));
+            I[t] = digits16<NDIG>(floor(im * P.rs.pscale));
+            NI[t] = digits16<NDIG>(floor(-im * P.rs.pscale));
           }
           const Digits16 r0a[4] = {R[0], NI[0], R[1], NI[1]}, r0b[4] = {R[2], NI[2], R[3], NI[3]};
           const Digits16 r1a[4] = {I[0], R[0], I[1], R[1]}, r1b[4] = {I[2], R[2], I[3], R[3]};
           int8_t* b0 = (int8_t*)P.planes + (2 * m) * P.kpad + 2 * k;
           int8_t* b1 = b0 + P.kpad;
-#pragma unroll 1
-          for (int i = 0; i < P.rs.n; ++i) {
-            *reinterpret_cast<uint2*>(b0 + i * P.pstride) = make_uint2(residue4(r0a, P.rs, i), residue4(r0b, P.rs, i));
-            *reinterpret_cast<uint2*>(b1 + i * P.pstride) = make_uint2(residue4(r1a, P.rs, i), residue4(r1b, P.rs, i));
-          }
+          for_moduli<0, kMaxModuli>(P.rs.n, [&](auto ic) {
+            constexpr int J = decltype(ic)::value;
+            *reinterpret_cast<uint2*>(b0 + J * P.pstride) =
+                make_uint2(residue4<NDIG, J>(r0a), residue4<NDIG, J>(r0b));
+            *reinterpret_cast<uint2*>(b1 + J * P.pstride) =
+                make_uint2(residue4<NDIG, J>(r1a), residue4<NDIG, J>(r1b));
+          });
         } else if constexpr (MODE == G_SLICE_R8) {
           const int se = sm_se[mm];
           long long X[4];
@@ -412,9 +459,12 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kGThreads, 3) gather_kernel(const __grid_constant__ GatherParams P) {
-  gather_body<MODE>(P, blockIdx.x, blockIdx.y, gridDim.y);
+// (the complex B' residue mode holds three digit sets per value: two CTAs per
+// SM leave it registers enough not to spill)
+template <int MODE, int NDIG = 3>
+__global__ void __launch_bounds__(kGThreads, MODE == G_RESID_C8B ? 2 : 3)
+    gather_kernel(const __grid_constant__ GatherParams P) {
+  gather_body<MODE, NDIG>(P, blockIdx.x, blockIdx.y, gridDim.y);
 }
 
 // Grouped form: CTA x works on row tile map[x].y of job map[x].x.
@@ -742,7 +792,14 @@ int run_gather(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStr
   // enough CTAs to fill the GPU several times over; each walks a strided set of K tiles
   int64_t gy = std::max<int64_t>(1, std::min<int64_t>(grid_k, (int64_t)num_sms() * 16 / std::max<int64_t>(1, grid_rows)));
   gy = std::min<int64_t>(gy, 65535);
-  gather_kernel<MODE><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+  if constexpr (MODE == G_RESID_R8 || MODE == G_RESID_C8A || MODE == G_RESID_C8B) {
+    if (P.rs.ndig > 3)
+      gather_kernel<MODE, 4><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+    else
+      gather_kernel<MODE, 3><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+  } else {
+    gather_kernel<MODE><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+  }
   TB_CHECK_LAUNCH();
   return 0;
 }
