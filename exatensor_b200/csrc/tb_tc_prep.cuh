@@ -577,10 +577,6 @@ __global__ void __launch_bounds__(256) nonfinite_fixup_kernel(const __grid_const
 }
 
 
-// Row maxima of the FP64 exponent fields (the slice scales), streamed without
-// shared-memory staging: each thread keeps the running maximum of the rows it
-// touches in registers over all K tiles of its CTA, and the CTA merges them once
-// at the end.  Thread -> (row, k) mapping as in gather_kernel.
 // ---- Ozaki scheme II reconstruction (Chinese remainder theorem) ------------------
 // With M = prod m_i, M_i = M / m_i and y_i = M_i^-1 mod m_i, the exact integer
 // dot product is C = sum_i t_i M_i mod M, t_i = (r_i y_i) mod m_i, taken in the
@@ -691,6 +687,10 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
   }
 }
 
+// Row maxima of the FP64 exponent fields (the slice scales), streamed without
+// shared-memory staging: each thread keeps the running maximum of the rows it
+// touches in registers over all K tiles of its CTA, and the CTA merges them once
+// at the end.  Thread -> (row, k) mapping as in gather_kernel.
 template <bool CPLX>
 __device__ __forceinline__ void rowmax_body(const GatherParams& P, int64_t rowtile, int ky, int kstep) {
   using E = typename std::conditional<CPLX, double2, double>::type;

@@ -217,6 +217,60 @@ int tb_bsc_autotune(tb_bsc_plan_t* plan, void* stream);
 int tb_bsc_plan_info(const tb_bsc_plan_t* plan, tb_bsc_info_t* info);
 int tb_bsc_plan_destroy(tb_bsc_plan_t* plan);
 
+/* ---- block-task lists from segment metadata --------------------------------
+ * A block-sparse tensor splits index k into nseg[k] segments of extents
+ * seg_ext (all indices' segments concatenated, index 0 first); a present block
+ * is one segment number per index (keys, nblocks x rank, index 0 first) with
+ * its dense body (dlf layout) in device memory. */
+typedef struct {
+  int rank;
+  const int* nseg;       /* [rank] */
+  const int* seg_ext;    /* [sum of nseg] */
+  int nblocks;
+  const int* keys;       /* [nblocks][rank] */
+  void* const* bodies;   /* [nblocks] */
+} tb_block_list_t;
+
+/* The block tasks of the contraction `pattern` over block-sparse D, L and R:
+ * every (L block, R block) pair whose contracted segments agree, with the D
+ * block their uncontracted segments name (pairs whose D block is absent give
+ * no task).  Replaces the matching of TensContractionSplitFunc
+ * (INTRAVIRT/tensor_recursive.F90:9202-9784), whose sub-contraction list
+ * TAVP-WRK executes block by block (INTERVIRT/tavp_worker.F90:9420).  Writes
+ * at most max_tasks tasks and the total count to *ntasks; tasks = NULL,
+ * max_tasks = 0 only counts.  Errors: segmentations that differ between the
+ * tensors carrying an index, out-of-range segment numbers, repeated D keys
+ * (TB_ERR_INVALID_ARGS); too small an array (TB_ERR_LIMIT, *ntasks = the
+ * count).  Host code only: no device work. */
+int tb_bsc_tasks_from_blocks(const char* pattern, const tb_block_list_t* d, const tb_block_list_t* l,
+                             const tb_block_list_t* r, int max_tasks, tb_block_task_t* tasks, int* ntasks);
+
+/* ---- caller-side batching ------------------------------------------------
+ * Collects block contractions (one pattern, data kind, alpha and
+ * accumulation) that a caller would issue one by one -- TAVP-WRK's
+ * talsh_tensor_contract per block (INTERVIRT/tavp_worker.F90:9467) -- and
+ * runs them at flush time as one grouped launch (R8, R4: tb_bsc_plan_create
+ * and tb_bsc_execute), or as a loop of tb_tensor_contract_str calls for the
+ * data kinds the grouped kernel does not take.  A flushed list equal to one
+ * flushed before (same tasks, same order) reuses its plan and CUDA graph; on
+ * its second use the plan's tile and slice choice is timed once.  The
+ * accumulative flag applies to each output block once per flush.  Blocks
+ * must stay allocated while a cached plan may run them. */
+typedef struct tb_batch_s tb_batch_t;
+typedef struct {
+  long long tasks;         /* tasks flushed */
+  int grouped_flushes, loop_flushes, plans_built, plan_reuses, autotunes, cached_plans;
+} tb_batch_stats_t;
+int tb_batch_create(const char* pattern, int data_kind, double alpha_real, double alpha_imag, int accumulative,
+                    const tb_plan_t* plan, tb_batch_t** out);
+int tb_batch_add(tb_batch_t* batch, int ntasks, const tb_block_task_t* tasks);
+/* Tasks queued since the last flush (-1 for a null batch). */
+int tb_batch_pending(const tb_batch_t* batch);
+int tb_batch_flush(tb_batch_t* batch, void* stream);
+int tb_batch_get_stats(const tb_batch_t* batch, tb_batch_stats_t* stats);
+/* Destroys the cached plans (after the device finishes their work). */
+int tb_batch_destroy(tb_batch_t* batch);
+
 /* ---- learned plan selection ---------------------------------------------
  * No counterpart in the reference, which always runs TTGT through cuBLAS.
  * A contraction descriptor (TB_DESC_FEATURES floats) feeds a 3-layer MLP that
