@@ -53,6 +53,18 @@ class BlockTask(C.Structure):
                 ("l_dims", C.c_int * 8), ("r_dims", C.c_int * 8)]
 
 
+class BlockList(C.Structure):
+    """tb_block_list_t: segment metadata and present blocks of a block-sparse tensor."""
+    _fields_ = [("rank", C.c_int), ("nseg", C.POINTER(C.c_int)), ("seg_ext", C.POINTER(C.c_int)),
+                ("nblocks", C.c_int), ("keys", C.POINTER(C.c_int)), ("bodies", C.POINTER(C.c_void_p))]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("tasks", C.c_longlong), ("grouped_flushes", C.c_int), ("loop_flushes", C.c_int),
+                ("plans_built", C.c_int), ("plan_reuses", C.c_int), ("autotunes", C.c_int),
+                ("cached_plans", C.c_int)]
+
+
 class BscInfo(C.Structure):
     _fields_ = [("tasks", C.c_int), ("left_blocks", C.c_int), ("right_blocks", C.c_int), ("out_blocks", C.c_int),
                 ("work_items", C.c_int), ("slices", C.c_int), ("tile_n", C.c_int), ("flops", C.c_double),
@@ -95,6 +107,15 @@ def lib() -> C.CDLL:
     L.tb_bsc_autotune.argtypes = [vp, vp]
     L.tb_bsc_plan_info.argtypes = [vp, C.POINTER(BscInfo)]
     L.tb_bsc_plan_destroy.argtypes = [vp]
+    bl = C.POINTER(BlockList)
+    L.tb_bsc_tasks_from_blocks.argtypes = [C.c_char_p, bl, bl, bl, C.c_int, C.POINTER(BlockTask), ip]
+    L.tb_batch_create.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(Plan),
+                                  C.POINTER(C.c_void_p)]
+    L.tb_batch_add.argtypes = [vp, C.c_int, C.POINTER(BlockTask)]
+    L.tb_batch_pending.argtypes = [vp]
+    L.tb_batch_flush.argtypes = [vp, vp]
+    L.tb_batch_get_stats.argtypes = [vp, C.POINTER(BatchStats)]
+    L.tb_batch_destroy.argtypes = [vp]
     fp = C.POINTER(C.c_float)
     L.tb_contract_descriptor.argtypes = [ip, C.c_int, C.c_int, ip, C.c_int, ip, C.c_int, ip, fp]
     L.tb_mlp_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]
@@ -208,6 +229,86 @@ def tensor_contract(pattern_or_cptrn, dtk, ddims, d_ptr, ldims, l_ptr, rdims, r_
                                         _stream(stream)))
 
 
+def _task_array(tasks):
+    tasks = list(tasks)
+    arr = (BlockTask * max(1, len(tasks)))()
+    for t, (dp, dd, lp, ld, rp, rd) in zip(arr, tasks):
+        t.d, t.l, t.r = dp, lp, rp
+        for k, v in enumerate(dd):
+            t.d_dims[k] = v
+        for k, v in enumerate(ld):
+            t.l_dims[k] = v
+        for k, v in enumerate(rd):
+            t.r_dims[k] = v
+    return arr, len(tasks)
+
+
+def _block_list(segments, keys, bodies):
+    """A BlockList over Python data; returns (struct, keepalive)."""
+    rank = len(segments)
+    nseg = iarr([len(s) for s in segments])
+    ext = iarr([e for s in segments for e in s])
+    flat = iarr([x for k in keys for x in k])
+    bod = (C.c_void_p * max(1, len(bodies)))(*[int(b) for b in bodies])
+    bl = BlockList(rank, nseg, ext, len(keys), flat, bod)
+    return bl, (nseg, ext, flat, bod)
+
+
+def bsc_tasks_from_blocks(pattern, d, l, r):
+    """Block tasks of a block-sparse contraction from segment metadata (see
+    tb_bsc_tasks_from_blocks).  d, l, r: (segments, keys, bodies) with
+    segments[k] the extents of index k's segments, keys the present blocks'
+    segment numbers and bodies their device addresses.  Returns a list of
+    (d_ptr, d_dims, l_ptr, l_dims, r_ptr, r_dims)."""
+    (bd, kd), (bl_, kl), (br, kr) = _block_list(*d), _block_list(*l), _block_list(*r)
+    n = C.c_int()
+    _check(lib().tb_bsc_tasks_from_blocks(pattern.encode(), C.byref(bd), C.byref(bl_), C.byref(br), 0, None,
+                                          C.byref(n)))
+    arr = (BlockTask * max(1, n.value))()
+    _check(lib().tb_bsc_tasks_from_blocks(pattern.encode(), C.byref(bd), C.byref(bl_), C.byref(br), n.value, arr,
+                                          C.byref(n)))
+    dr, lr, rr = len(d[0]), len(l[0]), len(r[0])
+    return [(t.d, list(t.d_dims[:dr]), t.l, list(t.l_dims[:lr]), t.r, list(t.r_dims[:rr])) for t in arr[:n.value]]
+
+
+class Batch:
+    """Caller-side batch of block contractions (tb_batch_*): add tasks one by
+    one or in groups, flush them as one grouped launch."""
+
+    def __init__(self, pattern, dtk, alpha=1.0, accumulative=True, plan: Plan | None = None):
+        a = complex(alpha)
+        h = C.c_void_p()
+        _check(lib().tb_batch_create(pattern.encode(), dtk, a.real, a.imag, int(accumulative),
+                                     C.byref(plan) if plan is not None else None, C.byref(h)))
+        self._h = h
+
+    def add(self, tasks):
+        arr, n = _task_array(tasks)
+        _check(lib().tb_batch_add(self._h, n, arr))
+
+    def pending(self) -> int:
+        return lib().tb_batch_pending(self._h)
+
+    def flush(self, stream=None):
+        _check(lib().tb_batch_flush(self._h, _stream(stream)))
+
+    def stats(self) -> BatchStats:
+        st = BatchStats()
+        _check(lib().tb_batch_get_stats(self._h, C.byref(st)))
+        return st
+
+    def close(self):
+        if self._h:
+            lib().tb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BlockSparsePlan:
     """A block-sparse contraction (list of block tasks under one pattern) run as
     one grouped tensor-core launch; see tb_bsc_plan_create.
@@ -215,19 +316,10 @@ class BlockSparsePlan:
     tasks: iterable of (d_ptr, d_dims, l_ptr, l_dims, r_ptr, r_dims)."""
 
     def __init__(self, pattern, dtk, tasks, alpha=1.0, accumulative=True, plan: Plan | None = None, stream=None):
-        tasks = list(tasks)
-        arr = (BlockTask * len(tasks))()
-        for t, (dp, dd, lp, ld, rp, rd) in zip(arr, tasks):
-            t.d, t.l, t.r = dp, lp, rp
-            for k, v in enumerate(dd):
-                t.d_dims[k] = v
-            for k, v in enumerate(ld):
-                t.l_dims[k] = v
-            for k, v in enumerate(rd):
-                t.r_dims[k] = v
+        arr, n = _task_array(tasks)
         a = complex(alpha)
         h = C.c_void_p()
-        _check(lib().tb_bsc_plan_create(pattern.encode(), dtk, len(tasks), arr, a.real, a.imag, int(accumulative),
+        _check(lib().tb_bsc_plan_create(pattern.encode(), dtk, n, arr, a.real, a.imag, int(accumulative),
                                         C.byref(plan) if plan is not None else None, C.byref(h), _stream(stream)))
         self._h = h
 

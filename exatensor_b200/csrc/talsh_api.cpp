@@ -9,6 +9,7 @@
 // Host requests return TALSH_NOT_AVAILABLE: nothing computes on the CPU.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1022,6 +1023,164 @@ int contract_streamed(const tb::ParsedPattern& P, const SliceSpec& sp, int dtk, 
   return err;
 }
 
+// Output decomposition for talshTensorContractXL.  TAL-SH's XL contraction
+// halves the largest dimension of the operation until its arguments fit the
+// device buffer (talshTensorOpDecompose2, talshc.cpp:3150) and runs the parts
+// one by one (ContractXL :5394-5642).  Here, when D, L and R live only on the
+// host and the contraction with its scratch would not fit in the device
+// budget, D is cut along its largest dimension (the slowest of equal ones):
+//   - that index belongs to one input, X; the other input, Y, moves to the
+//     GPU once and stays;
+//   - each D slab and the matching X slab move in (D only when accumulating)
+//     on the copy stream, are contracted on the compute stream, and D's slab
+//     moves back on the copy stream, through two buffer sets, so that the
+//     transfers of one slab overlap the contraction of the other;
+//   - slabs are 2-D strided copies: inner dims x slab extent, times outer dims.
+// Every D element is computed whole by one sub-contraction (its K sum is not
+// split), with the same method choice as any contraction.  The budget is
+// TB_XL_DEVICE_MB when set, else 80% of the GPU's free memory; the
+// contraction's scratch is counted as twice its operands.
+struct DSplit {
+  int dpos = -1;           // sliced position of D
+  int xop = 0, xpos = -1;  // input carrying it (1 = L, 2 = R) and its position there
+  int64_t ext = 0, step = 0;
+};
+
+thread_local DSplit g_last_split;
+
+bool slab_pitch_ok(const int* dims, int rank, int pos, int64_t es) {
+  return prod_dims(dims, pos + 1, rank) == 1 || prod_dims(dims, 0, pos + 1) * es < ((int64_t)1 << 31);
+}
+
+DSplit plan_out_of_core(const tb::ParsedPattern& P, const talsh_tens_t* d, const talsh_tens_t* l,
+                        const talsh_tens_t* r, int dtk, int gpu) {
+  DSplit sp;
+  if (P.hyper || P.drank < 1) return sp;
+  if (!host_only(d, dtk, gpu) || !host_only(l, dtk, gpu) || !host_only(r, dtk, gpu)) return sp;
+  int64_t budget = 0;
+  if (const char* mb = std::getenv("TB_XL_DEVICE_MB")) {
+    budget = (int64_t)std::atoll(mb) << 20;
+  } else {
+    size_t fr = 0, tot = 0;
+    cudaSetDevice(gpu);
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); return sp; }
+    budget = (int64_t)(0.8 * (double)fr);
+  }
+  const int64_t es = elem_size(dtk);
+  const int64_t db = (int64_t)volume_of(d) * es, lb = (int64_t)volume_of(l) * es, rb = (int64_t)volume_of(r) * es;
+  if (3 * (db + lb + rb) <= budget) return sp;  // fits whole
+  const int* dd = d->shape_p->dims;
+  for (int p = 0; p < P.drank; ++p)
+    if (dd[p] >= 2 && (sp.dpos < 0 || dd[p] >= dd[sp.dpos])) sp.dpos = p;
+  if (sp.dpos < 0) return DSplit();
+  for (int i = 0; i < P.lrank; ++i)
+    if (P.cptrn[i] == sp.dpos + 1) { sp.xop = 1; sp.xpos = i; }
+  for (int j = 0; j < P.rrank; ++j)
+    if (P.cptrn[P.lrank + j] == sp.dpos + 1) { sp.xop = 2; sp.xpos = j; }
+  if (!sp.xop) return DSplit();
+  const talsh_tens_t* x = sp.xop == 1 ? l : r;
+  const int xrank = sp.xop == 1 ? P.lrank : P.rrank;
+  if (!slab_pitch_ok(dd, P.drank, sp.dpos, es) || !slab_pitch_ok(x->shape_p->dims, xrank, sp.xpos, es))
+    return DSplit();
+  sp.ext = dd[sp.dpos];
+  const int64_t yb = sp.xop == 1 ? rb : lb, xb = sp.xop == 1 ? lb : rb;
+  const int64_t per = (db + xb) / sp.ext;  // D and X bytes per unit of the sliced extent
+  // resident: Y + two slab sets; scratch of one sub-contraction: twice its operands
+  const int64_t room = budget - 3 * yb;
+  if (per <= 0 || room < 5 * per) return DSplit();
+  sp.step = std::min<int64_t>(room / (5 * per), (sp.ext + 1) / 2);
+  return sp;
+}
+
+cudaError_t copy_slab(void* dev, char* host, int64_t inner, int64_t ext, int64_t outer, int64_t x0, int64_t w,
+                      int64_t es, bool to_dev, cudaStream_t st) {
+  const size_t width = (size_t)(inner * w * es), pitch = (size_t)(inner * ext * es);
+  char* h = host + x0 * inner * es;
+  if (outer == 1)
+    return to_dev ? cudaMemcpyAsync(dev, h, width, cudaMemcpyHostToDevice, st)
+                  : cudaMemcpyAsync(h, dev, width, cudaMemcpyDeviceToHost, st);
+  return to_dev ? cudaMemcpy2DAsync(dev, width, h, pitch, width, (size_t)outer, cudaMemcpyHostToDevice, st)
+                : cudaMemcpy2DAsync(h, pitch, dev, width, width, (size_t)outer, cudaMemcpyDeviceToHost, st);
+}
+
+int contract_out_of_core(const tb::ParsedPattern& P, const DSplit& sp, int dtk, talsh_tens_t* dtens,
+                         talsh_tens_t* ltens, talsh_tens_t* rtens, double sr, double si, int accumulative,
+                         const tb_plan_t* plan, cudaStream_t s, std::vector<Operand>& o) {
+  int g = 0;
+  cudaGetDevice(&g);
+  if (!g_dev[g].xstream && cudaStreamCreateWithFlags(&g_dev[g].xstream, cudaStreamNonBlocking) != cudaSuccess)
+    return TALSH_FAILURE;
+  cudaStream_t xs = g_dev[g].xstream;
+  const int64_t es = elem_size(dtk);
+  talsh_tens_t* xt = sp.xop == 1 ? ltens : rtens;
+  talsh_tens_t* yt = sp.xop == 1 ? rtens : ltens;
+  char* dh = (char*)dtens->dev_rsc[o[0].src].gmem_p;
+  char* xh = (char*)xt->dev_rsc[o[sp.xop].src].gmem_p;
+  const char* yh = (const char*)yt->dev_rsc[o[3 - sp.xop].src].gmem_p;
+  const int xrank = sp.xop == 1 ? P.lrank : P.rrank;
+  int dd[MAX_TENSOR_RANK], xd[MAX_TENSOR_RANK];
+  std::memcpy(dd, dtens->shape_p->dims, sizeof(int) * P.drank);
+  std::memcpy(xd, xt->shape_p->dims, sizeof(int) * xrank);
+  const int64_t din = prod_dims(dd, 0, sp.dpos), dout = prod_dims(dd, sp.dpos + 1, P.drank);
+  const int64_t xin = prod_dims(xd, 0, sp.xpos), xout = prod_dims(xd, sp.xpos + 1, xrank);
+  const size_t dslab = (size_t)(din * sp.step * dout * es), xslab = (size_t)(xin * sp.step * xout * es);
+  const size_t ybytes = volume_of(yt) * es;
+  void* yb = nullptr;
+  void* db[2] = {nullptr, nullptr};
+  void* xb[2] = {nullptr, nullptr};
+  cudaEvent_t ev[8] = {};  // ready[2], computed[2], freed[2], start, copies_done
+  int err = alloc_on(flat_gpu(g), ybytes, &yb, s);
+  for (int i = 0; i < 2 && !err; ++i) {
+    if ((err = alloc_on(flat_gpu(g), dslab, &db[i], s))) break;
+    err = alloc_on(flat_gpu(g), xslab, &xb[i], s);
+  }
+  for (int i = 0; i < 8 && !err; ++i)
+    if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) err = TALSH_FAILURE;
+  cudaEvent_t *ready = ev, *computed = ev + 2, *freed = ev + 4, start = ev[6], copies_done = ev[7];
+  const int64_t nsl = (sp.ext + sp.step - 1) / sp.step;
+  if (!err) {
+    cudaEventRecord(start, s);  // buffers allocated (stream-ordered on s)
+    cudaStreamWaitEvent(xs, start, 0);
+    if (cudaMemcpyAsync(yb, yh, ybytes, cudaMemcpyHostToDevice, xs) != cudaSuccess) err = TALSH_FAILURE;
+    for (int64_t k = 0; k < nsl && !err; ++k) {
+      const int slot = (int)(k & 1);
+      const int64_t x0 = k * sp.step, w = std::min(sp.step, sp.ext - x0);
+      if (k >= 2) cudaStreamWaitEvent(xs, freed[slot], 0);
+      if (copy_slab(xb[slot], xh, xin, sp.ext, xout, x0, w, es, true, xs) != cudaSuccess) { err = TALSH_FAILURE; break; }
+      const cudaError_t ce = accumulative ? copy_slab(db[slot], dh, din, sp.ext, dout, x0, w, es, true, xs)
+                                          : cudaMemsetAsync(db[slot], 0, (size_t)(din * w * dout * es), xs);
+      if (ce != cudaSuccess) { err = TALSH_FAILURE; break; }
+      cudaEventRecord(ready[slot], xs);
+      cudaStreamWaitEvent(s, ready[slot], 0);
+      dd[sp.dpos] = (int)w;
+      xd[sp.xpos] = (int)w;
+      const void* lp = sp.xop == 1 ? xb[slot] : yb;
+      const void* rp = sp.xop == 1 ? yb : xb[slot];
+      const int* ldims = sp.xop == 1 ? xd : ltens->shape_p->dims;
+      const int* rdims = sp.xop == 1 ? rtens->shape_p->dims : xd;
+      err = map_tb(tb_tensor_contract(P.cptrn, dtk, P.drank, dd, db[slot], P.lrank, ldims, lp, P.rrank, rdims, rp, sr,
+                                      si, P.conj_bits, accumulative, plan, s));
+      cudaEventRecord(computed[slot], s);
+      cudaStreamWaitEvent(xs, computed[slot], 0);
+      if (!err && copy_slab(db[slot], dh, din, sp.ext, dout, x0, w, es, false, xs) != cudaSuccess) err = TALSH_FAILURE;
+      cudaEventRecord(freed[slot], xs);
+    }
+    cudaEventRecord(copies_done, xs);
+    cudaStreamWaitEvent(s, copies_done, 0);
+  }
+  if (err) cudaGetLastError();
+  if (yb) cudaFreeAsync(yb, s);
+  for (int i = 0; i < 2; ++i) {
+    if (db[i]) cudaFreeAsync(db[i], s);
+    if (xb[i]) cudaFreeAsync(xb[i], s);
+  }
+  cudaStreamSynchronize(s);
+  for (auto& e : ev) if (e) cudaEventDestroy(e);
+  g_last_split = sp;
+  if (!err) g_last_split.step = nsl;  // reported: the number of slabs
+  return err;
+}
+
 }  // namespace
 
 extern "C" int talshTensorContract(const char* cptrn, talsh_tens_t* dtens, talsh_tens_t* ltens, talsh_tens_t* rtens,
@@ -1066,10 +1225,47 @@ extern "C" int talshTensorContract(const char* cptrn, talsh_tens_t* dtens, talsh
 
 extern "C" int talshTensorContractXL(const char* cptrn, talsh_tens_t* dtens, talsh_tens_t* ltens, talsh_tens_t* rtens,
                                      double sr, double si, int dev_id, int dev_kind, int accumulative) {
-  // The XL form is a blocking contraction (talshc.cpp:5394).  Host-resident
-  // inputs of 1 GiB and more stream through the GPU in slices (see
-  // contract_streamed), so they need not fit in HBM; D is staged whole.
+  // The XL form is a blocking contraction (talshc.cpp:5394).  When D, L and R
+  // live on the host and would not fit in the device budget together, D is
+  // decomposed into slabs (contract_out_of_core); otherwise host-resident
+  // inputs of 1 GiB and more stream through the GPU in slices
+  // (contract_streamed) and D is staged whole.
+  g_last_split = DSplit();
+  if (!cptrn || !dtens || !ltens || !rtens) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(dtens) == YEP || talshTensorIsEmpty(ltens) == YEP || talshTensorIsEmpty(rtens) == YEP)
+    return TALSH_OBJECT_IS_EMPTY;
+  tb::ParsedPattern P;
+  if (tb::parse_pattern(cptrn, &P) || P.rrank < 0) return TALSH_INVALID_ARGS;
+  if (P.drank != dtens->shape_p->num_dim || P.lrank != ltens->shape_p->num_dim || P.rrank != rtens->shape_p->num_dim)
+    return TALSH_INVALID_ARGS;
+  const int dtk = data_kind_of(dtens);
+  int gpu = -1;
+  DSplit sp;
+  if (!P.hyper && dtk == data_kind_of(ltens) && dtk == data_kind_of(rtens) && !resolve_gpu(dev_id, dev_kind, &gpu)) {
+    tb::Matricization Z;
+    if (!tb::matricize(P.cptrn, P.drank, dtens->shape_p->dims, P.lrank, ltens->shape_p->dims, P.rrank,
+                       rtens->shape_p->dims, &Z))
+      sp = plan_out_of_core(P, dtens, ltens, rtens, dtk, gpu);
+    if (sp.dpos >= 0) {
+      const double flops = ((dtk == C4 || dtk == C8) ? 8.0 : 2.0) * (double)Z.M * (double)Z.N * (double)Z.K;
+      const std::vector<char> sliced{1, 1, 1};
+      return run_op({dtens, ltens, rtens}, COPY_MTT, dev_id, dev_kind, nullptr,
+                    [&](cudaStream_t s, std::vector<Operand>& o) {
+                      int g = 0; cudaGetDevice(&g);
+                      tb_plan_t plan; std::memset(&plan, 0, sizeof(plan));
+                      plan.method = g_dev[g].fast_math ? TB_METHOD_AUTO : TB_METHOD_TTGT;
+                      return contract_out_of_core(P, sp, dtk, dtens, ltens, rtens, sr, si, accumulative, &plan, s, o);
+                    }, flops, &sliced);
+    }
+  }
   return talshTensorContract(cptrn, dtens, ltens, rtens, sr, si, dev_id, dev_kind, COPY_MTT, accumulative, nullptr);
+}
+
+extern "C" int tb_xl_last_split(int* d_dim, int* slabs) {
+  if (!d_dim || !slabs) return TB_ERR_INVALID_ARGS;
+  *d_dim = g_last_split.dpos;
+  *slabs = g_last_split.dpos >= 0 ? (int)g_last_split.step : 0;
+  return 0;
 }
 
 extern "C" int talshTensorGetScalar(talsh_tens_t* t, double* sr, double* si) {

@@ -57,6 +57,7 @@ def api() -> C.CDLL:
         L.talshTensorAdd.argtypes = [C.c_char_p, vp, vp, d, d, ip, ip, ip, vp]
         L.talshTensorContract.argtypes = [C.c_char_p, vp, vp, vp, d, d, ip, ip, ip, ip, vp]
         L.talshTensorContractXL.argtypes = [C.c_char_p, vp, vp, vp, d, d, ip, ip, ip]
+        L.tb_xl_last_split.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.talshTaskCreate.argtypes = [C.POINTER(vp)]
         L.talshTaskDestroy.argtypes = [vp]
         L.talshTaskWait.argtypes = [vp, C.POINTER(C.c_int)]
@@ -157,6 +158,22 @@ def contract(pattern, d: Tensor, l: Tensor, r: Tensor, alpha=1.0, dev_id=0, dev_
     a = complex(alpha)
     return api().talshTensorContract(pattern.encode(), d.h, l.h, r.h, a.real, a.imag, dev_id, dev_kind, copy_ctrl,
                                      int(accumulative), task.h if task else None)
+
+
+def contract_xl(pattern, d: Tensor, l: Tensor, r: Tensor, alpha=1.0, dev_id=0, dev_kind=DEV_NVIDIA_GPU,
+                accumulative=True) -> int:
+    """talshTensorContractXL: a blocking contraction whose arguments may exceed
+    the GPU's memory (host-resident D, L, R are decomposed into D slabs)."""
+    a = complex(alpha)
+    return api().talshTensorContractXL(pattern.encode(), d.h, l.h, r.h, a.real, a.imag, dev_id, dev_kind,
+                                       int(accumulative))
+
+
+def xl_last_split():
+    """(D dimension, slabs) of this thread's last contract_xl; (-1, 0) if undecomposed."""
+    dd, ns = C.c_int(), C.c_int()
+    api().tb_xl_last_split(C.byref(dd), C.byref(ns))
+    return dd.value, ns.value
 
 
 def copy(pattern, d: Tensor, l: Tensor, dev_id=0, dev_kind=DEV_NVIDIA_GPU, copy_ctrl=COPY_MT, task=None) -> int:

@@ -217,6 +217,11 @@ int tb_bsc_autotune(tb_bsc_plan_t* plan, void* stream);
 int tb_bsc_plan_info(const tb_bsc_plan_t* plan, tb_bsc_info_t* info);
 int tb_bsc_plan_destroy(tb_bsc_plan_t* plan);
 
+/* Diagnostic of the calling thread's last talshTensorContractXL: the D
+ * dimension its output was decomposed along and the number of slabs, or -1
+ * and 0 when it ran undecomposed. */
+int tb_xl_last_split(int* d_dim, int* slabs);
+
 /* ---- block-task lists from segment metadata --------------------------------
  * A block-sparse tensor splits index k into nseg[k] segments of extents
  * seg_ext (all indices' segments concatenated, index 0 first); a present block

@@ -177,3 +177,58 @@ def test_streamed_contraction_uneven_slices(talsh):
     got, _ = _contract_host("D(a,b,i)+=L(a,b,k)*R(k,i)", dd, ld, rd, l, r, d0, -1.5, T.COPY_TTT, stream=True)
     ref = d0 - 1.5 * np.einsum("abk,ki->abi", _fortran(l, ld), _fortran(r, rd)).ravel(order="F")
     assert _rel(got, ref) <= 1e-13
+
+
+# ---- output decomposition (talshTensorContractXL with D beyond the budget) --
+def _contract_xl(pattern, dd, ld, rd, l, r, d0, alpha, accumulative, budget_mb, dtk=R8):
+    """talshTensorContractXL with host tensors under a device budget of
+    budget_mb (TB_XL_DEVICE_MB); returns D and the split it reported."""
+    import os
+    old = os.environ.get("TB_XL_DEVICE_MB")
+    os.environ["TB_XL_DEVICE_MB"] = str(budget_mb)
+    try:
+        d = d0.copy()
+        td, tl, tr = T.Tensor(dd, dtk, ext=d), T.Tensor(ld, dtk, ext=l), T.Tensor(rd, dtk, ext=r)
+        assert T.contract_xl(pattern, td, tl, tr, alpha, accumulative=accumulative) == 0
+        return d, T.xl_last_split()
+    finally:
+        if old is None:
+            os.environ.pop("TB_XL_DEVICE_MB", None)
+        else:
+            os.environ["TB_XL_DEVICE_MB"] = old
+
+
+@pytest.mark.parametrize("accumulative", [True, False])
+def test_xl_decomposes_the_output_beyond_the_budget(talsh, accumulative):
+    # D and L are 42 MB each, R 2.6 MB: under a 64 MB budget D is cut along
+    # b (extent 96, the slowest of the largest), which L carries
+    rng = np.random.default_rng(11)
+    v, o = 96, 24
+    ld, rd, dd = [v, v, o, o], [o, o, o, o], [v, v, o, o]
+    l = rng.uniform(-1, 1, int(np.prod(ld)))
+    r = rng.uniform(-1, 1, int(np.prod(rd)))
+    d0 = rng.uniform(-1, 1, int(np.prod(dd)))
+    pat = "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)"
+    got, split = _contract_xl(pat, dd, ld, rd, l, r, d0, 0.5, accumulative, 64)
+    assert split[0] == 1 and split[1] >= 4, split
+    prod = 0.5 * np.einsum("abcd,cdij->abij", _fortran(l, ld), _fortran(r, rd)).ravel(order="F")
+    ref = d0 + prod if accumulative else prod
+    assert _rel(got, ref) <= 1e-12
+    if accumulative:  # the undecomposed contraction of the same tensors
+        whole, _ = _contract_host(pat, dd, ld, rd, l, r, d0, 0.5, T.COPY_TTT, stream=False)
+        assert _rel(got, whole) <= 1e-12
+
+
+def test_xl_decomposes_along_the_right_operand_complex(talsh):
+    # the largest D extent (j = 80) comes from R; complex data, conjugated L
+    from exatensor_b200 import C8
+    rng = np.random.default_rng(12)
+    ld, rd, dd = [20, 30, 16], [16, 40, 80], [20, 30, 40, 80]
+    cplx = lambda n: rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    l, r = cplx(int(np.prod(ld))), cplx(int(np.prod(rd)))
+    d0 = cplx(int(np.prod(dd)))
+    pat = "D(a,b,i,j)+=L+(a,b,k)*R(k,i,j)"
+    got, split = _contract_xl(pat, dd, ld, rd, l, r, d0, 1.0, True, 24, dtk=C8)
+    assert split[0] == 3 and split[1] >= 2, split
+    ref = d0 + np.einsum("abk,kij->abij", np.conj(_fortran(l, ld)), _fortran(r, rd)).ravel(order="F")
+    assert _rel(got, ref) <= 1e-12
