@@ -1054,6 +1054,20 @@ def run_profile(args):
     if args.profile == "permsweep":
         print(json.dumps({"profile": "permsweep", **permute_sweep_repeated(X, s, s_obj, reps=max(1, args.steps))}))
         return
+    if args.profile == "permute" and args.case:
+        # one case, e.g. --case 4:37x37x37x37x37:1,3,5,4,2 (data kind : extents : O2N permutation)
+        k, dstr, pstr = args.case.split(":")
+        dtk, dims, perm = int(k), [int(x) for x in dstr.split("x")], [int(x) for x in pstr.split(",")]
+        es = X.ELEM_BYTES[dtk]
+        v = vol(dims)
+        a = torch.empty(v * es, dtype=torch.uint8, device="cuda")
+        b = torch.empty_like(a)
+        X.fill_uniform(dtk, v, a.data_ptr(), 3, stream=s)
+        ms = time_steps(lambda: X.tensor_copy(dtk, dims, perm, a.data_ptr(), b.data_ptr(), 0, s), args.steps,
+                        args.warmup, 1, s_obj)
+        print(json.dumps({"profile": "permute", "case": args.case,
+                          "GB/s": round(2.0 * v * es * args.steps / (ms / 1e3) / 1e9, 1)}))
+        return
     if args.profile == "permute":
         n = args.v or 76
         v = n ** 4
@@ -1103,6 +1117,7 @@ def main():
                                           "configs", "sweep", "peaks", "c1"],
                     default=None,
                     help="run one part on a small case for a profiler (no bench line)")
+    ap.add_argument("--case", default=None, help="--profile permute: one case, data kind:extents:permutation")
     ap.add_argument("--v", type=int, default=0, help="--profile: virtual extent (permute: n; bsc: segments per index)")
     ap.add_argument("--o", type=int, default=0, help="--profile: occupied extent (bsc: largest segment)")
     args = ap.parse_args()

@@ -142,12 +142,14 @@ int bsc_enqueue(tb_bsc_plan_s* pl, cudaStream_t s) {
     TB_CHECK_LAUNCH();
   }
   // the gathers read the slice count from the jobs: keep them in sync with the configuration
+  const cudaError_t ga = pl->i8 ? gather_grouped_prepare<G_SLICE_R8>() : gather_grouped_prepare<G_SPLIT_R4>();
+  if (ga != cudaSuccess) { set_error("grouped gather smem attribute: %s", cudaGetErrorString(ga)); return TB_ERR_CUDA; }
   if (pl->i8)
-    gather_grouped_kernel<G_SLICE_R8><<<dim3((unsigned)pl->g_ctas, (unsigned)pl->g_gy), kGThreads, 0, s>>>(pl->jobs,
-                                                                                                          pl->g_map);
+    gather_grouped_kernel<G_SLICE_R8><<<dim3((unsigned)pl->g_ctas, (unsigned)pl->g_gy), kGThreads,
+                                        gather_smem_bytes<G_SLICE_R8>(), s>>>(pl->jobs, pl->g_map);
   else
-    gather_grouped_kernel<G_SPLIT_R4><<<dim3((unsigned)pl->g_ctas, (unsigned)pl->g_gy), kGThreads, 0, s>>>(pl->jobs,
-                                                                                                          pl->g_map);
+    gather_grouped_kernel<G_SPLIT_R4><<<dim3((unsigned)pl->g_ctas, (unsigned)pl->g_gy), kGThreads,
+                                        gather_smem_bytes<G_SPLIT_R4>(), s>>>(pl->jobs, pl->g_map);
   TB_CHECK_LAUNCH();
   if (cudaMemsetAsync(pl->queue, 0, sizeof(unsigned), s) != cudaSuccess) return TB_ERR_CUDA;
   BscParams P;
@@ -317,6 +319,15 @@ int plan_create(const char* pattern, int dtk, int ntasks, const tb_block_task_t*
   auto* pl = new tb_bsc_plan_s();
   pl->dtk = dtk;
   pl->i8 = dtk == kR8;
+  {
+    // attribute set here, before any graph capture of the plan's launches
+    const cudaError_t ga = pl->i8 ? gather_grouped_prepare<G_SLICE_R8>() : gather_grouped_prepare<G_SPLIT_R4>();
+    if (ga != cudaSuccess) {
+      set_error("grouped gather smem attribute: %s", cudaGetErrorString(ga));
+      delete pl;
+      return TB_ERR_CUDA;
+    }
+  }
   pl->slices = pl->i8 ? ((plan && plan->slices >= 2 && plan->slices <= 7) ? plan->slices : 6) : 2;
   pl->max_slices = pl->i8 ? std::max(pl->slices, 6) : 2;  // planes allocated (the autotuner stays within them)
   pl->bn = (plan && plan->tile_n == 128) ? 128 : 256;

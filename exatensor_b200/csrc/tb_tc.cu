@@ -171,8 +171,10 @@ bool plan_residues(int64_t Kr, int want, ResiduePlan* out) {
     if (n > kMaxModuli) return false;
   }
   if (n < kMinModuli || n > kMaxModuli) return false;
-  // at most 52 bits: X = floor(x 2^(p+1)) must be exact in FP64
-  const int p = std::min(residue_bits(n, Kr), 52);
+  // at most 52 bits: X = x 2^(p+1) rounded to an integer must be exact in
+  // FP64; the automatic choice keeps the 46-bit target (three 16-bit digits
+  // per operand in the gathers), an explicit moduli count all its bits
+  const int p = std::min(residue_bits(n, Kr), want > 0 ? 52 : kResidueBitsTarget);
   if (p < 20) return false;
   ResiduePlan& R = *out;
   std::memset(&R, 0, sizeof(R));
@@ -185,7 +187,8 @@ bool plan_residues(int64_t Kr, int want, ResiduePlan* out) {
   R.crt.M_hi = (uint64_t)(M >> 64);
   R.crt.Md = (double)(uint64_t)(M >> 64) * 18446744073709551616.0 + (double)(uint64_t)M;
   R.crt.shift = 2 * (p + 1);
-  R.rs.ndig = p <= 47 ? 3 : 4;
+  R.rs.p = p;
+  R.rs.ndig = p <= 46 ? 3 : 4;
   for (int i = 0; i < n; ++i) {
     const int m = kModuliTable[i];
     const u128 Mi = M / (u128)m;

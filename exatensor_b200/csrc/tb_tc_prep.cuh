@@ -141,8 +141,9 @@ TB_HD constexpr int residue_cdig(int i, int j) {
 
 struct ResidueSpec {
   int n;                    // moduli: residue_modulus(0 .. n-1)
+  int p;                    // operand bits: |X| <= 2^p
   double pscale;            // 2^(p+1)
-  int ndig;                 // balanced 16-bit digits of X: 3 (p <= 47) or 4
+  int ndig;                 // balanced 16-bit digits of X: 3 (p <= 46) or 4
 };
 
 struct GatherParams {
@@ -193,21 +194,56 @@ __device__ __forceinline__ Digits16 digits16(double X) {
   return g;
 }
 
-// r + 1.5 * 2^23 for modulus I: the low byte of its bit pattern is the residue
+// Three balanced 16-bit digits of X = rint(v), |v| <= 2^46, without
+// conversions: Y = v + (1.5 * 2^52 + B), B = 2^15 (1 + 2^16 + 2^32), rounds v
+// to the nearest integer (one rounding: Y lies in [2^52, 2^53)) and leaves
+// X + B in Y's low 48 mantissa bits.  Its 16-bit fields u_j (0 <= u_j < 2^16)
+// give X = sum_j (u_j - 2^15) 2^(16 j); a field placed under the bit pattern
+// of 1.5 * 2^23 (one byte permute) is the float 1.5 * 2^23 + u_j, and one
+// subtraction gives d_j = u_j - 2^15 exactly.
+__device__ __forceinline__ Digits16 digits16_rint(double v) {
+  constexpr double kMB = 6896139076927488.0;  // 1.5 * 2^52 + 2^15 + 2^31 + 2^47
+  constexpr float kBias = 12582912.0f + 32768.0f;
+  const double Y = v + kMB;
+  const uint32_t lo = (uint32_t)__double2loint(Y), hi = (uint32_t)__double2hiint(Y);
+  Digits16 g;
+  g.d[0] = __uint_as_float(__byte_perm(lo, 0x4B400000u, 0x7610)) - kBias;
+  g.d[1] = __uint_as_float(__byte_perm(lo, 0x4B400000u, 0x7632)) - kBias;
+  g.d[2] = __uint_as_float(__byte_perm(hi, 0x4B400000u, 0x7610)) - kBias;
+  g.d[3] = 0.f;
+  return g;
+}
+
+// Digits of one operand value x of a row with scale exponent se: X = rint(x
+// 2^(se + p + 1)) for NDIG = 3 (sc = 2^(se + p + 1) when that is a double,
+// else 0), floor of the same for NDIG = 4.  Both are integers with |X| <= 2^p.
+template <int NDIG>
+__device__ __forceinline__ Digits16 operand_digits(double x, int se, double sc, double pscale) {
+  if constexpr (NDIG == 3) {
+    return digits16_rint(sc != 0.0 ? x * sc : scale2(x, se) * pscale);
+  } else {
+    return digits16<NDIG>(floor(scale2(x, se) * pscale));
+  }
+}
+
+// r + 1.5 * 2^23 for modulus I of two values at once (packed FP32 pairs,
+// each component rounded as fmaf / __fadd_rn): the low byte of each
+// component's bit pattern is its residue
 template <int NDIG, int I>
-__device__ __forceinline__ float residue_shifted(const Digits16& g) {
+__device__ __forceinline__ float2 residue_shifted2(const float2 (&d)[4]) {
   constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
   constexpr int m = residue_modulus(I);
+  const float2 magic = make_float2(kMagic, kMagic);
   if constexpr (m == 256) {
-    return g.d[0] + kMagic;
+    return __fadd2_rn(d[0], magic);
   } else {
-    constexpr float mf = (float)m, inv = 1.0f / (float)m;
+    constexpr float negm = -(float)m, inv = 1.0f / (float)m;
     constexpr float c1 = (float)residue_cdig(I, 1), c2 = (float)residue_cdig(I, 2), c3 = (float)residue_cdig(I, 3);
-    float raw = fmaf(g.d[1], c1, g.d[0]);
-    raw = fmaf(g.d[2], c2, raw);
-    if constexpr (NDIG > 3) raw = fmaf(g.d[3], c3, raw);
-    const float q = fmaf(raw, inv, kMagic) - kMagic;
-    return fmaf(-q, mf, raw) + kMagic;
+    float2 raw = __ffma2_rn(d[1], make_float2(c1, c1), d[0]);
+    raw = __ffma2_rn(d[2], make_float2(c2, c2), raw);
+    if constexpr (NDIG > 3) raw = __ffma2_rn(d[3], make_float2(c3, c3), raw);
+    const float2 q = __fadd2_rn(__ffma2_rn(raw, make_float2(inv, inv), magic), make_float2(-kMagic, -kMagic));
+    return __fadd2_rn(__ffma2_rn(q, make_float2(negm, negm), raw), magic);
   }
 }
 
@@ -221,8 +257,14 @@ __device__ __forceinline__ uint32_t pack_low_bytes(float a, float b, float c, fl
 // Residue I of four values, packed little-endian.
 template <int NDIG, int I>
 __device__ __forceinline__ uint32_t residue4(const Digits16 (&g)[4]) {
-  return pack_low_bytes(residue_shifted<NDIG, I>(g[0]), residue_shifted<NDIG, I>(g[1]),
-                        residue_shifted<NDIG, I>(g[2]), residue_shifted<NDIG, I>(g[3]));
+  float2 a[4], b[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    a[j] = make_float2(g[0].d[j], g[1].d[j]);
+    b[j] = make_float2(g[2].d[j], g[3].d[j]);
+  }
+  const float2 ra = residue_shifted2<NDIG, I>(a), rb = residue_shifted2<NDIG, I>(b);
+  return pack_low_bytes(ra.x, ra.y, rb.x, rb.y);
 }
 
 // f(integral_constant<int, I>) for I = I0 .. min(n, N) - 1 (n uniform)
@@ -256,55 +298,109 @@ __device__ __forceinline__ uint32_t slice4(long long y0, long long y1, long long
          flip;
 }
 
-template <int MODE, int NDIG = 3>
-__device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowtile, int ky, int kstep) {
-  constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B ||
-                        MODE == G_RESID_C8A || MODE == G_RESID_C8B;
-  constexpr bool F32 = MODE == G_SPLIT_R4 || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
+// Operand element type of a gather mode.
+template <int MODE>
+struct GatherElem {
+  static constexpr bool CPLX = MODE == G_SLICE_C8A || MODE == G_SLICE_C8B || MODE == G_SPLIT_C4A ||
+                               MODE == G_SPLIT_C4B || MODE == G_RESID_C8A || MODE == G_RESID_C8B;
+  static constexpr bool F32 = MODE == G_SPLIT_R4 || MODE == G_SPLIT_C4A || MODE == G_SPLIT_C4B;
   using R = typename std::conditional<F32, float, double>::type;
   using E = typename std::conditional<CPLX, typename std::conditional<F32, float2, double2>::type, R>::type;
+};
+// Dynamic shared memory of a gather CTA: two tile buffers, a ring of three
+// tiles' K offsets, the row offsets and the row scale exponents.
+template <int MODE>
+constexpr int gather_smem_bytes() {
+  using E = typename GatherElem<MODE>::E;
+  return 2 * gather_rows<E>() * (kGK + 1) * (int)sizeof(E) + 3 * kGK * 8 + gather_rows<E>() * 20;
+}
+
+// Asynchronous copy of one element into shared memory; zero-filled when
+// !valid (src is then any valid address and is not read).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* sdst, const void* gsrc, bool valid) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  const int n = valid ? BYTES : 0;
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(gsrc), "n"(BYTES), "r"(n) : "memory");
+}
+
+template <int MODE, int NDIG = 3>
+__device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowtile, int ky, int kstep) {
+  constexpr bool CPLX = GatherElem<MODE>::CPLX;
+  constexpr bool F32 = GatherElem<MODE>::F32;
+  using R = typename GatherElem<MODE>::R;
+  using E = typename GatherElem<MODE>::E;
+  (void)sizeof(R);
   constexpr int TM = gather_rows<E>(), TK = kGK;
-  __shared__ E tile[TM][TK + 1];
-  __shared__ int64_t sm_lm[TM];
-  __shared__ int sm_se[TM];  // slice modes: the row's scale exponent
+  // Tiles move global -> shared with cp.async, double-buffered: tile i+1 is in
+  // flight while tile i converts, without passing through registers.  Its
+  // source addresses need the K offsets of tile i+1, which sit in shared
+  // memory: they were read from global memory (into a register, by one thread
+  // per k) during tile i-1's conversion and stored at its end.
+  extern __shared__ __align__(16) unsigned char gather_smem[];
+  E* tbuf = reinterpret_cast<E*>(gather_smem);                                        // [2][TM][TK+1]
+  int64_t* lkbuf = reinterpret_cast<int64_t*>(gather_smem + 2 * TM * (TK + 1) * sizeof(E));  // [3][TK]
+  int64_t* sm_lm = lkbuf + 3 * TK;                                                     // [TM]
+  double* sm_sc = reinterpret_cast<double*>(sm_lm + TM);  // residue modes: 2^(se + p + 1), or 0
+  int* sm_se = reinterpret_cast<int*>(sm_sc + TM);  // slice and residue modes: the row's scale exponent
+  auto tile_at = [&](int b) { return reinterpret_cast<E (*)[TK + 1]>(tbuf + (size_t)b * TM * (TK + 1)); };
+  // Within a row, k sits at column (k % 4) * TK/4 + k / 4: the conversion's
+  // lanes read k = 4j + t for lanes j = 0..15 of a row, which then fall on
+  // consecutive columns (no bank conflicts) instead of every fourth one.
+  auto col = [](int k) { return (k & 3) * (TK / 4) + (k >> 2); };
   const int64_t m0 = rowtile * TM;
   const int tid = threadIdx.x;
-  if (tid < TM) {
-    sm_lm[tid] = (m0 + tid < P.rows) ? P.lm[m0 + tid] : -1;
-    if constexpr (!F32) sm_se[tid] = 1021 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1021u);
-  }
   const E* src = (const E*)P.src;
   const int64_t ntiles = (P.kpad / (CPLX ? 2 : 1)) / TK;  // conversion also writes the padding
-  // The next tile's values are loaded into registers while the current one is
-  // converted (the loads' latency overlaps the conversion arithmetic); the
-  // K offsets of the next tile are read by the threads that load them.
+  if (ky >= ntiles) return;  // uniform: no tile for this CTA
+  if (tid < TM) {
+    sm_lm[tid] = (m0 + tid < P.rows) ? P.lm[m0 + tid] : -1;
+    if constexpr (!F32) {
+      const int se = 1021 - (int)(m0 + tid < P.rows ? P.rowE[m0 + tid] : 1021u);
+      sm_se[tid] = se;
+      sm_sc[tid] = se + P.rs.p + 1 <= 1023 ? pow2d(se + P.rs.p + 1) : 0.0;
+    }
+  }
+  if (tid < TK) {
+    for (int j = 0; j < 2; ++j) {
+      const int64_t k = ((int64_t)ky + (int64_t)j * kstep) * TK + tid;
+      lkbuf[j * TK + tid] = k < P.K ? P.lk[k] : 0;
+    }
+  }
   constexpr int IT = TM * TK / kGThreads;
-  E v[IT];
-  auto load_tile = [&](int64_t k0) {
+  auto issue_tile = [&](int64_t k0, int b, const int64_t* lkt) {
+    E (*t)[TK + 1] = tile_at(b);
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
       const int idx = tid + it * kGThreads;
       const int mm = P.lanes_on_k ? idx / TK : idx % TM;
       const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-      if constexpr (CPLX) { v[it].x = 0; v[it].y = 0; } else { v[it] = 0; }
-      const int64_t k = k0 + kk;
-      if (sm_lm[mm] >= 0 && k < P.K) v[it] = src[sm_lm[mm] + P.lk[k]];
+      const bool valid = sm_lm[mm] >= 0 && k0 + kk < P.K;
+      cp_async_elem<(int)sizeof(E)>(&t[mm][col(kk)], valid ? src + sm_lm[mm] + lkt[kk] : src, valid);
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  __syncthreads();  // sm_lm ready
-  if (ky < ntiles) load_tile((int64_t)ky * TK);
-  for (int64_t kt = ky; kt < ntiles; kt += kstep) {
+  __syncthreads();  // sm_lm and the first two tiles' K offsets ready
+  issue_tile((int64_t)ky * TK, 0, lkbuf);
+  int i = 0;
+  for (int64_t kt = ky; kt < ntiles; kt += kstep, ++i) {
     const int64_t k0 = kt * TK;
-    __syncthreads();  // previous tile consumed
-#pragma unroll
-    for (int it = 0; it < IT; ++it) {
-      const int idx = tid + it * kGThreads;
-      const int mm = P.lanes_on_k ? idx / TK : idx % TM;
-      const int kk = P.lanes_on_k ? idx % TK : idx / TM;
-      tile[mm][kk] = v[it];
+    __syncthreads();  // buffer (i+1) & 1 consumed; K offsets of tile i+1 visible
+    if (kt + kstep < ntiles)
+      issue_tile((kt + kstep) * TK, (i + 1) & 1, lkbuf + ((i + 1) % 3) * TK);
+    else
+      asm volatile("cp.async.commit_group;\n" ::: "memory");  // empty group: keeps the count
+    int64_t lk2 = 0;  // K offset of tile i+2 (one per thread < TK), stored after the conversion
+    {
+      const int64_t k = (kt + 2 * (int64_t)kstep) * TK + tid;
+      if (tid < TK && kt + 2 * (int64_t)kstep < ntiles && k < P.K) lk2 = P.lk[k];
     }
-    __syncthreads();
-    if (kt + kstep < ntiles) load_tile((kt + kstep) * TK);
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this thread's copies of tile i
+    __syncthreads();                                          // everyone's
+    E (*tile)[TK + 1] = tile_at(i & 1);
     {
       // convert: thread -> (row mm, 4 consecutive k)
       for (int idx = tid; idx < TM * (TK / 4); idx += kGThreads) {
@@ -312,9 +408,10 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
         const int64_t m = m0 + mm, k = k0 + kq;
         if constexpr (MODE == G_RESID_R8) {
           const int se = sm_se[mm];
+          const double sc = sm_sc[mm];
           Digits16 g[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) g[t] = digits16<NDIG>(floor(scale2(tile[mm][kq + t], se) * P.rs.pscale));
+          for (int t = 0; t < 4; ++t) g[t] = operand_digits<NDIG>(tile[mm][col(kq + t)], se, sc, P.rs.pscale);
           int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
           for_moduli<0, kMaxModuli>(P.rs.n, [&](auto ic) {
             constexpr int I = decltype(ic)::value;
@@ -323,14 +420,15 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
         } else if constexpr (MODE == G_RESID_C8A) {
           // A' row m: (re, im) interleaved along K
           const int se = sm_se[mm];
+          const double sc = sm_sc[mm];
           Digits16 ga[4], gb[4];
 #pragma unroll
           for (int t = 0; t < 2; ++t) {
-            const E v0 = tile[mm][kq + t], v1 = tile[mm][kq + 2 + t];
-            ga[2 * t] = digits16<NDIG>(floor(scale2(v0.x, se) * P.rs.pscale));
-            ga[2 * t + 1] = digits16<NDIG>(floor(scale2(P.isign * v0.y, se) * P.rs.pscale));
-            gb[2 * t] = digits16<NDIG>(floor(scale2(v1.x, se) * P.rs.pscale));
-            gb[2 * t + 1] = digits16<NDIG>(floor(scale2(P.isign * v1.y, se) * P.rs.pscale));
+            const E v0 = tile[mm][col(kq + t)], v1 = tile[mm][col(kq + 2 + t)];
+            ga[2 * t] = operand_digits<NDIG>(v0.x, se, sc, P.rs.pscale);
+            ga[2 * t + 1] = operand_digits<NDIG>(P.isign * v0.y, se, sc, P.rs.pscale);
+            gb[2 * t] = operand_digits<NDIG>(v1.x, se, sc, P.rs.pscale);
+            gb[2 * t + 1] = operand_digits<NDIG>(P.isign * v1.y, se, sc, P.rs.pscale);
           }
           int8_t* base = (int8_t*)P.planes + m * P.kpad + 2 * k;
           for_moduli<0, kMaxModuli>(P.rs.n, [&](auto ic) {
@@ -340,14 +438,14 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
         } else if constexpr (MODE == G_RESID_C8B) {
           // B' rows 2n = (re, -im), 2n+1 = (im, re) interleaved along K
           const int se = sm_se[mm];
+          const double sc = sm_sc[mm];
           Digits16 R[4], I[4], NI[4];
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
-            const double im = scale2(P.isign * v.y, se);
-            R[t] = digits16<NDIG>(floor(scale2(v.x, se) * P.rs.pscale));
-            I[t] = digits16<NDIG>(floor(im * P.rs.pscale));
-            NI[t] = digits16<NDIG>(floor(-im * P.rs.pscale));
+            const E v = tile[mm][col(kq + t)];
+            R[t] = operand_digits<NDIG>(v.x, se, sc, P.rs.pscale);
+            I[t] = operand_digits<NDIG>(P.isign * v.y, se, sc, P.rs.pscale);
+            NI[t] = operand_digits<NDIG>(-P.isign * v.y, se, sc, P.rs.pscale);
           }
           const Digits16 r0a[4] = {R[0], NI[0], R[1], NI[1]}, r0b[4] = {R[2], NI[2], R[3], NI[3]};
           const Digits16 r1a[4] = {I[0], R[0], I[1], R[1]}, r1b[4] = {I[2], R[2], I[3], R[3]};
@@ -364,7 +462,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           const int se = sm_se[mm];
           long long X[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) X[t] = fixed55(scale2(tile[mm][kq + t], se));
+          for (int t = 0; t < 4; ++t) X[t] = fixed55(scale2(tile[mm][col(kq + t)], se));
           int8_t* base = (int8_t*)P.planes + m * P.kpad + k;
 #pragma unroll
           for (int i = 0; i < kMaxSlicesDev; ++i)
@@ -375,7 +473,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           long long R[4], I[4];
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
+            const E v = tile[mm][col(kq + t)];
             R[t] = fixed55(scale2(v.x, se));
             I[t] = fixed55(scale2(P.isign * v.y, se));
           }
@@ -392,7 +490,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           long long R[4], I[4], NI[4];
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
+            const E v = tile[mm][col(kq + t)];
             const double im = scale2(P.isign * v.y, se);
             R[t] = fixed55(scale2(v.x, se));
             I[t] = fixed55(im);
@@ -413,8 +511,8 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           bool nf = false;
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
-            split_bf16(tile[mm][kq + t], h[t], l[t]);
-            nf |= !isfinite(tile[mm][kq + t]);
+            split_bf16(tile[mm][col(kq + t)], h[t], l[t]);
+            nf |= !isfinite(tile[mm][col(kq + t)]);
           }
           if (nf && P.rowE && m < P.rows) atomicMax(&P.rowE[m], 2047u);  // row left to the non-finite fix-up
           __nv_bfloat16* base = (__nv_bfloat16*)P.planes + m * P.kpad + k;
@@ -427,7 +525,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
           bool nf = false;
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
-            const E v = tile[mm][kq + t];
+            const E v = tile[mm][col(kq + t)];
             const float im = (float)P.isign * v.y;
             split_bf16(v.x, hr[t], lr[t]);
             split_bf16(im, hi[t], li[t]);
@@ -456,6 +554,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
         }
       }
     }
+    if (tid < TK) lkbuf[((i + 2) % 3) * TK + tid] = lk2;
   }
 }
 
@@ -474,6 +573,14 @@ __global__ void __launch_bounds__(kGThreads, 3) gather_grouped_kernel(const Gath
   const int2 jm = map[blockIdx.x];
   const GatherParams P = jobs[jm.x];
   gather_body<MODE>(P, jm.y, blockIdx.y, gridDim.y);
+}
+
+// Sets the grouped gather's dynamic shared-memory limit on the current device
+// (once per device; call it before any stream capture).
+template <int MODE>
+cudaError_t gather_grouped_prepare() {
+  static DeviceOnce once;
+  return smem_limit_once(once, gather_grouped_kernel<MODE>, gather_smem_bytes<MODE>());
 }
 
 // exponents: rowexp[r] = rowE[r / rep] - 1021 (rep = 2 for complex B' rows).
@@ -792,14 +899,21 @@ int run_gather(const GatherParams& P, int64_t grid_rows, int64_t grid_k, cudaStr
   // enough CTAs to fill the GPU several times over; each walks a strided set of K tiles
   int64_t gy = std::max<int64_t>(1, std::min<int64_t>(grid_k, (int64_t)num_sms() * 16 / std::max<int64_t>(1, grid_rows)));
   gy = std::min<int64_t>(gy, 65535);
+  constexpr int smem = gather_smem_bytes<MODE>();
+  auto launch = [&](auto kern, DeviceOnce& once) -> int {
+    const cudaError_t e = smem_limit_once(once, kern, smem);
+    if (e != cudaSuccess) { set_error("gather smem attribute: %s", cudaGetErrorString(e)); return TB_ERR_CUDA; }
+    kern<<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, smem, s>>>(P);
+    return 0;
+  };
+  static DeviceOnce once3, once4;
+  int err = 0;
   if constexpr (MODE == G_RESID_R8 || MODE == G_RESID_C8A || MODE == G_RESID_C8B) {
-    if (P.rs.ndig > 3)
-      gather_kernel<MODE, 4><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
-    else
-      gather_kernel<MODE, 3><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+    err = P.rs.ndig > 3 ? launch(gather_kernel<MODE, 4>, once4) : launch(gather_kernel<MODE, 3>, once3);
   } else {
-    gather_kernel<MODE><<<dim3((unsigned)grid_rows, (unsigned)gy), kGThreads, 0, s>>>(P);
+    err = launch(gather_kernel<MODE>, once3);
   }
+  if (err) return err;
   TB_CHECK_LAUNCH();
   return 0;
 }

@@ -1,9 +1,9 @@
-"""GPU parity of the tensor-core contraction (TB_METHOD_FUSED): INT8-slice
-FP64 (R8/C8) and split-BF16 FP32 (R4/C4) through tcgen05, against the
-double-double FP64 oracle.
+"""GPU parity of the tensor-core contraction (TB_METHOD_FUSED): FP64 (R8/C8)
+by modular residues or INT8 slices and FP32 (R4/C4) by split BF16 through
+tcgen05, against the double-double FP64 oracle.
 
 Tolerances (relative Frobenius error vs the oracle), stated per data kind:
-  R8/C8: 1e-12 with the default 6 slices (the FP64 accuracy target)
+  R8/C8: 1e-12 with the default residues or 6 slices (the FP64 accuracy target)
   R4/C4: 1e-4  (3-term split-BF16; its products keep about 16 mantissa bits)
 """
 import numpy as np
@@ -43,6 +43,38 @@ def test_fused_r8_square(xt, dev):
                     plan=xt.make_plan(XB.METHOD_FUSED, moduli=-1))
     assert err <= TOL[O.R8], err
     assert st.moduli == 0 and st.slices == 6 and st.passes >= 6 and st.products == 21
+
+
+@pytest.mark.parametrize("dtk,bits", [(O.R8, 20), (O.C8, 19)])
+def test_residue_path_is_exact_on_integer_data(xt, dev, dtk, bits):
+    """Integer operands of up to `bits` bits: every step of the residue path is
+    exact (the row scaling keeps the integers, the residues are the integers'
+    residues, the INT8 products are exact, the CRT recovers the exact sum), so
+    D must equal the integer product bit for bit."""
+    rng = np.random.default_rng(4)
+    M, N, K = 512, 384, 4096
+    ints = lambda n: rng.integers(-(2 ** bits), 2 ** bits + 1, size=n)
+    if dtk == O.R8:
+        l, r = ints(K * M).astype(np.float64), ints(K * N).astype(np.float64)
+        ref = l.astype(np.int64).reshape(M, K) @ r.astype(np.int64).reshape(N, K).T
+        want = ref.astype(np.float64).T.ravel()  # D(i,j), i fastest
+    else:
+        l = ints(K * M) + 1j * ints(K * M)
+        r = ints(K * N) + 1j * ints(K * N)
+        lr, li = l.real.astype(np.int64).reshape(M, K), l.imag.astype(np.int64).reshape(M, K)
+        rr, ri = r.real.astype(np.int64).reshape(N, K), r.imag.astype(np.int64).reshape(N, K)
+        re, im = lr @ rr.T - li @ ri.T, lr @ ri.T + li @ rr.T
+        want = (re.astype(np.float64) + 1j * im.astype(np.float64)).T.ravel()
+    # L(k,i) with k fastest: row i of the matrix above is contiguous along k
+    d = np.zeros(M * N, dtype=want.dtype)
+    dd, ld, rd = dev.put(d), dev.put(l), dev.put(r)
+    xt.tensor_contract("D(i,j)+=L(k,i)*R(k,j)", dtk, [M, N], dd.data_ptr(), [K, M], ld.data_ptr(), [K, N],
+                       rd.data_ptr(), 1.0, accumulative=False, plan=xt.make_plan(XB.METHOD_FUSED), stream=dev.stream())
+    got = dev.get(dd, d.dtype, d.size)
+    xt.device_check(dev.stream())
+    st = xt.last_contract_stats()
+    assert st.method == XB.METHOD_FUSED and st.moduli >= 8
+    assert np.array_equal(got, want)
 
 
 @pytest.mark.parametrize("dtk", [O.R8, O.C8])
