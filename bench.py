@@ -717,22 +717,26 @@ def selector_case(X):
         return None
     d = np.load(SELECTOR_CORPUS)
     F, T = d["features"], d["log_ms"]
-    ok = np.isfinite(T).all(axis=1)
+    if T.shape[1] != len(S.PLANS):
+        return None  # a corpus of another plan space
+    always = [i for i in range(T.shape[1]) if i not in S.FP64_ONLY]
+    ok = np.isfinite(T[:, always]).all(axis=1)
     F, T = F[ok], T[ok]
     n_train = int(0.8 * len(F))
     t0 = time.perf_counter()
     params, mean, scale, hist = S.train(F[:n_train], T[:n_train], hidden=128, epochs=150, seed=0, log_every=149)
     train_s = time.perf_counter() - t0
     pred = S.predict(params, mean, scale, F[n_train:], hidden=128)
-    learned = S.evaluate(T[n_train:], pred.argmin(axis=1))
+    learned = S.evaluate(T[n_train:], S.choose(pred, F[n_train:]))
     rule = S.evaluate(T[n_train:], [S.rule_choice(f) for f in F[n_train:]])
     always = {name: S.evaluate(T[n_train:], [i] * (len(F) - n_train))["total_time_regret"]
-              for i, name in enumerate(S.PLAN_NAMES)}
+              for i, name in enumerate(S.PLAN_NAMES) if i not in S.FP64_ONLY}
     X.selector_install(128, params, mean, scale)
     t0 = time.perf_counter()
     for f in F[n_train:n_train + 2000]:
         X.selector_choose(f)
     host_us = (time.perf_counter() - t0) / min(2000, len(F) - n_train) * 1e6
+    lib_us = float(np.median([X.selector_time(f, 2000) for f in F[n_train:n_train + 16]]))
     X.selector_install(0, None, None, None)
     net = X.MLP(F.shape[1], 128, len(S.PLANS), max_batch=1024)
     net.set_params(params)
@@ -752,7 +756,8 @@ def selector_case(X):
                       f"{len(F) - n_train} held out", "plans": S.PLAN_NAMES,
             "learned": learned, "size_rule": rule, "always_one_plan_total_regret": always,
             "train_seconds": round(train_s, 1), "final_train_loss": round(hist[-1][1], 4) if hist else None,
-            "selection_us_host": round(host_us, 2), "selection_us_gpu_batched": round(gpu_us, 4)}
+            "selection_us_library": round(lib_us, 3), "selection_us_python": round(host_us, 2),
+            "selection_us_gpu_batched": round(gpu_us, 4)}
 
 
 def e2e_talsh(X, wl, steps, case=None):
@@ -790,6 +795,24 @@ def e2e_talsh(X, wl, steps, case=None):
            "api": "talshTensorContract(COPY_TTT), host tensors, wall clock incl. H2D/D2H",
            "path": ("inputs streamed to the GPU in slices under the computation" if os.environ.get("TB_STREAM") != "0"
                     else "inputs staged whole, then the contraction")}
+    # PCIe ceiling: pinned host <-> device copies of 1 GiB, CUDA events
+    hb = torch.empty(1 << 30, dtype=torch.uint8, pin_memory=True)
+    db = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    bw = {}
+    for name, fn in (("h2d", lambda: db.copy_(hb, non_blocking=True)), ("d2h", lambda: hb.copy_(db, non_blocking=True))):
+        fn()
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        e1.synchronize()
+        bw[name] = 3 * (1 << 30) / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del hb, db
+    xfer_ms = (res["h2d_bytes_per_step"] / bw["h2d"] + res["d2h_bytes_per_step"] / bw["d2h"]) / 1e6
+    res["pcie"] = {"h2d_gbs": sig(bw["h2d"]), "d2h_gbs": sig(bw["d2h"]), "transfer_ms_per_step": sig(xfer_ms),
+                   "transfer_frac_of_step": sig(xfer_ms / (dt * 1e3), 3),
+                   "how": "pinned 1 GiB copies, CUDA events; transfer_ms = H2D bytes / H2D rate + D2H bytes / D2H rate"}
     if seeded and getattr(case, "dchosen", None) is not None:
         got = torch.from_numpy(D.host_array().copy()).cuda() / float(2 + steps)
         res["rel_frob_vs_device_result"] = sig(full_rel(got.view(torch.uint8), case.dchosen), 3)

@@ -129,6 +129,7 @@ def lib() -> C.CDLL:
     L.tb_mlp_adam_step.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, vp]
     L.tb_selector_install.argtypes = [C.c_int, fp, fp, fp, C.c_float, C.c_int]
     L.tb_selector_choose.argtypes = [fp, fp]
+    L.tb_selector_time.argtypes = [fp, C.c_int, C.POINTER(C.c_double)]
     L.tb_fill_uniform.argtypes = [C.c_int, C.c_size_t, vp, C.c_uint64, C.c_double, C.c_double, vp]
     L.tb_last_contract_stats.argtypes = [C.POINTER(ContractStats)]
     L.tb_peak_measure.argtypes = [C.c_int, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), vp]
@@ -347,7 +348,7 @@ class BlockSparsePlan:
             pass
 
 
-DESC_FEATURES, SELECT_PLANS = 16, 3
+DESC_FEATURES, SELECT_PLANS = 16, 5
 
 
 def contract_descriptor(pattern, dtk, ddims, ldims, rdims):
@@ -427,6 +428,15 @@ def selector_choose(features):
     y = (C.c_float * SELECT_PLANS)()
     idx = lib().tb_selector_choose(fp, y)
     return idx, (np.array(y[:]) if idx >= 0 else None)
+
+
+def selector_time(features, iters=10000) -> float:
+    """Microseconds per selection (host inference timed inside the library)."""
+    _f, fp = _fptr(features)
+    us = C.c_double()
+    if lib().tb_selector_time(fp, int(iters), C.byref(us)) != 0:
+        raise TBError(-1, "no selector installed")
+    return us.value
 
 
 NOALLOC_ARENA_BYTES = 64 << 20  # TB_NOALLOC_ARENA_BYTES

@@ -352,6 +352,7 @@ int contract_impl(const int* cptrn, int dtk, int drank, const int* ddims, void* 
       cp.method = c == 0 ? TB_METHOD_TTGT : TB_METHOD_FUSED;
       cp.tile_n = c == 1 ? 128 : (c >= 2 ? 256 : 0);
       cp.tile_m = c == kCandPair ? 256 : 0;
+      if (c == kCandSlices) { cp.slices = 6; cp.moduli = -1; }
       return cp;
     };
     if (selector_pick(f, &idx, &tune, &key) == 0) {

@@ -25,11 +25,13 @@ int descriptor_of(const Matricization& Z, int dtk, float* features);
 // -1 when no selector is installed; else 0 with the chosen plan index, whether
 // the two best predictions are too close to call (and autotuning is on), and a
 // cache key of the descriptor.
-// Candidate plans of the measured fallback: 0 TTGT, 1 tensor cores with N
-// tile 128, 2 with N tile 256 (the network's outputs), 3 (kCandPair) the
-// 256-wide tile on SM pairs (cta_group::2, 256-row tiles).
+// Candidate plans (the network's outputs, TB_SELECT_PLANS of them): 0 TTGT,
+// 1 tensor cores with N tile 128, 2 with N tile 256, 3 (kCandPair) the
+// 256-wide tile on SM pairs (cta_group::2, 256-row tiles), 4 (kCandSlices)
+// the 256-wide tile with 6 INT8 slices (FP64 only).
 constexpr int kCandPair = 3;
-constexpr int kNumCandidates = 4;
+constexpr int kCandSlices = 4;
+constexpr int kNumCandidates = 5;
 // The network's choice for a descriptor (idx), or the cached measured one;
 // tune_mask: candidates to time before choosing (0: none).
 int selector_pick(const float* features, int* idx, unsigned* tune_mask, uint64_t* key);

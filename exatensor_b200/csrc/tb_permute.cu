@@ -1,6 +1,7 @@
 // tb_permute.cu -- permutation plans, tiled and scatter permutation kernels,
 // and the tb_tensor_copy / tb_tensor_add entry points.
 #include "tb_permute.cuh"
+#include "tb_perm_tma.cuh"
 
 #include <algorithm>
 #include <map>
@@ -164,7 +165,10 @@ constexpr int64_t kTuneMinBytes = (int64_t)32 << 20;
 // A further candidate for long row copies: the default plan in the bulk-copy
 // kernel (measured faster for 4-byte elements, slower for 8-byte ones).
 constexpr int kBulkRowsCand = kNumTileCandidates;
-constexpr int kNumPlanCandidates = kNumTileCandidates + 1;
+// the TMA-staged transpose kernel (tb_perm_tma.cuh) on the default plan's
+// reduced view, where its layout requirements hold
+constexpr int kTmaCand = kNumTileCandidates + 1;
+constexpr int kNumPlanCandidates = kNumTileCandidates + 2;
 
 bool long_row_copy(const PermParams& P) { return P.rows2d && P.tma_ok && (int64_t)P.LA * P.es >= 4096; }
 
@@ -202,13 +206,21 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
   static const bool tune_on = [] { const char* e = getenv("TB_PERM_TUNE"); return !(e && e[0] == '0'); }();
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) { cudaGetLastError(); cap = cudaStreamCaptureStatusActive; }
-  const bool tune = pick < 0 && tune_on && vol * (int64_t)sizeof(E) >= kTuneMinBytes && cap == cudaStreamCaptureStatusNone;
+  // TB_PERM_TMA=1 / 0: the TMA-staged kernel wherever it applies / never
+  // (tuning and test switch; results are identical)
+  static const int tma_env = [] { const char* e = getenv("TB_PERM_TMA"); return e ? (e[0] == '1' ? 1 : 0) : -1; }();
+  const bool tune = pick < 0 && tune_on && tma_env < 0 && vol * (int64_t)sizeof(E) >= kTuneMinBytes &&
+                    cap == cudaStreamCaptureStatusNone;
   if (!tune) {
-    const int c = pick < 0 ? 0 : pick;
-    const TileBounds b = kTileCandidates[c == kBulkRowsCand ? 0 : c];
+    const int c = tma_env == 1 ? kTmaCand : (pick < 0 ? 0 : pick);
+    const TileBounds b = kTileCandidates[(c == kBulkRowsCand || c == kTmaCand) ? 0 : c];
     PermParams P;
     int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb, b.min_run);
     if (e == 0) {
+      if (c == kTmaCand && tma_env != 0) {
+        TmaPermParams T;
+        if (tma_perm_plan(P, in, &T)) return launch_perm_tma<E, Store>(T, st, s);
+      }
       if (c == kBulkRowsCand && long_row_copy(P)) P.bulk_rows = 1;
       return launch_perm<E, Store>(P, in, st, s);
     }
@@ -235,16 +247,22 @@ int run_copy_measured(int rank, const int* dims, const int* cptrn, const E* in, 
     plans[n].bulk_rows = 1;
     idx[n++] = kBulkRowsCand;
   }
-  if (n == 1) { remember_choice(key, 0); return launch_perm<E, Store>(plans[0], in, st, s); }
+  static TmaPermParams tma;  // large (a tensor map); built under the lock
+  const bool with_tma = tma_perm_plan(plans[0], in, &tma);
+  if (n == 1 && !with_tma) { remember_choice(key, 0); return launch_perm<E, Store>(plans[0], in, st, s); }
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) { set_error("cudaEventCreate failed"); return TB_ERR_CUDA; }
   if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); set_error("cudaEventCreate failed"); return TB_ERR_CUDA; }
   float best_ms = 0.f, ms0 = 0.f;
   int best = 0, err = 0;
+  if (with_tma) idx[n++] = kTmaCand;
+  auto run = [&](int k) {
+    return idx[k] == kTmaCand ? launch_perm_tma<E, Store>(tma, st, s) : launch_perm<E, Store>(plans[k], in, st, s);
+  };
   for (int k = 0; k < n && !err; ++k) {
-    if ((err = launch_perm<E, Store>(plans[k], in, st, s))) break;  // untimed: first launch of a variant
+    if ((err = run(k))) break;  // untimed: first launch of a variant
     cudaEventRecord(e0, s);
-    if ((err = launch_perm<E, Store>(plans[k], in, st, s))) break;
+    if ((err = run(k))) break;
     cudaEventRecord(e1, s);
     float ms = 0.f;
     if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
@@ -287,7 +305,7 @@ int run_permutation(int rank, const int* dims, const int* cptrn, const E* in, co
       auto it = g_tune.find(key);
       if (it != g_tune.end()) pick = it->second;
     }
-    const TileBounds b = kTileCandidates[(pick < 0 || pick == kBulkRowsCand) ? 0 : pick];
+    const TileBounds b = kTileCandidates[(pick < 0 || pick == kBulkRowsCand || pick == kTmaCand) ? 0 : pick];
     PermParams P;
     int e = build_perm_plan_o2n((int)sizeof(E), rank, dims, cptrn, &P, b.vmin_kb, b.vmax_kb, b.min_run);
     for (int c : {kListCand, kListCandShort}) {

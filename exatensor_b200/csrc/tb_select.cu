@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <cstring>
 #include <string>
 #include <mutex>
@@ -126,17 +127,23 @@ int descriptor_of(const Matricization& Z0, int dtk, float* f) {
 // this many the sets are cleared, so memory stays bounded in long runs.
 constexpr size_t kMaxRemembered = (size_t)1 << 16;
 
+// Plans the descriptor allows: INT8 slices (plan kCandSlices) are FP64-only.
+bool plan_applies(const float* f, int i) { return i != kCandSlices || f[15] != 0.f; }
+
+int best_plan(const float* f, const float* y) {
+  int best = 0;
+  for (int i = 1; i < TB_SELECT_PLANS; ++i)
+    if (plan_applies(f, i) && y[i] < y[best]) best = i;
+  return best;
+}
+
 int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) {
   Selector& S = sel();
   std::lock_guard<std::mutex> lk(S.mu);
   if (!S.on) return -1;
   float y[TB_SELECT_PLANS];
   mlp_host(S, f, y);
-  int best = 0, second = -1;
-  for (int i = 1; i < TB_SELECT_PLANS; ++i)
-    if (y[i] < y[best]) best = i;
-  for (int i = 0; i < TB_SELECT_PLANS; ++i)
-    if (i != best && (second < 0 || y[i] < y[second])) second = i;
+  const int best = best_plan(f, y);
   *idx = best;
   // key: the descriptor quantised to 1/64 (log2 units)
   uint64_t h = 1469598103934665603ull;
@@ -145,18 +152,14 @@ int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) 
     h *= 1099511628211ull;
   }
   *key = h;
-  // Timing candidates costs a few contractions: only worth it for large ones.
-  // Close predictions time the three plans; a large fused prediction also
-  // times the CTA-pair form of the 256-wide tile (kCandPair), which the
-  // network does not predict: it pays off where long K panels stop fitting
-  // in L2 (C8 CCSD-like, K' = 73728: 20% faster; R8, K = 36864: 5% slower).
+  // Timing candidates costs a few contractions: only worth it for large ones,
+  // and only for the plans predicted within the margin of the best.
   constexpr float kTuneMinLog2Flops = 34.0f;  // about 1.7e10 FLOP
-  constexpr float kPairMinLog2Flops = 36.0f;  // about 6.9e10 FLOP
   unsigned mask = 0;
-  if (S.autotune && second >= 0 && (y[second] - y[best]) < S.margin && f[3] >= kTuneMinLog2Flops)
-    mask = (1u << TB_SELECT_PLANS) - 1;
-  if (S.autotune && f[3] >= kPairMinLog2Flops && (best != 0 || mask))
-    mask |= (1u << best) | (1u << kCandPair);
+  if (S.autotune && f[3] >= kTuneMinLog2Flops)
+    for (int i = 0; i < TB_SELECT_PLANS; ++i)
+      if (plan_applies(f, i) && y[i] - y[best] < S.margin) mask |= 1u << i;
+  if (mask == (1u << best)) mask = 0;  // nothing close: the prediction stands
   if (mask) {
     auto it = S.cache.find(h);
     if (it != S.cache.end()) {
@@ -225,11 +228,25 @@ extern "C" int tb_selector_choose(const float* features, float* predicted) {
   if (!S.on || !features) return -1;
   float y[TB_SELECT_PLANS];
   mlp_host(S, features, y);
-  int best = 0;
-  for (int i = 1; i < TB_SELECT_PLANS; ++i)
-    if (y[i] < y[best]) best = i;
   if (predicted) std::memcpy(predicted, y, sizeof(y));
-  return best;
+  return best_plan(features, y);
+}
+
+extern "C" int tb_selector_time(const float* features, int iters, double* us_per_call) {
+  if (!features || iters < 1 || !us_per_call) return TB_ERR_INVALID_ARGS;
+  Selector& S = sel();
+  if (!S.on) return -1;
+  volatile int sink = 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0; i < iters; ++i) {
+    std::lock_guard<std::mutex> lk(S.mu);
+    float y[TB_SELECT_PLANS];
+    mlp_host(S, features, y);
+    sink = sink + best_plan(features, y);
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  *us_per_call = std::chrono::duration<double, std::micro>(t1 - t0).count() / iters;
+  return 0;
 }
 
 // Weights file: "TBSEL001", int32 features, hidden, outputs, float32 margin,

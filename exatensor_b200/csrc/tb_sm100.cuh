@@ -41,7 +41,12 @@ __device__ __forceinline__ uint64_t global_ns() {
 // and returns false, so that a barrier that never completes ends the kernel
 // with an error status that names the wait.
 constexpr uint64_t kWaitNanos = 2000000000ull;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err, unsigned code = 1u) {
+// sleep_ns > 0: after a few polls the waiting thread sleeps that long between
+// polls, leaving its scheduler's issue slots to the warps it shares them with
+// (for waits that last many microseconds, such as an epilogue waiting for the
+// next accumulator).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* err, unsigned code = 1u,
+                                          unsigned sleep_ns = 0) {
   uint32_t done = 0;
   uint64_t t0 = 0;
   for (uint32_t it = 0; it < kSpinLimit; ++it) {
@@ -51,6 +56,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (done) return true;
+    if (sleep_ns && it >= 4) __nanosleep(sleep_ns);
     if ((it & 1023u) == 0) {
       const uint64_t t = global_ns();
       if (it == 0) t0 = t;
@@ -65,8 +71,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
 // together when any lane's wait expired, so that the warp-collective
 // operations after it (tcgen05.ld, __syncwarp, shuffles) are reached by all
 // 32 lanes or by none.
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, unsigned int* err, unsigned code = 1u) {
-  const bool ok = mbar_wait(bar, parity, err, code);
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, unsigned int* err, unsigned code = 1u,
+                                               unsigned sleep_ns = 0) {
+  const bool ok = mbar_wait(bar, parity, err, code, sleep_ns);
   return __all_sync(0xffffffffu, ok ? 1 : 0) != 0;
 }
 

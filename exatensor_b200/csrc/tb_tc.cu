@@ -449,6 +449,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     for (size_t p = 0; p < passes.size(); ++p) {
       P.pass_first[p] = q;
       P.pass_shift[p] = shifts[p];
+      P.pass_magic[p] = resid ? (int)(4294967296ull / (unsigned long long)shifts[p]) : 0;
       for (auto& e : passes[p]) {
         P.prod_a[q] = e.a; P.prod_b[q] = e.b; P.prod_kb0[q] = e.kb0; P.prod_kb1[q] = e.kb1;
         ++q;

@@ -22,6 +22,11 @@
 namespace tb {
 
 constexpr int kStagesTC = 4;
+// The epilogue warps wait a whole accumulator pass (tens of microseconds) for
+// their next accumulator; they poll every this many nanoseconds, so that the
+// warps sharing their schedulers with the TMA and MMA threads do not take
+// issue slots from them.
+constexpr unsigned kEpilogueSleepNs = 200;
 constexpr int kMaxProducts = 64;  // entries (plane pair and K range) over all passes
 constexpr int kTcThreads = 192;
 
@@ -41,7 +46,8 @@ struct __align__(64) TcGemmParams {
   int pass_first[kMaxProducts + 1];  // entries of pass p: [pass_first[p], pass_first[p+1])
   int prod_a[kMaxProducts], prod_b[kMaxProducts];    // plane of A and of B
   int prod_kb0[kMaxProducts], prod_kb1[kMaxProducts];  // K-block range
-  int pass_shift[kMaxProducts];      // INT8 slices: the pass's weight is 2^-pass_shift
+  int pass_shift[kMaxProducts];      // INT8 slices: the pass's weight is 2^-pass_shift; residues: the modulus
+  int pass_magic[kMaxProducts];      // residues: floor(2^32 / modulus), for the epilogue's reduction
   void* D;
   const int64_t* dm;          // D offset of row m (elements of D's data kind)
   const int64_t* dn;          // D offset of column n (complex: of column pair n/2)
@@ -135,7 +141,7 @@ __device__ __forceinline__ double scale2(double x, int e) {
 // flight instead of waiting on each one.
 template <int BN, int EPI, class EP>
 __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool mval, int64_t dmo, int re, int nb,
-                                              bool first, int shift) {
+                                              bool first, int shift, int magic = 0) {
   using namespace sm100;
   constexpr bool OZ = EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C;
   constexpr bool CPLX = EPI == EPI_OZAKI_C || EPI == EPI_BF16_C;
@@ -147,17 +153,22 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
     tmem_ld32(tcol + (uint32_t)(c * 32), r);
     const int n0 = nb * BN + c * 32;
     if constexpr (EPI == EPI_RESID) {
-      // residues of the exact INT32 sums: shift is the modulus, and the
-      // caller passes this pass's plane through P.res / res_plane
+      // residues of the exact INT32 sums: shift is the modulus m, and the
+      // caller passes this pass's plane through P.res / res_plane.  v mod m
+      // by a multiply-high with magic = floor(2^32 / m): the quotient estimate
+      // is off by at most one either way, so two conditional corrections give
+      // the residue in [0, m) (integer pipes only; no division).
       if constexpr (std::is_same<EP, TcGemmParams>::value) {
         if (mval) {
           uint8_t* col = P.res + dmo;  // dmo: this pass's plane offset + row
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             if (n0 + j >= P.N) break;
-            int v = (int)r[j] % shift;
-            if (v < 0) v += shift;
-            col[(int64_t)(n0 + j) * P.res_ld] = (uint8_t)v;
+            const int v = (int)r[j];
+            int rr = v - __mulhi(v, magic) * shift;
+            rr += rr < 0 ? shift : 0;
+            rr -= rr >= shift ? shift : 0;
+            col[(int64_t)(n0 + j) * P.res_ld] = (uint8_t)rr;
           }
         }
       }
@@ -273,8 +284,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
   auto take_unit = [&](uint32_t j, bool warp_wide) -> int {
     const int r = (int)(j % kUnitRing);
     const uint32_t ph = (j / kUnitRing) & 1;
-    const bool got =
-        warp_wide ? mbar_wait_warp(&bars->unit_full[r], ph, P.err) : mbar_wait(&bars->unit_full[r], ph, P.err);
+    const bool got = warp_wide ? mbar_wait_warp(&bars->unit_full[r], ph, P.err, 1u, kEpilogueSleepNs)
+                               : mbar_wait(&bars->unit_full[r], ph, P.err);
     if (!got) { ok = false; return -1; }
     const int u = *(volatile int*)&bars->unit[r];
     if (warp_wide) {
@@ -374,13 +385,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
       for (int p = w.p0; p < w.p1 && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
+        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 1u, kEpilogueSleepNs))) break;
         tc_fence_after();
         const bool first = (p == 0);
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C || EPI == EPI_RESID) ? P.pass_shift[p] : 0;
         const int64_t dmp = EPI == EPI_RESID ? (int64_t)p * P.res_plane + m : dmo;
         epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN),
-                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, first, shift);
+                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, first, shift,
+                               EPI == EPI_RESID ? P.pass_magic[p] : 0);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&bars->acc_empty[a]);
@@ -529,12 +541,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
       for (int p = w.p0; p < w.p1 && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err))) break;
+        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 1u, kEpilogueSleepNs))) break;
         tc_fence_after();
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C || EPI == EPI_RESID) ? P.pass_shift[p] : 0;
         const int64_t dmp = EPI == EPI_RESID ? (int64_t)p * P.res_plane + m : dmo;
         epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN),
-                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, p == 0, shift);
+                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, p == 0, shift,
+                               EPI == EPI_RESID ? P.pass_magic[p] : 0);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive_cluster(acc_empty0 + (uint32_t)(a * sizeof(uint64_t)));

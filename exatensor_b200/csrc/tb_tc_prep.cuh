@@ -309,10 +309,15 @@ struct GatherElem {
 };
 // Dynamic shared memory of a gather CTA: two tile buffers, a ring of three
 // tiles' K offsets, the row offsets and the row scale exponents.
+// K tile of a gather mode (64 for all: 32-wide tiles with four CTAs per SM
+// ran the real residue gather 1.7x slower)
+template <int MODE>
+constexpr int gather_tk() { return kGK; }
 template <int MODE>
 constexpr int gather_smem_bytes() {
   using E = typename GatherElem<MODE>::E;
-  return 2 * gather_rows<E>() * (kGK + 1) * (int)sizeof(E) + 3 * kGK * 8 + gather_rows<E>() * 20;
+  return 2 * gather_rows<E>() * (gather_tk<MODE>() + 1) * (int)sizeof(E) + 3 * gather_tk<MODE>() * 8 +
+         gather_rows<E>() * 20;
 }
 
 // Asynchronous copy of one element into shared memory; zero-filled when
@@ -334,7 +339,7 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
   using R = typename GatherElem<MODE>::R;
   using E = typename GatherElem<MODE>::E;
   (void)sizeof(R);
-  constexpr int TM = gather_rows<E>(), TK = kGK;
+  constexpr int TM = gather_rows<E>(), TK = gather_tk<MODE>();
   // Tiles move global -> shared with cp.async, double-buffered: tile i+1 is in
   // flight while tile i converts, without passing through registers.  Its
   // source addresses need the K offsets of tile i+1, which sit in shared
@@ -348,8 +353,9 @@ __device__ __forceinline__ void gather_body(const GatherParams& P, int64_t rowti
   int* sm_se = reinterpret_cast<int*>(sm_sc + TM);  // slice and residue modes: the row's scale exponent
   auto tile_at = [&](int b) { return reinterpret_cast<E (*)[TK + 1]>(tbuf + (size_t)b * TM * (TK + 1)); };
   // Within a row, k sits at column (k % 4) * TK/4 + k / 4: the conversion's
-  // lanes read k = 4j + t for lanes j = 0..15 of a row, which then fall on
-  // consecutive columns (no bank conflicts) instead of every fourth one.
+  // lanes read k = 4j + t for the TK/4 lanes j of a row, which then fall on
+  // consecutive columns (no bank conflicts within a row) instead of every
+  // fourth one.
   auto col = [](int k) { return (k & 3) * (TK / 4) + (k >> 2); };
   const int64_t m0 = rowtile * TM;
   const int tid = threadIdx.x;

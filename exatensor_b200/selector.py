@@ -20,9 +20,16 @@ import string
 
 import numpy as np
 
-# Candidate plans: (method, tile_n).  All of them meet the accuracy bounds.
-PLANS = [(1, 0), (2, 128), (2, 256)]   # TTGT; tensor cores with 128- or 256-wide tiles
-PLAN_NAMES = ["ttgt", "fused_n128", "fused_n256"]
+# Candidate plans (make_plan arguments), in the order of the network's outputs
+# and of the library's candidates (TB_SELECT_PLANS).  All of them meet the
+# accuracy bounds; the INT8-slice plan applies to FP64 data only.
+PLANS = [dict(method=1),                              # TTGT
+         dict(method=2, tile_n=128),                  # tensor cores, 128-wide N tile
+         dict(method=2, tile_n=256),                  # 256-wide N tile
+         dict(method=2, tile_n=256, tile_m=256),      # 256-wide tile on SM pairs
+         dict(method=2, tile_n=256, slices=6)]        # 6 INT8 slices instead of residues
+PLAN_NAMES = ["ttgt", "fused_n128", "fused_n256", "fused_n256_pair", "fused_n256_slices6"]
+FP64_ONLY = {4}
 NFEAT = 16
 
 
@@ -66,22 +73,39 @@ def rule_choice(desc):
     return 2 if N >= 192 else 1
 
 
+def choose(pred, features):
+    """Plan with the smallest prediction among those the descriptor allows
+    (the library's rule: INT8 slices for FP64 only)."""
+    p = np.array(pred, dtype=np.float64, copy=True)
+    fp64 = np.asarray(features)[..., 15] != 0
+    for i in FP64_ONLY:
+        p[..., i] = np.where(fp64, p[..., i], np.inf)
+    return p.argmin(axis=-1)
+
+
 def regret(times, choice):
-    """Mean relative slowdown of the chosen plans against the best plan."""
+    """Mean relative slowdown of the chosen plans against the best plan
+    (plans without a label, NaN, do not count as best)."""
     t = np.asarray(times, dtype=np.float64)
-    best = t.min(axis=1)
+    best = np.nanmin(t, axis=1)
     got = t[np.arange(len(t)), np.asarray(choice)]
     return float(np.mean(got / best - 1.0)), float(got.sum() / best.sum() - 1.0)
 
 
 # ----------------------------------------------------------------------------- corpus labelling (GPU)
-def label_corpus(n, seed=0, out=None, reps=2, log=None, start=0):
+def label_corpus(n, seed=0, out=None, reps=2, log=None, start=0, long_ms=25.0, ttgt_long_ms=100.0):
     """Times every candidate plan of n seeded random contractions on the GPU.
 
     Returns (features [n][NFEAT], log-times [n][len(PLANS)] in ln(ms), NaN where
-    a plan failed, patterns).  Inputs are seeded uniform data in one buffer
-    sized for the 4 GiB footprint cap; each plan runs once untimed, then reps
-    times between CUDA events on the launching stream."""
+    a plan failed or does not apply, patterns).  Inputs are seeded uniform data
+    in one buffer sized for the 4 GiB footprint cap.  Each plan's first run is
+    timed between CUDA events on the launching stream; when it takes long_ms or
+    more its time is the label (first-use costs are small beside it), else reps
+    more runs are timed and their mean is the label.  TTGT's first run of a
+    shape also chooses its permutation plans: it is the label only from
+    ttgt_long_ms on, else a second run is timed (and reps more below
+    long_ms).  A plan that fails, or leaves an error in the device error
+    word, gets NaN."""
     import time
 
     import torch
@@ -90,13 +114,29 @@ def label_corpus(n, seed=0, out=None, reps=2, log=None, start=0):
     X.device_init(0)
     s_obj = torch.cuda.current_stream()
     s = s_obj.cuda_stream
+    # one input buffer per element type, each filled with finite values of its
+    # own type (FP64 bit patterns read as FP32 would hold NaNs and infinities,
+    # whose fix-up pass is not what the plans should be timed on); D goes to a
+    # buffer of its own, so the inputs keep their values from one entry to the next
     cap = (4 << 30) + (1 << 20)
-    buf = torch.empty(cap, dtype=torch.uint8, device="cuda")
-    X.fill_uniform(8, cap // 8, buf.data_ptr(), 1234, stream=s)
+    bufs = {}
+    for kind in (4, 8):
+        bufs[kind] = torch.empty(cap, dtype=torch.uint8, device="cuda")
+        X.fill_uniform(kind, cap // (8 if kind == 8 else 4), bufs[kind].data_ptr(), 1234, stream=s)
+    dbuf = torch.empty(cap, dtype=torch.uint8, device="cuda")
     rng = np.random.default_rng(seed)
     feats, times, pats = [], [], []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_start = time.time()
+
+    def timed(run, k):
+        e0.record(s_obj)
+        for _ in range(k):
+            run()
+        e1.record(s_obj)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
     for i in range(n):
         pattern, dd, ld, rd, dtk = random_contraction(rng)
         if i < start:
@@ -105,30 +145,33 @@ def label_corpus(n, seed=0, out=None, reps=2, log=None, start=0):
         vol = lambda d: int(np.prod(d)) if d else 1
         lo = 0
         ro = (vol(ld) * es + 255) // 256 * 256
-        do = ro + (vol(rd) * es + 255) // 256 * 256
-        base = buf.data_ptr()
+        base = bufs[8 if dtk == 8 else 4].data_ptr()
+        dptr = dbuf.data_ptr()
         row = []
-        for method, tile_n in PLANS:
-            plan = X.make_plan(method, tile_n=tile_n)
+        for j, kw in enumerate(PLANS):
+            if j in FP64_ONLY and dtk != 8:
+                row.append(float("nan"))
+                continue
+            plan = X.make_plan(**kw)
+            run = lambda: X.tensor_contract(pattern, dtk, dd, dptr, ld, base + lo, rd, base + ro, 1.0,
+                                            accumulative=False, plan=plan, stream=s)
             try:
-                X.tensor_contract(pattern, dtk, dd, base + do, ld, base + lo, rd, base + ro, 1.0,
-                                  accumulative=False, plan=plan, stream=s)
-                e0.record(s_obj)
-                for _ in range(reps):
-                    X.tensor_contract(pattern, dtk, dd, base + do, ld, base + lo, rd, base + ro, 1.0,
-                                      accumulative=False, plan=plan, stream=s)
-                e1.record(s_obj)
-                e1.synchronize()
-                row.append(math.log(max(e0.elapsed_time(e1) / reps, 1e-4)))
+                t = timed(run, 1)
+                if kw["method"] == 1 and t < ttgt_long_ms:
+                    t = timed(run, 1)
+                if t < long_ms:
+                    t = timed(run, reps)
+                X.device_check(s)
+                row.append(math.log(max(t, 1e-4)))
             except X.TBError:
                 torch.cuda.synchronize()
                 row.append(float("nan"))
         feats.append(X.contract_descriptor(pattern, dtk, dd, ld, rd))
         times.append(row)
         pats.append(pattern + f" | {dd} {ld} {rd} dtk={dtk}")
-        if out and ((i + 1) % 500 == 0 or i + 1 == n):
+        if out and ((i + 1) % 250 == 0 or i + 1 == n):
             np.savez_compressed(out, features=np.array(feats, np.float32), log_ms=np.array(times, np.float32),
-                                patterns=np.array(pats), seed=seed)
+                                patterns=np.array(pats), seed=seed, start=start)
             if log:
                 print(f"{i + 1}/{n} labelled, {time.time() - t_start:.0f} s", file=log, flush=True)
     return np.array(feats, np.float32), np.array(times, np.float32), pats
@@ -194,15 +237,19 @@ def predict(params, mean, scale, Xf, hidden=128):
 
 
 def evaluate(log_ms, choice):
-    """Regret of plan choices against the best measured plan (rows with a NaN
-    for the chosen plan count as failures)."""
+    """Regret of plan choices against the best measured plan.  Rows need a
+    label for every plan that applies to all data kinds; the FP64-only plan's
+    label is NaN for FP32 rows and then does not count."""
     t = np.exp(np.asarray(log_ms, np.float64))
-    ok = np.isfinite(t).all(axis=1)
+    always = [i for i in range(t.shape[1]) if i not in FP64_ONLY]
+    ok = np.isfinite(t[:, always]).all(axis=1)
     t = t[ok]
     c = np.asarray(choice)[ok]
+    if not np.all(np.isfinite(t[np.arange(len(t)), c])):
+        raise ValueError("a plan was chosen that has no label")
     mean_regret, total_regret = regret(t, c)
     return {"rows": int(ok.sum()), "mean_regret": mean_regret, "total_time_regret": total_regret,
-            "picked_best": float(np.mean(c == t.argmin(axis=1)))}
+            "picked_best": float(np.mean(c == np.nanargmin(t, axis=1)))}
 
 
 def save_weights(path, params, mean, scale, hidden=128, margin=0.0, autotune=0):
@@ -220,7 +267,8 @@ def main(argv=None):
     import argparse
     import sys
     ap = argparse.ArgumentParser(description="selector corpus labelling and training")
-    ap.add_argument("cmd", choices=["label", "train"])
+    ap.add_argument("cmd", choices=["label", "train", "merge"])
+    ap.add_argument("--parts", nargs="*", default=[], help="merge: chunk files written by label --start")
     ap.add_argument("--corpus", default=None, help="train: labelled corpus (.npz)")
     ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--margin", type=float, default=0.25, help="train: ln-time margin below which AUTO times plans")
@@ -233,6 +281,20 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.cmd == "label":
         label_corpus(a.n, a.seed, a.out, reps=a.reps, log=sys.stdout, start=a.start)
+        return
+    if a.cmd == "merge":
+        # chunks of one seeded sequence, each starting where the previous ended
+        parts = sorted((np.load(p) for p in a.parts), key=lambda d: int(d["start"]))
+        nxt = 0
+        for d in parts:
+            if int(d["start"]) != nxt:
+                raise SystemExit(f"chunk starting at {int(d['start'])} does not follow entry {nxt}")
+            nxt += len(d["features"])
+        np.savez_compressed(a.out, features=np.concatenate([d["features"] for d in parts]),
+                            log_ms=np.concatenate([d["log_ms"] for d in parts]),
+                            patterns=np.concatenate([d["patterns"] for d in parts]), seed=int(parts[0]["seed"]),
+                            plans=np.array(PLAN_NAMES))
+        print(f"{nxt} entries -> {a.out}")
         return
     d = np.load(a.corpus)
     params, mean, scale, hist = train(d["features"], d["log_ms"], hidden=128, epochs=a.epochs, seed=a.seed,

@@ -279,12 +279,14 @@ int tb_batch_destroy(tb_batch_t* batch);
 /* ---- learned plan selection ---------------------------------------------
  * No counterpart in the reference, which always runs TTGT through cuBLAS.
  * A contraction descriptor (TB_DESC_FEATURES floats) feeds a 3-layer MLP that
- * predicts the log-runtime of each candidate plan (TTGT; tensor cores with
- * N tiles 128 and 256); TB_METHOD_AUTO then takes the fastest predicted plan.
- * Every candidate meets the accuracy bounds, so the choice changes speed, not
- * what is computed beyond those bounds. */
+ * predicts the log-runtime of each candidate plan: 0 TTGT; tensor cores with
+ * 1 the 128-wide N tile, 2 the 256-wide N tile, 3 the 256-wide tile on SM
+ * pairs (256-row tiles), 4 the 256-wide tile with 6 INT8 slices instead of
+ * modular residues (FP64 data only).  TB_METHOD_AUTO then takes the fastest
+ * predicted plan.  Every candidate meets the accuracy bounds, so the choice
+ * changes speed, not what is computed beyond those bounds. */
 #define TB_DESC_FEATURES 16
-#define TB_SELECT_PLANS 3
+#define TB_SELECT_PLANS 5
 
 /* Descriptor of a contraction (host only, no GPU work). */
 int tb_contract_descriptor(const int* cptrn, int data_kind, int drank, const int* d_dims, int lrank,
@@ -308,16 +310,19 @@ int tb_mlp_adam_step(tb_mlp_t* net, float lr, float beta1, float beta2, float ep
 /* Installs a trained selector for TB_METHOD_AUTO: the parameters of a
  * (TB_DESC_FEATURES -> hidden -> hidden -> TB_SELECT_PLANS) network and the
  * feature normalisation (x - mean) / scale.  params = NULL removes it (the
- * rule-based choice returns).  margin: when the two best predictions differ
- * by less than this (in natural-log units), autotune != 0 and the contraction
- * is large (about 1.7e10 FLOP or more), the second call with the same
- * descriptor times every plan once (alpha = 0, beta = 1 runs, D unchanged)
+ * rule-based choice returns).  margin: when other plans' predictions lie
+ * within this of the best (in natural-log units), autotune != 0 and the
+ * contraction is large (about 1.7e10 FLOP or more), the second call with the
+ * same descriptor times those plans (alpha = 0, beta = 1 runs, D unchanged)
  * and caches the winner; one-off shapes keep the prediction. */
 int tb_selector_install(int n_hidden, const float* params, const float* mean, const float* scale, float margin,
                         int autotune);
-/* The selector's choice for a descriptor: plan index (0 TTGT, 1 tensor cores
- * N tile 128, 2 N tile 256) and the predicted log-runtimes (may be NULL). */
+/* The selector's choice for a descriptor: plan index (as listed above; plan 4
+ * only for FP64 descriptors) and the predicted log-runtimes (may be NULL). */
 int tb_selector_choose(const float* features, float* predicted);
+/* Host time of one selection (descriptor already built), averaged over iters
+ * calls of the inference that TB_METHOD_AUTO runs; -1 without a selector. */
+int tb_selector_time(const float* features, int iters, double* us_per_call);
 /* Installs a selector from a weights file ("TBSEL001" header, features,
  * hidden, outputs, margin, autotune, mean, scale, parameters).  tb_device_init
  * loads selector_weights.bin from the library's directory when present

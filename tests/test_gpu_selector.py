@@ -74,12 +74,14 @@ def test_training_fits_a_smooth_target(xt):
 def test_trained_selector_beats_the_size_rule(xt):
     d = np.load(CORPUS)
     F, T = d["features"], d["log_ms"]
-    ok = np.isfinite(T).all(axis=1)
+    assert T.shape[1] == XB.SELECT_PLANS == len(S.PLANS)
+    always = [i for i in range(T.shape[1]) if i not in S.FP64_ONLY]
+    ok = np.isfinite(T[:, always]).all(axis=1)
     F, T = F[ok], T[ok]
     n_train = int(0.8 * len(F))
     params, mean, scale, _ = S.train(F[:n_train], T[:n_train], hidden=128, epochs=150, seed=0)
     pred = S.predict(params, mean, scale, F[n_train:], hidden=128)
-    learned = S.evaluate(T[n_train:], pred.argmin(axis=1))
+    learned = S.evaluate(T[n_train:], S.choose(pred, F[n_train:]))
     rule = S.evaluate(T[n_train:], [S.rule_choice(f) for f in F[n_train:]])
     assert learned["total_time_regret"] < rule["total_time_regret"], (learned, rule)
     assert learned["mean_regret"] < rule["mean_regret"], (learned, rule)
@@ -96,12 +98,12 @@ def test_auto_uses_the_installed_selector(xt, dev):
     vol = lambda s: int(np.prod(s))
     d, l, r = rand_host(O.R8, vol(ddims), 1), rand_host(O.R8, vol(ldims), 2), rand_host(O.R8, vol(rdims), 3)
     exact = oracle_dd(pattern, d, ddims, l, ldims, r, rdims, 1.0, True)
-    nh = 8
-    n = 16 * nh + nh + nh * nh + nh + nh * 3 + 3
+    nh, P = 8, XB.SELECT_PLANS
+    n = 16 * nh + nh + nh * nh + nh + nh * P + P
     for favoured, method in ((0, XB.METHOD_TTGT), (2, XB.METHOD_FUSED)):
         p = np.zeros(n, np.float32)
-        p[-3:] = 5.0
-        p[-3 + favoured] = 1.0           # constant prediction: this plan is fastest
+        p[-P:] = 5.0
+        p[-P + favoured] = 1.0           # constant prediction: this plan is fastest
         XB.selector_install(nh, p, np.zeros(16, np.float32), np.ones(16, np.float32))
         try:
             dd, ld, rd = dev.put(d), dev.put(l), dev.put(r)
@@ -136,11 +138,12 @@ def test_auto_uses_the_installed_selector(xt, dev):
     xt.device_check(dev.stream())
 
 
-def test_large_fused_prediction_times_the_sm_pair_tile(xt, dev):
-    """A large contraction (>= 2^36 FLOP) predicted fused is timed on its
-    second call against the 256-wide tile on SM pairs, which the network does
-    not predict.  Whichever tile is kept, the INT8 sums are exact, so D equals
-    the single-SM plan's result bit for bit."""
+def test_close_predictions_time_only_the_close_plans(xt, dev):
+    """A large contraction whose network predictions put the 256-wide tile on
+    one SM and on an SM pair within the margin of each other, and every other
+    plan far behind, is timed on its second call on those two plans only.
+    Whichever tile is kept, the residue products are exact, so D equals the
+    single-SM plan's result bit for bit."""
     from tests.test_gpu_permute import rand_host
     m = 3328  # 2 * m^3 = 7.4e10 FLOP
     pattern = "D(i,j)+=L(k,i)*R(k,j)"
@@ -150,24 +153,45 @@ def test_large_fused_prediction_times_the_sm_pair_tile(xt, dev):
     xt.tensor_contract(pattern, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(), 1.0,
                        plan=xt.make_plan(XB.METHOD_FUSED, tile_n=256), stream=dev.stream())
     want = dev.get(dd, np.float64, d.size)
-    nh = 8
-    n = 16 * nh + nh + nh * nh + nh + nh * 3 + 3
+    nh, P = 8, XB.SELECT_PLANS
+    n = 16 * nh + nh + nh * nh + nh + nh * P + P
     p = np.zeros(n, np.float32)
-    p[-3:] = 5.0
-    p[-1] = 1.0  # the network predicts the 256-wide tile fastest, far ahead of the rest
+    p[-P:] = 5.0
+    p[-P + 2] = 1.0  # the 256-wide tile on one SM ...
+    p[-P + 3] = 1.1  # ... and on an SM pair, within the margin
     XB.selector_install(nh, p, np.zeros(16, np.float32), np.ones(16, np.float32), margin=0.25, autotune=True)
     try:
         tiles = []
-        for _ in range(3):  # first: prediction; second: prediction against the SM pair; third: kept choice
+        for _ in range(3):  # first: prediction; second: the two close plans timed; third: kept choice
             dd = dev.put(d)
             xt.tensor_contract(pattern, O.R8, [m, m], dd.data_ptr(), [m, m], ld.data_ptr(), [m, m], rd.data_ptr(),
                                1.0, stream=dev.stream())
             got = dev.get(dd, np.float64, d.size)
             st = xt.last_contract_stats()
-            assert st.method == XB.METHOD_FUSED and st.tile_n == 256
+            assert st.method == XB.METHOD_FUSED and st.tile_n == 256 and st.moduli > 0
             tiles.append(st.tile_m)
             assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
         assert tiles[0] == 128 and tiles[1] == tiles[2] and tiles[2] in (128, 256)
     finally:
         XB.selector_install(0, None, None, None)
     xt.device_check(dev.stream())
+
+
+def test_fp64_only_plan_is_never_chosen_for_fp32(xt):
+    """The INT8-slice plan applies to FP64 data only: for an FP32 descriptor
+    the selector passes over it even when it is predicted fastest."""
+    nh, P = 8, XB.SELECT_PLANS
+    n = 16 * nh + nh + nh * nh + nh + nh * P + P
+    p = np.zeros(n, np.float32)
+    p[-P:] = 5.0
+    p[-P + 4] = 0.5  # slices predicted fastest
+    p[-P + 1] = 1.0
+    XB.selector_install(nh, p, np.zeros(16, np.float32), np.ones(16, np.float32))
+    try:
+        f64 = XB.contract_descriptor("D(i,j)+=L(k,i)*R(k,j)", 8, [512, 512], [512, 512], [512, 512])
+        f32 = XB.contract_descriptor("D(i,j)+=L(k,i)*R(k,j)", 4, [512, 512], [512, 512], [512, 512])
+        assert XB.selector_choose(f64)[0] == 4
+        assert XB.selector_choose(f32)[0] == 1
+        assert XB.selector_time(f64, 1000) > 0
+    finally:
+        XB.selector_install(0, None, None, None)

@@ -40,8 +40,8 @@ def test_regret_arithmetic():
 
 def test_host_inference_matches_the_reference_network():
     rng = np.random.default_rng(5)
-    nh = 32
-    n = 16 * nh + nh + nh * nh + nh + nh * 3 + 3
+    nh, P = 32, XB.SELECT_PLANS
+    n = 16 * nh + nh + nh * nh + nh + nh * P + P
     p = rng.normal(0, 0.3, n).astype(np.float32)
     mean = rng.normal(0, 1, 16).astype(np.float32)
     scale = rng.uniform(0.5, 2, 16).astype(np.float32)
@@ -49,8 +49,9 @@ def test_host_inference_matches_the_reference_network():
     try:
         for _ in range(20):
             x = rng.normal(0, 3, 16).astype(np.float32)
+            x[15] = 1.0  # an FP64 descriptor: every plan applies
             idx, y = XB.selector_choose(x)
-            ref, _ = mlp_ref.forward(p, ((x - mean) / scale)[None, :], 16, nh, 3)
+            ref, _ = mlp_ref.forward(p, ((x - mean) / scale)[None, :], 16, nh, P)
             assert np.allclose(y, ref[0], rtol=1e-4, atol=1e-4)
             assert idx == int(np.argmin(y))
     finally:
