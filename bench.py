@@ -719,10 +719,13 @@ def selector_case(X):
     F, T = d["features"], d["log_ms"]
     if T.shape[1] != len(S.PLANS):
         return None  # a corpus of another plan space
+    # the first 16000 entries train, the last 4000 are held out (rows without
+    # a label for a plan that applies to every data kind are left out of both)
     always = [i for i in range(T.shape[1]) if i not in S.FP64_ONLY]
     ok = np.isfinite(T[:, always]).all(axis=1)
+    split = int(0.8 * len(F))
+    n_train = int(ok[:split].sum())
     F, T = F[ok], T[ok]
-    n_train = int(0.8 * len(F))
     t0 = time.perf_counter()
     params, mean, scale, hist = S.train(F[:n_train], T[:n_train], hidden=128, epochs=150, seed=0, log_every=149)
     train_s = time.perf_counter() - t0
@@ -752,8 +755,9 @@ def selector_case(X):
     torch.cuda.synchronize()
     gpu_us = e0.elapsed_time(e1) / 10 * 1e3 / len(xn)
     net.close()
-    return {"corpus": f"{int(ok.sum())} labelled random contractions (seed 0), {n_train} train / "
-                      f"{len(F) - n_train} held out", "plans": S.PLAN_NAMES,
+    return {"corpus": f"{len(ok)} random contractions (seed 0), {int(ok.sum())} with every plan labelled: "
+                      f"{n_train} of the first {split} train, {len(F) - n_train} of the last {len(ok) - split} "
+                      f"held out", "plans": S.PLAN_NAMES,
             "learned": learned, "size_rule": rule, "always_one_plan_total_regret": always,
             "train_seconds": round(train_s, 1), "final_train_loss": round(hist[-1][1], 4) if hist else None,
             "selection_us_library": round(lib_us, 3), "selection_us_python": round(host_us, 2),

@@ -62,31 +62,35 @@ Selector& sel() {
   return S;
 }
 
+// Host inference of the network, layer by layer with the weight rows read in
+// order (W_l is [in][out]): out += x_i * W[i][:] over the inputs, plain
+// multiply-adds that the compiler vectorises.
 void mlp_host(const Selector& S, const float* x, float* y) {
-  const int F = TB_DESC_FEATURES, H = S.nh, O = TB_SELECT_PLANS;
+  constexpr int F = TB_DESC_FEATURES, O = TB_SELECT_PLANS, kMaxH = 4096;
+  const int H = S.nh;
   const float* W1 = S.p.data();
   const float* b1 = W1 + (size_t)F * H;
   const float* W2 = b1 + H;
   const float* b2 = W2 + (size_t)H * H;
   const float* W3 = b2 + H;
   const float* b3 = W3 + (size_t)H * O;
-  std::vector<float> xn(F), h1(H), h2(H);
+  alignas(64) float h1[kMaxH], h2[kMaxH];
+  float xn[F], out[O];
   for (int i = 0; i < F; ++i) xn[i] = (x[i] - S.mean[i]) / S.scale[i];
-  for (int o = 0; o < H; ++o) {
-    float a = b1[o];
-    for (int i = 0; i < F; ++i) a = std::fma(xn[i], W1[(size_t)i * H + o], a);
-    h1[o] = a > 0.f ? a : 0.f;
-  }
-  for (int o = 0; o < H; ++o) {
-    float a = b2[o];
-    for (int i = 0; i < H; ++i) a = std::fma(h1[i], W2[(size_t)i * H + o], a);
-    h2[o] = a > 0.f ? a : 0.f;
-  }
-  for (int o = 0; o < O; ++o) {
-    float a = b3[o];
-    for (int i = 0; i < H; ++i) a = std::fma(h2[i], W3[(size_t)i * O + o], a);
-    y[o] = a;
-  }
+  auto layer = [](const float* in, int n_in, const float* W, const float* b, int n_out, float* o, bool relu) {
+    for (int k = 0; k < n_out; ++k) o[k] = b[k];
+    for (int i = 0; i < n_in; ++i) {
+      const float xi = in[i];
+      const float* w = W + (size_t)i * n_out;
+      for (int k = 0; k < n_out; ++k) o[k] += xi * w[k];
+    }
+    if (relu)
+      for (int k = 0; k < n_out; ++k) o[k] = o[k] > 0.f ? o[k] : 0.f;
+  };
+  layer(xn, F, W1, b1, H, h1, true);
+  layer(h1, H, W2, b2, H, h2, true);
+  layer(h2, H, W3, b3, O, out, false);
+  for (int k = 0; k < O; ++k) y[k] = out[k];
 }
 
 }  // namespace
@@ -207,7 +211,10 @@ extern "C" int tb_selector_install(int n_hidden, const float* params, const floa
   S.cache.clear();
   S.seen.clear();
   if (!params) { S.on = false; return 0; }
-  if (n_hidden < 1 || !mean || !scale) { set_error("tb_selector_install: bad arguments"); return TB_ERR_INVALID_ARGS; }
+  if (n_hidden < 1 || n_hidden > 4096 || !mean || !scale) {
+    set_error("tb_selector_install: bad arguments (hidden units 1..4096)");
+    return TB_ERR_INVALID_ARGS;
+  }
   const int F = TB_DESC_FEATURES, O = TB_SELECT_PLANS;
   const size_t n = (size_t)F * n_hidden + n_hidden + (size_t)n_hidden * n_hidden + n_hidden + (size_t)n_hidden * O + O;
   S.p.assign(params, params + n);

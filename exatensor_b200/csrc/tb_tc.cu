@@ -137,6 +137,7 @@ constexpr bool moduli_table_matches() {
 }
 static_assert(moduli_table_matches(), "the gathers' compile-time moduli must be the plan's table");
 constexpr int kMinModuli = 8;
+constexpr int kMaxPassBlocks = 1023;  // K blocks of one exact INT32 pass (128^3 each, below 2^31)
 constexpr int kResidueBitsTarget = 46;  // operand bits kept by the default choice (INT8 slices keep 47)
 
 using u128 = unsigned __int128;
@@ -258,20 +259,24 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
   const int kblocks = (int)(Kpad * (i8 ? 1 : 2) / 128);  // 128-byte K blocks
   int S = 0, npa = 2, npb = 2;
   // R8/C8: modular residues (one exact INT8 GEMM per modulus, fewer than the
-  // slice pairs) unless the plan asks for INT8 slices, or the contraction is
-  // longer than one exact INT32 pass (1023 K blocks) or needs more moduli
+  // slice pairs) unless the plan asks for INT8 slices or the contraction
+  // needs more moduli; K ranges longer than one exact INT32 pass (1023 K
+  // blocks) are cut into equal chunks whose residues the epilogue adds mod m.
   ResiduePlan RP;
-  const bool resid = i8 && !(plan && (plan->slices > 0 || plan->moduli < 0)) && kblocks <= 1023 &&
-                     plan_residues(Kr, plan ? plan->moduli : 0, &RP);
+  const int res_nch = (kblocks + kMaxPassBlocks - 1) / kMaxPassBlocks;
+  const bool resid = i8 && !(plan && (plan->slices > 0 || plan->moduli < 0)) &&
+                     plan_residues(Kr, plan ? plan->moduli : 0, &RP) && RP.rs.n * res_nch <= kMaxProducts;
   if (i8 && plan && plan->moduli > 0 && !resid) {
     set_error("modular residues: %d moduli do not fit this contraction (K = %lld)", plan->moduli, (long long)Kr);
     return TB_ERR_INVALID_ARGS;
   }
   if (resid) {
-    for (int i = 0; i < RP.rs.n; ++i) {
-      passes.push_back({{i, i, 0, kblocks}});
-      shifts.push_back(RP.crt.mod[i]);  // the epilogue's modulus
-    }
+    const int chunk = (kblocks + res_nch - 1) / res_nch;
+    for (int i = 0; i < RP.rs.n; ++i)
+      for (int kb = 0; kb < kblocks; kb += chunk) {
+        passes.push_back({{i, i, kb, std::min(kblocks, kb + chunk)}});
+        shifts.push_back(RP.crt.mod[i]);  // the epilogue's modulus
+      }
     npa = npb = RP.rs.n;
   } else if (i8) {
     S = (plan && plan->slices > 0) ? plan->slices : kDefaultSlices;
@@ -445,6 +450,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
     P.mtiles = (int)(Mpad / TM); P.ntiles = (int)(Npad / BN);
     P.kblocks = (int)(Kpad * oes / 128);
     P.npass = (int)passes.size();
+    P.res_nch = resid ? res_nch : 1;
     int q = 0;
     for (size_t p = 0; p < passes.size(); ++p) {
       P.pass_first[p] = q;
@@ -497,7 +503,8 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       const cudaError_t ea = cplx ? smem_limit_once(crt_attr_c, crt_kernel<true>, kCrtTableBytes)
                                   : smem_limit_once(crt_attr_r, crt_kernel<false>, kCrtTableBytes);
       if (ea != cudaSuccess) { set_error("residue reconstruction smem attribute: %s", cudaGetErrorString(ea)); err = TB_ERR_CUDA; break; }
-      const unsigned cg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(Nc, 3 * num_sms()));
+      const int64_t groups = cplx ? (Nc + 1) / 2 : (Nc + 3) / 4;  // column groups of crt_kernel
+      const unsigned cg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, 3 * num_sms()));
       if (cplx) crt_kernel<true><<<cg, 256, kCrtTableBytes, s>>>(C);
       else crt_kernel<false><<<cg, 256, kCrtTableBytes, s>>>(C);
       count_launch();

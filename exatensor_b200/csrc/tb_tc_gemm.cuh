@@ -58,28 +58,30 @@ struct __align__(64) TcGemmParams {
   int nf_skip;                // 1: leave entries of flagged rows / columns to the non-finite fix-up
   uint8_t* res;               // EPI_RESID: residue planes
   int64_t res_ld, res_plane;  // EPI_RESID: column stride and plane stride (bytes)
+  int res_nch;                // EPI_RESID: passes per modulus (K chunks of at most
+                              // 1023 blocks each, added up mod m by the epilogue)
   unsigned int* sched;        // single-SM kernel: zeroed work-unit counter (dynamic
                               // scheduling), or null for a static round robin
   int l2hint;                 // 1: A tiles are loaded evict-first and B tiles
                               // evict-last (B planes are re-read by every m-tile)
 };
 
-// Work units of the GEMMs.  EPI_RESID: one (pass, tile) per unit with the
-// passes outermost -- every pass is one modulus with its own output plane,
-// so all CTAs work on one modulus at a time and its B plane can stay in L2.
-// Other epilogues: one tile with all its passes (they accumulate into D in
-// order).
+// Work units of the GEMMs.  EPI_RESID: one (modulus, tile) per unit with the
+// moduli outermost -- every modulus has its own output plane, so all CTAs
+// work on one modulus at a time and its B plane can stay in L2; the unit's
+// passes are that modulus's K chunks, in order.  Other epilogues: one tile
+// with all its passes (they accumulate into D in order).
 template <int EPI>
 __host__ __device__ __forceinline__ int gemm_units(const TcGemmParams& P) {
-  return EPI == EPI_RESID ? P.npass * P.mtiles * P.ntiles : P.mtiles * P.ntiles;
+  return EPI == EPI_RESID ? (P.npass / P.res_nch) * P.mtiles * P.ntiles : P.mtiles * P.ntiles;
 }
 struct GemmUnit { int t, p0, p1; };
 template <int EPI>
 __device__ __forceinline__ GemmUnit gemm_unit(const TcGemmParams& P, int u) {
   const int nt = P.mtiles * P.ntiles;
   if (EPI == EPI_RESID) {
-    const int p = u / nt;
-    return {u - p * nt, p, p + 1};
+    const int i = u / nt;
+    return {u - i * nt, i * P.res_nch, (i + 1) * P.res_nch};
   }
   return {u, 0, P.npass};
 }
@@ -157,10 +159,11 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
       // caller passes this pass's plane through P.res / res_plane.  v mod m
       // by a multiply-high with magic = floor(2^32 / m): the quotient estimate
       // is off by at most one either way, so two conditional corrections give
-      // the residue in [0, m) (integer pipes only; no division).
+      // the residue in [0, m) (integer pipes only; no division).  Later K
+      // chunks of a modulus (!first) add their residue to the stored one.
       if constexpr (std::is_same<EP, TcGemmParams>::value) {
         if (mval) {
-          uint8_t* col = P.res + dmo;  // dmo: this pass's plane offset + row
+          uint8_t* col = P.res + dmo;  // dmo: this modulus's plane offset + row
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             if (n0 + j >= P.N) break;
@@ -168,7 +171,12 @@ __device__ __forceinline__ void epilogue_pass(const EP& P, uint32_t tcol, bool m
             int rr = v - __mulhi(v, magic) * shift;
             rr += rr < 0 ? shift : 0;
             rr -= rr >= shift ? shift : 0;
-            col[(int64_t)(n0 + j) * P.res_ld] = (uint8_t)rr;
+            uint8_t* dst = col + (int64_t)(n0 + j) * P.res_ld;
+            if (!first) {
+              rr += *dst;
+              rr -= rr >= shift ? shift : 0;
+            }
+            *dst = (uint8_t)rr;
           }
         }
       }
@@ -387,9 +395,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
         const uint32_t aph = (acc_it >> 1) & 1;
         if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 1u, kEpilogueSleepNs))) break;
         tc_fence_after();
-        const bool first = (p == 0);
+        const bool first = EPI == EPI_RESID ? (p - w.p0 == 0) : (p == 0);
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C || EPI == EPI_RESID) ? P.pass_shift[p] : 0;
-        const int64_t dmp = EPI == EPI_RESID ? (int64_t)p * P.res_plane + m : dmo;
+        const int64_t dmp = EPI == EPI_RESID ? (int64_t)(p / P.res_nch) * P.res_plane + m : dmo;
         epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN),
                                EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, first, shift,
                                EPI == EPI_RESID ? P.pass_magic[p] : 0);
@@ -544,9 +552,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
         if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 1u, kEpilogueSleepNs))) break;
         tc_fence_after();
         const int shift = (EPI == EPI_OZAKI_R || EPI == EPI_OZAKI_C || EPI == EPI_RESID) ? P.pass_shift[p] : 0;
-        const int64_t dmp = EPI == EPI_RESID ? (int64_t)p * P.res_plane + m : dmo;
+        const int64_t dmp = EPI == EPI_RESID ? (int64_t)(p / P.res_nch) * P.res_plane + m : dmo;
         epilogue_pass<BN, EPI>(P, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN),
-                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb, p == 0, shift,
+                               EPI == EPI_RESID ? m < P.M : mval, dmp, re, nb,
+                               EPI == EPI_RESID ? (p - w.p0 == 0) : (p == 0), shift,
                                EPI == EPI_RESID ? P.pass_magic[p] : 0);
         tc_fence_before();
         __syncwarp();

@@ -727,12 +727,15 @@ __device__ __forceinline__ double u128_to_double(unsigned __int128 x) {
 constexpr int kCrtTableBytes = kMaxModuli * 256 * 16;
 struct alignas(16) CrtEntry { uint64_t lo, hi; };
 
-__device__ __forceinline__ double crt_value(const CrtParams& P, const CrtEntry* tab, int64_t col, int64_t m) {
+// Residues of D entry (col, m) from the n planes (independent byte loads).
+__device__ __forceinline__ void crt_load(const CrtParams& P, int64_t col, int64_t m, uint32_t (&r)[kMaxModuli]) {
   const uint8_t* rp = P.res + col * P.res_ld + m;
-  // all residue loads first (independent), then the table lookups
-  int r[kMaxModuli];
 #pragma unroll
-  for (int i = 0; i < kMaxModuli; ++i) r[i] = i < P.n ? rp[i * P.res_plane] : 0;
+  for (int i = 0; i < kMaxModuli; ++i) r[i] = i < P.n ? rp[i * P.res_plane] : 0u;
+}
+
+// The exact integer from its residues, in FP64 (about one rounding).
+__device__ __forceinline__ double crt_combine(const CrtParams& P, const CrtEntry* tab, const uint32_t (&r)[kMaxModuli]) {
   uint64_t lo = 0, hi = 0;
 #pragma unroll
   for (int i = 0; i < kMaxModuli; ++i) {
@@ -754,6 +757,10 @@ __device__ __forceinline__ double crt_value(const CrtParams& P, const CrtEntry* 
   return neg ? -v : v;
 }
 
+// Each CTA takes groups of four residue columns (four real D columns, or two
+// complex ones) and each thread, for every row it owns, issues the residue
+// loads of the whole group before combining them, so that four entries'
+// loads are in flight per thread.
 template <bool CPLX>
 __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
   extern __shared__ __align__(16) unsigned char crt_smem[];
@@ -770,31 +777,57 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     tab[e] = t;
   }
   __syncthreads();
-  for (int64_t n = blockIdx.x; n < P.cols; n += gridDim.x) {
-    const int ce = P.colexp[CPLX ? 2 * n : n];
-    if (ce >= kNonFiniteExp) continue;  // flagged column: the fix-up's
-    const int64_t dno = P.dn[n];
+  constexpr int G = CPLX ? 2 : 4;   // D entries per group
+  constexpr int RC = CPLX ? 2 : 1;  // residue columns per D entry
+  const int64_t ngroups = (P.cols + G - 1) / G;
+  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    int ce[G];
+    int64_t dno[G];
+    bool cok[G];
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < G; ++c) {
+      const int64_t n = grp * G + c;
+      cok[c] = n < P.cols;
+      ce[c] = cok[c] ? P.colexp[CPLX ? 2 * n : n] : 0;
+      cok[c] = cok[c] && ce[c] < kNonFiniteExp;  // flagged column: the fix-up's
+      dno[c] = cok[c] ? P.dn[n] : 0;
+      any = any || cok[c];
+    }
+    if (!any) continue;
     for (int64_t m = threadIdx.x; m < P.rows; m += blockDim.x) {
       const int re = P.rowexp[m];
       if (re >= kNonFiniteExp) continue;  // flagged row: the fix-up's
-      const int e = re + ce - P.shift;
-      const int64_t o = P.dm[m] + dno;
-      if constexpr (!CPLX) {
-        double* D = (double*)P.D;
-        const double v = P.ar * scale2(crt_value(P, tab, n, m), e);
-        D[o] = P.br == 0.0 ? v : fma(P.br, D[o], v);
-      } else {
-        double2* D = (double2*)P.D;
-        const double xr = scale2(crt_value(P, tab, 2 * n, m), e), xi = scale2(crt_value(P, tab, 2 * n + 1, m), e);
-        double2 v;
-        v.x = P.ar * xr - P.ai * xi;
-        v.y = P.ar * xi + P.ai * xr;
-        if (P.br != 0.0 || P.bi != 0.0) {
-          const double2 d = D[o];
-          v.x += P.br * d.x - P.bi * d.y;
-          v.y += P.br * d.y + P.bi * d.x;
+      uint32_t r[G * RC][kMaxModuli];
+#pragma unroll
+      for (int c = 0; c < G; ++c)
+#pragma unroll
+        for (int j = 0; j < RC; ++j) {
+          if (cok[c]) crt_load(P, (grp * G + c) * RC + j, m, r[c * RC + j]);
         }
-        D[o] = v;
+      const int64_t dmo = P.dm[m];
+#pragma unroll
+      for (int c = 0; c < G; ++c) {
+        if (!cok[c]) continue;
+        const int e = re + ce[c] - P.shift;
+        const int64_t o = dmo + dno[c];
+        if constexpr (!CPLX) {
+          double* D = (double*)P.D;
+          const double v = P.ar * scale2(crt_combine(P, tab, r[c]), e);
+          D[o] = P.br == 0.0 ? v : fma(P.br, D[o], v);
+        } else {
+          double2* D = (double2*)P.D;
+          const double xr = scale2(crt_combine(P, tab, r[2 * c]), e), xi = scale2(crt_combine(P, tab, r[2 * c + 1]), e);
+          double2 v;
+          v.x = P.ar * xr - P.ai * xi;
+          v.y = P.ar * xi + P.ai * xr;
+          if (P.br != 0.0 || P.bi != 0.0) {
+            const double2 d = D[o];
+            v.x += P.br * d.x - P.bi * d.y;
+            v.y += P.br * d.y + P.bi * d.x;
+          }
+          D[o] = v;
+        }
       }
     }
   }

@@ -45,14 +45,15 @@ def test_fused_r8_square(xt, dev):
     assert st.moduli == 0 and st.slices == 6 and st.passes >= 6 and st.products == 21
 
 
-@pytest.mark.parametrize("dtk,bits", [(O.R8, 20), (O.C8, 19)])
-def test_residue_path_is_exact_on_integer_data(xt, dev, dtk, bits):
+@pytest.mark.parametrize("dtk,bits,K", [(O.R8, 20, 4096), (O.C8, 19, 4096), (O.R8, 16, 200000)])
+def test_residue_path_is_exact_on_integer_data(xt, dev, dtk, bits, K):
     """Integer operands of up to `bits` bits: every step of the residue path is
     exact (the row scaling keeps the integers, the residues are the integers'
     residues, the INT8 products are exact, the CRT recovers the exact sum), so
-    D must equal the integer product bit for bit."""
+    D must equal the integer product bit for bit.  K = 200000 is longer than
+    one exact INT32 pass: its residues come from two K chunks added mod m."""
     rng = np.random.default_rng(4)
-    M, N, K = 512, 384, 4096
+    M, N = (512, 384) if K <= 4096 else (128, 96)
     ints = lambda n: rng.integers(-(2 ** bits), 2 ** bits + 1, size=n)
     if dtk == O.R8:
         l, r = ints(K * M).astype(np.float64), ints(K * N).astype(np.float64)
@@ -74,6 +75,7 @@ def test_residue_path_is_exact_on_integer_data(xt, dev, dtk, bits):
     xt.device_check(dev.stream())
     st = xt.last_contract_stats()
     assert st.method == XB.METHOD_FUSED and st.moduli >= 8
+    assert st.passes == st.moduli * (1 if K <= 4096 else 2)
     assert np.array_equal(got, want)
 
 

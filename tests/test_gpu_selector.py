@@ -77,8 +77,8 @@ def test_trained_selector_beats_the_size_rule(xt):
     assert T.shape[1] == XB.SELECT_PLANS == len(S.PLANS)
     always = [i for i in range(T.shape[1]) if i not in S.FP64_ONLY]
     ok = np.isfinite(T[:, always]).all(axis=1)
+    n_train = int(ok[:int(0.8 * len(F))].sum())  # the first 80% of the entries train
     F, T = F[ok], T[ok]
-    n_train = int(0.8 * len(F))
     params, mean, scale, _ = S.train(F[:n_train], T[:n_train], hidden=128, epochs=150, seed=0)
     pred = S.predict(params, mean, scale, F[n_train:], hidden=128)
     learned = S.evaluate(T[n_train:], S.choose(pred, F[n_train:]))
