@@ -157,12 +157,15 @@ int selector_pick(const float* f, int* idx, unsigned* tune_mask, uint64_t* key) 
   }
   *key = h;
   // Timing candidates costs a few contractions: only worth it for large ones,
-  // and only for the plans predicted within the margin of the best.
-  constexpr float kTuneMinLog2Flops = 34.0f;  // about 1.7e10 FLOP
+  // and only for the plans predicted within the margin of the best -- or, for
+  // very large ones (beyond the corpus's 4 GiB footprints the network
+  // extrapolates, and a wrong pick costs most), for every plan.
+  constexpr float kTuneMinLog2Flops = 34.0f;     // about 1.7e10 FLOP
+  constexpr float kTuneAllMinLog2Flops = 38.0f;  // about 2.7e11 FLOP
   unsigned mask = 0;
   if (S.autotune && f[3] >= kTuneMinLog2Flops)
     for (int i = 0; i < TB_SELECT_PLANS; ++i)
-      if (plan_applies(f, i) && y[i] - y[best] < S.margin) mask |= 1u << i;
+      if (plan_applies(f, i) && (y[i] - y[best] < S.margin || f[3] >= kTuneAllMinLog2Flops)) mask |= 1u << i;
   if (mask == (1u << best)) mask = 0;  // nothing close: the prediction stands
   if (mask) {
     auto it = S.cache.find(h);

@@ -225,10 +225,13 @@ def predict(params, mean, scale, Xf, hidden=128):
 
     import exatensor_b200 as X
     Xn = ((np.asarray(Xf, np.float32) - mean) / scale).astype(np.float32)
-    net = X.MLP(Xn.shape[1], hidden, len(PLANS), max_batch=1024)
+    nin = Xn.shape[1]
+    # outputs from the parameter count: nin*h + h + h*h + h + h*o + o
+    n_out = (len(params) - nin * hidden - 2 * hidden - hidden * hidden) // (hidden + 1)
+    net = X.MLP(nin, hidden, n_out, max_batch=1024)
     net.set_params(params)
     dx = torch.from_numpy(Xn).cuda()
-    dy = torch.empty((len(Xn), len(PLANS)), dtype=torch.float32, device="cuda")
+    dy = torch.empty((len(Xn), n_out), dtype=torch.float32, device="cuda")
     net.forward(dx.data_ptr(), len(Xn), dy.data_ptr())
     torch.cuda.synchronize()
     out = dy.cpu().numpy()

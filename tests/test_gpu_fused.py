@@ -169,20 +169,30 @@ def test_kat_single_block_40(xt, dev):
 def test_long_k_splits_exact_int32_passes(xt, dev):
     """K = 131200 (1025 K blocks) with every slice below the top equal to -128:
     each K block adds exactly 2^21 to an INT32 accumulator, so a pass may hold at
-    most 1023 blocks.  The slice pairs must be split along K into exact passes;
-    an overflow would show as a grossly wrong D."""
+    most 1023 blocks.  The slice pairs (INT8 slices, on request) must be split
+    along K into exact passes, and the residue products (the default) into K
+    chunks whose residues add up mod m; an overflow would show as a grossly
+    wrong D."""
     from fractions import Fraction
     K, M, N = 131200, 128, 64
     word = 63 * 2 ** 48 + 128 * sum(2 ** (8 * i) for i in range(6))
     v = -word / 2.0 ** 55                      # balanced digits (-63, -128, ..., -128)
     assert Fraction(v) == Fraction(-word, 2 ** 55)
     l = np.full(K * M, v); r = np.full(K * N, v)
-    d = np.zeros(M * N)
-    got = run_gpu(xt, dev, "D(i,j)+=L(k,i)*R(k,j)", d, [M, N], l, [K, M], r, [K, N], 0.5, True, XB.METHOD_FUSED)
-    st = xt.last_contract_stats()
-    assert st.method == XB.METHOD_FUSED and st.products == 21 and st.passes > 6
     want = float(Fraction(v) ** 2 * K / 2)
-    assert np.allclose(got, want, rtol=1e-13, atol=0), (got[:4], want)
+    pat = "D(i,j)+=L(k,i)*R(k,j)"
+    for plan in (xt.make_plan(XB.METHOD_FUSED, moduli=-1), xt.make_plan(XB.METHOD_FUSED)):
+        dd, ld, rd = dev.put(np.zeros(M * N)), dev.put(l), dev.put(r)
+        xt.tensor_contract(pat, O.R8, [M, N], dd.data_ptr(), [K, M], ld.data_ptr(), [K, N], rd.data_ptr(), 0.5,
+                           accumulative=True, plan=plan, stream=dev.stream())
+        got = dev.get(dd, np.float64, M * N)
+        st = xt.last_contract_stats()
+        assert st.method == XB.METHOD_FUSED
+        if st.moduli:
+            assert st.products == st.moduli and st.passes == 2 * st.moduli
+        else:
+            assert st.products == 21 and st.passes > 6
+        assert np.allclose(got, want, rtol=1e-13, atol=0), (st.moduli, got[:4], want)
 
 
 @pytest.mark.parametrize("dtk", [O.R8, O.C8, O.R4, O.C4])
