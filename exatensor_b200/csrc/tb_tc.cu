@@ -503,7 +503,7 @@ int contract_fused(const Matricization& Z0, int dtk, const int* ddims, void* d, 
       const cudaError_t ea = cplx ? smem_limit_once(crt_attr_c, crt_kernel<true>, kCrtTableBytes)
                                   : smem_limit_once(crt_attr_r, crt_kernel<false>, kCrtTableBytes);
       if (ea != cudaSuccess) { set_error("residue reconstruction smem attribute: %s", cudaGetErrorString(ea)); err = TB_ERR_CUDA; break; }
-      const int64_t groups = cplx ? (Nc + 1) / 2 : (Nc + 3) / 4;  // column groups of crt_kernel
+      const int64_t groups = Nc;  // column groups of crt_kernel (one D column each)
       const unsigned cg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, 3 * num_sms()));
       if (cplx) crt_kernel<true><<<cg, 256, kCrtTableBytes, s>>>(C);
       else crt_kernel<false><<<cg, 256, kCrtTableBytes, s>>>(C);
