@@ -88,18 +88,16 @@ struct tb_bsc_plan_s {
   int2* g_map = nullptr;           // gather grouped launch
   int64_t rm_ctas = 0, g_ctas = 0;
   int rm_gy = 1, g_gy = 1;
-  tb::BscLOp* lops = nullptr;
-  tb::BscROp* rops[2] = {nullptr, nullptr};   // tensor maps for BN = 128 / 256
   CUtensorMap* maps = nullptr;
   tb::BscDBlk* dblks = nullptr;
-  tb::BscPair* pairs = nullptr;
   tb::BscItem* items[2] = {nullptr, nullptr};  // items for BN = 128 / 256
   tb::BscPass* passes = nullptr;   // per output block, for the current slice count
-  tb::BscChunk* chunks = nullptr;
-  size_t passes_cap = 0, chunks_cap = 0;
-  std::vector<tb::BscDBlk> dblk_host;            // output blocks (pass ranges rewritten per slice count)
+  tb::BscRun* runs = nullptr;
+  size_t passes_cap = 0, runs_cap = 0;
+  std::vector<tb::BscDBlk> dblk_host;            // output blocks (pass and run ranges rewritten per slice count)
   std::vector<std::vector<int>> dpair_kb;       // K blocks of every pair of every output block
   std::vector<int> dpair0;                      // first global pair index of every output block
+  std::vector<const CUtensorMap*> pair_maps;    // per global pair: A map, B map (BN 128), B map (BN 256)
   unsigned* queue = nullptr;
   // graph of the current configuration
   cudaGraph_t graph = nullptr;
@@ -154,9 +152,9 @@ int bsc_enqueue(tb_bsc_plan_s* pl, cudaStream_t s) {
   if (cudaMemsetAsync(pl->queue, 0, sizeof(unsigned), s) != cudaSuccess) return TB_ERR_CUDA;
   BscParams P;
   std::memset(&P, 0, sizeof(P));
-  P.lops = pl->lops; P.rops = pl->rops[bi]; P.dblks = pl->dblks; P.pairs = pl->pairs; P.items = pl->items[bi];
+  P.dblks = pl->dblks; P.items = pl->items[bi];
   P.queue = pl->queue; P.nitems = pl->n_items[bi];
-  P.passes = pl->passes; P.chunks = pl->chunks;
+  P.passes = pl->passes; P.runs = pl->runs;
   P.ar = pl->ar; P.ai = pl->ai; P.br = pl->br; P.bi = pl->bi;
   P.err = device_error_word();
   const int grid = std::max(1, std::min(P.nitems, num_sms()));
@@ -173,7 +171,9 @@ void drop_graph(tb_bsc_plan_s* pl) {
   pl->graph = nullptr;
 }
 
-// Accumulator passes of every output block for the current slice count.
+// Accumulator passes of every output block for the current slice count, and
+// their runs (what the producer streams: one block pair's K range in one
+// plane pair).
 // INT8: slice pairs (i, j) of equal i + j share a pass while the K blocks
 // summed into it stay within 1023 (each adds at most 128^3 = 2^21, so the
 // INT32 sum is exact); a product over many pairs is split at pair boundaries.
@@ -182,28 +182,39 @@ void drop_graph(tb_bsc_plan_s* pl) {
 // the FP32 accumulation of the tensor cores loses accuracy with the length
 // of the sum, and the epilogue adds each pass into D with one rounding.
 constexpr int kBscBf16PassKBlocks = 32;
-void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, std::vector<BscChunk>& chunks,
+void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, std::vector<BscRun>& runs,
                  std::vector<BscDBlk>* dbl) {
   passes.clear();
-  chunks.clear();
+  runs.clear();
+  const bool maps = !pl->pair_maps.empty();
+  auto new_pass = [&](int shift) { passes.push_back(BscPass{(int)runs.size(), 0, shift, 0}); };
+  // run of global pair q over K blocks [k0, k1) in planes (a, b), added to the last pass
+  auto add_run = [&](int q, int a, int b, int k0, int k1) {
+    BscRun r{};
+    if (maps) {
+      r.amap = pl->pair_maps[3 * (size_t)q];
+      r.bmap[0] = pl->pair_maps[3 * (size_t)q + 1];
+      r.bmap[1] = pl->pair_maps[3 * (size_t)q + 2];
+    }
+    r.a = a; r.b = b; r.kb0 = k0; r.kb1 = k1;
+    runs.push_back(r);
+    passes.back().nrun++;
+  };
   for (size_t d = 0; d < pl->dpair_kb.size(); ++d) {
     const std::vector<int>& kb = pl->dpair_kb[d];
     const int p0 = pl->dpair0[d], np = (int)kb.size();
-    const int pass0 = (int)passes.size();
+    const int pass0 = (int)passes.size(), run0 = (int)runs.size();
     if (!pl->i8) {
       int load = kBscBf16PassKBlocks;  // forces a new pass first
       for (int q = 0; q < np; ++q) {
         for (int k0 = 0; k0 < kb[q];) {
           if (load >= kBscBf16PassKBlocks) {
-            passes.push_back(BscPass{(int)chunks.size(), 0, 0, 0});
+            new_pass(0);
             load = 0;
           }
           const int n = std::min(kBscBf16PassKBlocks - load, kb[q] - k0);
-          const bool whole = k0 == 0 && n == kb[q];
           const int terms[3][2] = {{0, 0}, {0, 1}, {1, 0}};
-          for (auto& t : terms)
-            chunks.push_back(BscChunk{t[0], t[1], p0 + q, p0 + q + 1, whole ? 0 : k0, whole ? 0 : k0 + n});
-          passes.back().nchunk += 3;
+          for (auto& t : terms) add_run(p0 + q, t[0], t[1], k0, k0 + n);
           load += n;
           k0 += n;
         }
@@ -214,40 +225,41 @@ void plan_passes(const tb_bsc_plan_s* pl, int S, std::vector<BscPass>& passes, s
         for (int i = 1; i < dsum; ++i) {
           const int j = dsum - i;
           if (i > S || j > S) continue;
-          int q = 0;
-          while (q < np) {
+          for (int q = 0; q < np; ++q) {
             if (load + kb[q] > 1023) {
-              passes.push_back(BscPass{(int)chunks.size(), 0, 8 * dsum - 2, 0});
+              new_pass(8 * dsum - 2);
               load = 0;
             }
-            int e = q, l = load;
-            while (e < np && l + kb[e] <= 1023) l += kb[e++];
-            chunks.push_back(BscChunk{i - 1, j - 1, p0 + q, p0 + e, 0, 0});
-            passes.back().nchunk++;
-            load = l;
-            q = e;
+            add_run(p0 + q, i - 1, j - 1, 0, kb[q]);
+            load += kb[q];
           }
         }
       }
     }
+    for (size_t p = pass0; p < passes.size(); ++p) {
+      runs[passes[p].run0].flags |= kBscRunFirst;
+      runs[passes[p].run0 + passes[p].nrun - 1].flags |= kBscRunLast;
+    }
     if (dbl) {
       (*dbl)[d].pass0 = pass0;
       (*dbl)[d].npass = (int)passes.size() - pass0;
+      (*dbl)[d].run0 = run0;
+      (*dbl)[d].nrun = (int)runs.size() - run0;
     }
   }
 }
 
 int build_passes(tb_bsc_plan_s* pl, cudaStream_t s) {
   std::vector<BscPass> passes;
-  std::vector<BscChunk> chunks;
-  plan_passes(pl, pl->slices, passes, chunks, &pl->dblk_host);
-  if (passes.size() > pl->passes_cap || chunks.size() > pl->chunks_cap) {
+  std::vector<BscRun> runs;
+  plan_passes(pl, pl->slices, passes, runs, &pl->dblk_host);
+  if (passes.size() > pl->passes_cap || runs.size() > pl->runs_cap) {
     set_error("block-sparse plan: pass table larger than allocated");
     return TB_ERR_LIMIT;
   }
   if (cudaMemcpyAsync(pl->passes, passes.data(), passes.size() * sizeof(BscPass), cudaMemcpyHostToDevice, s) !=
           cudaSuccess ||
-      cudaMemcpyAsync(pl->chunks, chunks.data(), chunks.size() * sizeof(BscChunk), cudaMemcpyHostToDevice, s) !=
+      cudaMemcpyAsync(pl->runs, runs.data(), runs.size() * sizeof(BscRun), cudaMemcpyHostToDevice, s) !=
           cudaSuccess ||
       cudaMemcpyAsync(pl->dblks, pl->dblk_host.data(), pl->dblk_host.size() * sizeof(BscDBlk), cudaMemcpyHostToDevice,
                       s) != cudaSuccess ||
@@ -510,57 +522,59 @@ int plan_create(const char* pattern, int dtk, int ntasks, const tb_block_task_t*
   }
   pl->maps = upload(pl, maps, &err, s);
   if (err) { plan_free(pl); return err; }
-  std::vector<BscLOp> lops(A.size());
-  for (size_t i = 0; i < A.size(); ++i)
-    lops[i] = BscLOp{pl->maps + i, pl->rowexp + A[i].e_off, (int)(A[i].Kpad * oes / 128), 0};
-  std::vector<BscROp> r128(B.size()), r256(B.size());
-  for (size_t i = 0; i < B.size(); ++i) {
-    r128[i] = BscROp{pl->maps + A.size() + i, pl->rowexp + B[i].e_off, (int)(B[i].Kpad * oes / 128), 0};
-    r256[i] = BscROp{pl->maps + A.size() + B.size() + i, pl->rowexp + B[i].e_off, (int)(B[i].Kpad * oes / 128), 0};
-  }
-  pl->lops = upload(pl, lops, &err, s);
-  pl->rops[0] = upload(pl, r128, &err, s);
-  pl->rops[1] = upload(pl, r256, &err, s);
-  // output blocks, pairs and work items (largest first)
+  // output blocks, their pairs (tensor maps and K blocks) and work items (largest first)
   std::vector<BscDBlk>& dbl = pl->dblk_host;
   dbl.assign(Ds.size(), BscDBlk{});
-  std::vector<BscPair> prs;
   pl->dpair_kb.assign(Ds.size(), {});
   pl->dpair0.assign(Ds.size(), 0);
+  pl->pair_maps.clear();
+  int npairs = 0;
   for (size_t d = 0; d < Ds.size(); ++d) {
     dbl[d].D = Ds[d].ptr;
     dbl[d].dm = pl->tables + dm_off[d];
     dbl[d].dn = pl->tables + dn_off[d];
+    // the block's A (B) blocks share one exponent component
+    dbl[d].rowexp = pl->rowexp + A[Ds[d].pairs[0].first].e_off;
+    dbl[d].colexp = pl->rowexp + B[Ds[d].pairs[0].second].e_off;
     dbl[d].M = (int)Ds[d].M; dbl[d].N = (int)Ds[d].N;
-    pl->dpair0[d] = (int)prs.size();
+    pl->dpair0[d] = npairs;
     for (auto& p : Ds[d].pairs) {
-      prs.push_back(BscPair{p.first, p.second});
+      pl->pair_maps.push_back(pl->maps + p.first);
+      pl->pair_maps.push_back(pl->maps + A.size() + p.second);
+      pl->pair_maps.push_back(pl->maps + A.size() + B.size() + p.second);
       pl->dpair_kb[d].push_back((int)(A[p.first].Kpad * oes / 128));
+      ++npairs;
     }
   }
   {
     std::vector<BscPass> ps;
-    std::vector<BscChunk> cs;
-    plan_passes(pl, pl->i8 ? pl->max_slices : 2, ps, cs, nullptr);  // the largest tables any slice count needs
+    std::vector<BscRun> rs;
+    plan_passes(pl, pl->i8 ? pl->max_slices : 2, ps, rs, nullptr);  // the largest tables any slice count needs
     pl->passes_cap = ps.size();
-    pl->chunks_cap = cs.size();
+    pl->runs_cap = rs.size();
     pl->passes = (BscPass*)dalloc(ps.size() * sizeof(BscPass), &err);
     if (pl->passes) pl->allocs.push_back(pl->passes);
-    pl->chunks = (BscChunk*)dalloc(cs.size() * sizeof(BscChunk), &err);
-    if (pl->chunks) pl->allocs.push_back(pl->chunks);
+    pl->runs = (BscRun*)dalloc(rs.size() * sizeof(BscRun), &err);
+    if (pl->runs) pl->allocs.push_back(pl->runs);
   }
   pl->dblks = upload(pl, dbl, &err, s);
-  pl->pairs = upload(pl, prs, &err, s);
   if (!err) err = build_passes(pl, s);
+  // Items of one output block go in bands of G N tiles, every M tile of a band
+  // before the next band: the CTAs working at the same time then share each
+  // A tile slab among about G items and each B slab among about 148 / G, so
+  // that fewer distinct slabs pass through L2 (G balances the A slab, 128
+  // rows, against the B slab, BN rows: about sqrt(148 * 128 / BN)).
   for (int bi = 0; bi < 2; ++bi) {
     const int BN = bi ? 256 : 128;
+    const int G = std::max(1, (int)std::lround(std::sqrt((double)num_sms() * 128.0 / BN)));
     std::vector<std::pair<int64_t, BscItem>> its;
     for (size_t d = 0; d < Ds.size(); ++d) {
       int64_t cost = 0;
       for (auto& p : Ds[d].pairs) cost += A[p.first].Kpad;
       const int mt = (int)((Ds[d].M + 127) / 128), nt = (int)((Ds[d].N + BN - 1) / BN);
-      for (int x = 0; x < mt; ++x)
-        for (int y = 0; y < nt; ++y) its.push_back({cost, BscItem{(int)d, x, y, 0}});
+      for (int y0 = 0; y0 < nt; y0 += G)
+        for (int x = 0; x < mt; ++x)
+          for (int y = y0; y < std::min(nt, y0 + G); ++y) its.push_back({cost, BscItem{(int)d, x, y, 0}});
     }
     std::stable_sort(its.begin(), its.end(), [](const std::pair<int64_t, BscItem>& a, const std::pair<int64_t, BscItem>& b) {
       return a.first > b.first;

@@ -11,7 +11,12 @@
 // pairs inside each TMEM accumulator pass (the operand blocks of an output
 // block share row and column scales, so that INT32 sums over several pairs
 // stay exact) and hands each pass to the epilogue, which adds it into the
-// output tile; pairs that share an output block therefore never race.  Roles as in tc_gemm_kernel:
+// output tile; pairs that share an output block therefore never race.  The
+// host flattens each output block's passes into runs (one pair's K range in
+// one plane pair, with its tensor maps), so that the producer and the MMA
+// issuer read one record per run, fetched two runs ahead, instead of chasing
+// pass -> chunk -> pair -> operand records at every pair boundary.  Roles as
+// in tc_gemm_kernel:
 //   warp 0   queue + TMA producer (one lane); it publishes every item it takes
 //            in a small shared-memory ring read by the other roles
 //   warp 1   TMEM allocation and the single MMA-issuing thread
@@ -24,48 +29,43 @@
 
 namespace tb {
 
-struct __align__(16) BscLOp {   // left operand block (A planes)
-  const CUtensorMap* map;       // (Kpad, Mpad, planes)
-  const int* rowexp;            // INT8 slices: per-row scale exponents
-  int kblocks;                  // 128-byte K blocks
-  int pad_;
-};
-struct __align__(16) BscROp {   // right operand block (B planes)
-  const CUtensorMap* map;       // (Kpad, Npad, planes)
-  const int* colexp;
-  int kblocks;
-  int pad_;
-};
 struct __align__(16) BscDBlk {  // output block
   void* D;
   const int64_t* dm;            // D offset of row m
   const int64_t* dn;            // D offset of column n
+  const int* rowexp;            // INT8 slices: per-row scale exponents (shared by the block's A blocks)
+  const int* colexp;            // INT8 slices: per-column scale exponents (shared by its B blocks)
   int M, N;
   int pass0, npass;             // its accumulator passes: passes[pass0 .. pass0 + npass)
+  int run0, nrun;               // its runs: runs[run0 .. run0 + nrun), pass after pass
 };
-struct BscPair { int l, r; };
 struct BscItem { int d, mt, nt, pad_; };
-// A pass is one exact TMEM accumulator: chunks[chunk0 .. chunk0 + nchunk),
-// each the product of plane a of A and plane b of B summed over the pairs
-// pairs[p0 .. p1) of the output block (all their K blocks).  INT8 slices: the
-// pass's weight is 2^-shift; the operand blocks of one output block share
-// their row (column) scales, so their products add up exactly in INT32.
-struct BscPass { int chunk0, nchunk, shift, pad_; };
-// kb1 > 0: the chunk covers only pair p0, over its K blocks [kb0, kb1)
-// (split-BF16 passes end inside a pair's K range); else all K blocks of the
-// pairs p0 .. p1 - 1.
-struct BscChunk { int a, b, p0, p1, kb0, kb1; };
+// A pass is one exact TMEM accumulator that the epilogue adds into the output
+// tile.  INT8 slices: its weight is 2^-shift; the operand blocks of one output
+// block share their row (column) scales, so products of several block pairs
+// add up exactly in INT32 within a pass.
+struct BscPass { int run0, nrun, shift, pad_; };
+// A run is what the producer streams without looking anything up: K blocks
+// [kb0, kb1) of plane a of one A block and plane b of one B block (tensor maps
+// for both N tiles).  The runs of an output block are flat, pass after pass;
+// flags mark the first and the last run of each pass.
+constexpr int kBscRunFirst = 1, kBscRunLast = 2;
+struct __align__(16) BscRun {
+  const CUtensorMap* amap;      // (Kpad, Mpad, planes)
+  const CUtensorMap* bmap[2];   // (Kpad, Npad, planes), boxes for BN = 128 / 256
+  int a, b;                     // planes
+  int kb0, kb1;                 // 128-byte K blocks
+  int flags;
+  int pad_;
+};
 
 constexpr int kBscRing = 4;
 
 struct __align__(64) BscParams {
-  const BscLOp* lops;
-  const BscROp* rops;
   const BscDBlk* dblks;
-  const BscPair* pairs;
   const BscItem* items;
   const BscPass* passes;
-  const BscChunk* chunks;
+  const BscRun* runs;
   unsigned int* queue;          // next item (zeroed before every launch)
   int nitems;
   double ar, ai, br, bi;        // beta applies to the first pass of each tile
@@ -94,12 +94,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* smA = base;
-  unsigned char* smB = base + (size_t)kStagesTC * 128 * 128;
-  BscSmemBarriers* bars = (BscSmemBarriers*)(smB + (size_t)kStagesTC * BN * 128);
+  constexpr int kStages = kStagesTC;
+  unsigned char* smB = base + (size_t)kStages * 128 * 128;
+  BscSmemBarriers* bars = (BscSmemBarriers*)(smB + (size_t)kStages * BN * 128);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStagesTC; ++s) { mbar_init(&bars->full[s], 1); mbar_init(&bars->empty[s], 1); }
+    for (int s = 0; s < kStages; ++s) { mbar_init(&bars->full[s], 1); mbar_init(&bars->empty[s], 1); }
     for (int a = 0; a < 2; ++a) { mbar_init(&bars->acc_full[a], 1); mbar_init(&bars->acc_empty[a], 4); }
     for (int s = 0; s < kBscRing; ++s) { mbar_init(&bars->item_full[s], 1); mbar_init(&bars->item_empty[s], 5); }
     fence_barrier_init();
@@ -128,27 +129,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
         if (cur < 0) break;
         const BscItem I = P.items[cur];
         const BscDBlk Dd = P.dblks[I.d];
-        for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p) {
-          const BscPass ps = P.passes[p];
-          for (int c = ps.chunk0; c < ps.chunk0 + ps.nchunk && ok; ++c) {
-            const BscChunk ch = P.chunks[c];
-            for (int pp = ch.p0; pp < ch.p1 && ok; ++pp) {
-              const BscPair pr = P.pairs[pp];
-              const BscLOp lo = P.lops[pr.l];
-              const CUtensorMap* rmap = P.rops[pr.r].map;
-              const int kbeg = ch.kb1 > 0 ? ch.kb0 : 0, kend = ch.kb1 > 0 ? ch.kb1 : lo.kblocks;
-              for (int kb = kbeg; kb < kend; ++kb, ++it) {
-                const int s = (int)(it % kStagesTC);
-                const uint32_t ph = (it / kStagesTC) & 1;
-                if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err, 12u))) break;
-                mbar_expect_tx(&bars->full[s], 128 * 128 + BN * 128);
-                tma_load_3d(smA + (size_t)s * 128 * 128, lo.map, kb * (I8 ? 128 : 64), I.mt * 128, ch.a,
-                            &bars->full[s]);
-                tma_load_3d(smB + (size_t)s * BN * 128, rmap, kb * (I8 ? 128 : 64), I.nt * BN, ch.b,
-                            &bars->full[s]);
-              }
-            }
+        // software pipeline over the runs: the record of run r + 1 was loaded
+        // during run r - 1 and its tensor maps are prefetched now; the record
+        // of run r + 2 loads while run r streams
+        const int rend = Dd.run0 + Dd.nrun;
+        BscRun ru = P.runs[Dd.run0];
+        BscRun n1 = Dd.nrun > 1 ? P.runs[Dd.run0 + 1] : ru;
+        prefetch_tmap(ru.amap);
+        prefetch_tmap(ru.bmap[BN == 256]);
+        for (int r = Dd.run0; r < rend && ok; ++r) {
+          if (r + 1 < rend) {
+            prefetch_tmap(n1.amap);
+            prefetch_tmap(n1.bmap[BN == 256]);
           }
+          const BscRun n2 = r + 2 < rend ? P.runs[r + 2] : n1;
+          const CUtensorMap* bmap = ru.bmap[BN == 256];
+          for (int kb = ru.kb0; kb < ru.kb1; ++kb, ++it) {
+            const int s = (int)(it % kStages);
+            const uint32_t ph = (it / kStages) & 1;
+            if (!(ok = mbar_wait(&bars->empty[s], ph ^ 1, P.err, 12u))) break;
+            mbar_expect_tx(&bars->full[s], 128 * 128 + BN * 128);
+            tma_load_3d(smA + (size_t)s * 128 * 128, ru.amap, kb * (I8 ? 128 : 64), I.mt * 128, ru.a, &bars->full[s]);
+            tma_load_3d(smB + (size_t)s * BN * 128, bmap, kb * (I8 ? 128 : 64), I.nt * BN, ru.b, &bars->full[s]);
+          }
+          ru = n1;
+          n1 = n2;
         }
       }
     }
@@ -162,38 +167,46 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
         if (!(ok = mbar_wait(&bars->item_full[slot], (k / kBscRing) & 1, P.err, 13u))) break;
         const int cur = bars->ring[slot];
         if (cur < 0) break;
-        const BscItem I = P.items[cur];
-        const BscDBlk Dd = P.dblks[I.d];
-        for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p, ++acc_it) {
-          const BscPass ps = P.passes[p];
+        const BscDBlk Dd = P.dblks[P.items[cur].d];
+        const int rend = Dd.run0 + Dd.nrun;
+        int2 ru = make_int2(0, 0), n1 = ru;  // (kb1 - kb0, flags) of runs r and r + 1
+        {
+          const BscRun x = P.runs[Dd.run0];
+          ru = make_int2(x.kb1 - x.kb0, x.flags);
+          if (Dd.nrun > 1) { const BscRun y = P.runs[Dd.run0 + 1]; n1 = make_int2(y.kb1 - y.kb0, y.flags); }
+        }
+        uint32_t dcol = 0;
+        bool first = true;
+        for (int r = Dd.run0; r < rend && ok; ++r) {
+          int2 n2 = n1;
+          if (r + 2 < rend) { const BscRun z = P.runs[r + 2]; n2 = make_int2(z.kb1 - z.kb0, z.flags); }
           const int a = acc_it & 1;
-          const uint32_t aph = (acc_it >> 1) & 1;
-          if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err, 14u))) break;
-          tc_fence_after();
-          const uint32_t dcol = tmem + (uint32_t)(a * BN);
-          bool first = true;
-          for (int c = ps.chunk0; c < ps.chunk0 + ps.nchunk && ok; ++c) {
-            const BscChunk ch = P.chunks[c];
-            for (int pp = ch.p0; pp < ch.p1 && ok; ++pp) {
-              const int kblocks = P.lops[P.pairs[pp].l].kblocks;
-              const int kbeg = ch.kb1 > 0 ? ch.kb0 : 0, kend = ch.kb1 > 0 ? ch.kb1 : kblocks;
-              for (int kb = kbeg; kb < kend; ++kb, ++it) {
-                const int s = (int)(it % kStagesTC);
-                const uint32_t ph = (it / kStagesTC) & 1;
-                if (!(ok = mbar_wait(&bars->full[s], ph, P.err, 15u))) break;
-                tc_fence_after();
-                const uint32_t sa = smem_u32(smA + (size_t)s * 128 * 128);
-                const uint32_t sb = smem_u32(smB + (size_t)s * BN * 128);
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                  mma<I8>(dcol, sdesc_k128(sa + kk * 32), sdesc_k128(sb + kk * 32), kIdesc,
-                          (first && kk == 0) ? 0u : 1u);
-                first = false;
-                mma_commit(&bars->empty[s]);
-              }
-            }
+          if (ru.y & kBscRunFirst) {
+            const uint32_t aph = (acc_it >> 1) & 1;
+            if (!(ok = mbar_wait(&bars->acc_empty[a], aph ^ 1, P.err, 14u))) break;
+            tc_fence_after();
+            dcol = tmem + (uint32_t)(a * BN);
+            first = true;
           }
-          mma_commit(&bars->acc_full[a]);
+          for (int kb = 0; kb < ru.x; ++kb, ++it) {
+            const int s = (int)(it % kStages);
+            const uint32_t ph = (it / kStages) & 1;
+            if (!(ok = mbar_wait(&bars->full[s], ph, P.err, 15u))) break;
+            tc_fence_after();
+            const uint32_t sa = smem_u32(smA + (size_t)s * 128 * 128);
+            const uint32_t sb = smem_u32(smB + (size_t)s * BN * 128);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+              mma<I8>(dcol, sdesc_k128(sa + kk * 32), sdesc_k128(sb + kk * 32), kIdesc, (first && kk == 0) ? 0u : 1u);
+            first = false;
+            mma_commit(&bars->empty[s]);
+          }
+          if (ok && (ru.y & kBscRunLast)) {
+            mma_commit(&bars->acc_full[a]);
+            ++acc_it;
+          }
+          ru = n1;
+          n1 = n2;
         }
         mbar_arrive(&bars->item_empty[slot]);
       }
@@ -213,13 +226,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) bsc_gemm_kernel(const __grid_co
       const bool mval = m < Dd.M;
       const int64_t dmo = mval ? Dd.dm[m] : 0;
       // all pairs of an output block share its row and column scales
-      const BscPair pr0 = P.pairs[P.chunks[P.passes[Dd.pass0].chunk0].p0];
-      const int re = (EPI == EPI_OZAKI_R) && mval ? P.lops[pr0.l].rowexp[m] : 0;
-      const EpiView V{Dd.D, Dd.dn, P.rops[pr0.r].colexp, Dd.N, P.ar, P.ai, P.br, P.bi, 0};
+      const int re = (EPI == EPI_OZAKI_R) && mval ? Dd.rowexp[m] : 0;
+      const EpiView V{Dd.D, Dd.dn, Dd.colexp, Dd.N, P.ar, P.ai, P.br, P.bi, 0};
       for (int p = Dd.pass0; p < Dd.pass0 + Dd.npass && ok; ++p, ++acc_it) {
         const int a = acc_it & 1;
         const uint32_t aph = (acc_it >> 1) & 1;
-        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 17u))) break;
+        if (!(ok = mbar_wait_warp(&bars->acc_full[a], aph, P.err, 17u, kEpilogueSleepNs))) break;
         tc_fence_after();
         const int shift = (EPI == EPI_OZAKI_R) ? P.passes[p].shift : 0;
         epilogue_pass<BN, EPI>(V, tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * BN), mval, dmo, re, I.nt,

@@ -433,14 +433,30 @@ int orc_tensor_add(const int* cptrn, int dtk, int rank, const int* ldims, void* 
 // tensor_block_scale (tensor_algebra_cpu.F90:1821-1890): d = d*a.
 int orc_scale(int dtk, int64_t vol, void* d, double sr, double si) {
   switch (dtk) {
-    case R4: { float a = (float)cmplx8_to_real8(sr, si); float* D = (float*)d;
-               for (int64_t i = 0; i < vol; ++i) D[i] = D[i] * a; return 0; }
-    case R8: { double a = cmplx8_to_real8(sr, si); double* D = (double*)d;
-               for (int64_t i = 0; i < vol; ++i) D[i] = D[i] * a; return 0; }
-    case C4: { cplx<float> a{(float)sr, (float)si}; cplx<float>* D = (cplx<float>*)d;
-               for (int64_t i = 0; i < vol; ++i) D[i] = cmul(D[i], a); return 0; }
-    case C8: { cplx<double> a{sr, si}; cplx<double>* D = (cplx<double>*)d;
-               for (int64_t i = 0; i < vol; ++i) D[i] = cmul(D[i], a); return 0; }
+    case R4: {
+      const float a = (float)cmplx8_to_real8(sr, si);
+      float* D = (float*)d;
+      for (int64_t i = 0; i < vol; ++i) D[i] = D[i] * a;
+      return 0;
+    }
+    case R8: {
+      const double a = cmplx8_to_real8(sr, si);
+      double* D = (double*)d;
+      for (int64_t i = 0; i < vol; ++i) D[i] = D[i] * a;
+      return 0;
+    }
+    case C4: {
+      const cplx<float> a{(float)sr, (float)si};
+      cplx<float>* D = (cplx<float>*)d;
+      for (int64_t i = 0; i < vol; ++i) D[i] = cmul(D[i], a);
+      return 0;
+    }
+    case C8: {
+      const cplx<double> a{sr, si};
+      cplx<double>* D = (cplx<double>*)d;
+      for (int64_t i = 0; i < vol; ++i) D[i] = cmul(D[i], a);
+      return 0;
+    }
   }
   return 1;
 }
@@ -448,12 +464,29 @@ int orc_scale(int dtk, int64_t vol, void* d, double sr, double si) {
 // tensor_block_init (tensor_algebra_cpu.F90:955-1395): d = val.
 int orc_init(int dtk, int64_t vol, void* d, double vr, double vi) {
   switch (dtk) {
-    case R4: { float* D = (float*)d; float v = (float)vr; for (int64_t i = 0; i < vol; ++i) D[i] = v; return 0; }
-    case R8: { double* D = (double*)d; for (int64_t i = 0; i < vol; ++i) D[i] = vr; return 0; }
-    case C4: { cplx<float>* D = (cplx<float>*)d; cplx<float> v{(float)vr, (float)vi};
-               for (int64_t i = 0; i < vol; ++i) D[i] = v; return 0; }
-    case C8: { cplx<double>* D = (cplx<double>*)d; cplx<double> v{vr, vi};
-               for (int64_t i = 0; i < vol; ++i) D[i] = v; return 0; }
+    case R4: {
+      float* D = (float*)d;
+      const float v = (float)vr;
+      for (int64_t i = 0; i < vol; ++i) D[i] = v;
+      return 0;
+    }
+    case R8: {
+      double* D = (double*)d;
+      for (int64_t i = 0; i < vol; ++i) D[i] = vr;
+      return 0;
+    }
+    case C4: {
+      cplx<float>* D = (cplx<float>*)d;
+      const cplx<float> v{(float)vr, (float)vi};
+      for (int64_t i = 0; i < vol; ++i) D[i] = v;
+      return 0;
+    }
+    case C8: {
+      cplx<double>* D = (cplx<double>*)d;
+      const cplx<double> v{vr, vi};
+      for (int64_t i = 0; i < vol; ++i) D[i] = v;
+      return 0;
+    }
   }
   return 1;
 }

@@ -134,3 +134,43 @@ def test_mismatched_block_is_rejected(xt, dev):
     bad = [(dp, dd, lp, ld, rp, rd), (dp, dd, lp, [x + 1 for x in ld], rp, rd)]
     with pytest.raises(XB.TBError):
         XB.BlockSparsePlan(PATTERN, O.R8, bad, stream=dev.stream())
+
+
+def fixed_problem(xt, dev, dtk, segl, segr, seed):
+    """Every block present, with the given segment extents (L: a b c d; R: c d i j)."""
+    import itertools
+    es = xt.ELEM_BYTES[dtk]
+    L = BS.BlockSparseTensor(segl, list(itertools.product(*[range(len(s)) for s in segl])), es)
+    R = BS.BlockSparseTensor(segr, list(itertools.product(*[range(len(s)) for s in segr])), es)
+    xt.fill_uniform(dtk, L.volume, L.data.data_ptr(), seed + 1, stream=dev.stream())
+    xt.fill_uniform(dtk, R.volume, R.data.data_ptr(), seed + 2, stream=dev.stream())
+    D, tasks, pairs = BS.contraction_tasks(PATTERN, L, R)
+    return L, R, D, tasks
+
+
+@pytest.mark.parametrize("dtk,tol", [(O.R8, 1e-12), (O.R4, 1e-4)])
+@pytest.mark.parametrize("tile_n", [128, 256])
+def test_wide_blocks_and_long_block_sums(xt, dev, dtk, tol, tile_n):
+    """Output blocks wider than one band of N tiles (items are issued band by
+    band), and one output block whose pairs sum 1056 K blocks of INT8 planes
+    (more than one exact INT32 pass holds, so passes end at pair
+    boundaries), against the per-block loop of plain contractions."""
+    import torch
+    probs = [
+        # 11 pairs of K = 96 * 128 into one 128 x 64 block
+        ([[16], [8], [96] * 11, [128]], [[96] * 11, [128], [8], [8]]),
+        # 256 x 3072 blocks: 24 (12) N tiles of 128 (256) columns
+        ([[16], [16], [8], [8, 16]], [[8], [8, 16], [64], [48]]),
+    ]
+    for i, (segl, segr) in enumerate(probs):
+        L, R, D, tasks = fixed_problem(xt, dev, dtk, segl, segr, 40 + i)
+        ref = per_block_loop(xt, dev, dtk, D, tasks, 1.0, False)
+        plan = XB.BlockSparsePlan(PATTERN, dtk, tasks, accumulative=False, plan=xt.make_plan(tile_n=tile_n),
+                                  stream=dev.stream())
+        plan.execute(stream=dev.stream())
+        torch.cuda.synchronize()
+        xt.device_check(dev.stream())
+        assert plan.info().tile_n == tile_n
+        dt = O.NP_DTYPE[dtk]
+        assert O.rel_frobenius(values(D, D.data, dt), values(D, ref, dt)) <= tol, (i, tile_n)
+        plan.close()
