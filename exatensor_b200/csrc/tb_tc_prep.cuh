@@ -727,11 +727,19 @@ __device__ __forceinline__ double u128_to_double(unsigned __int128 x) {
 constexpr int kCrtTableBytes = kMaxModuli * 256 * 16;
 struct alignas(16) CrtEntry { uint64_t lo, hi; };
 
-// Residues of D entry (col, m) from the n planes (independent byte loads).
-__device__ __forceinline__ void crt_load(const CrtParams& P, int64_t col, int64_t m, uint32_t (&r)[kMaxModuli]) {
+// Residues of the four D entries (col, m .. m + 3) from the n planes: one
+// 32-bit load per plane (m a multiple of 4; the planes' row length and plane
+// stride are multiples of 4 bytes, so the words are aligned and lie inside the
+// padded plane even past the last row), byte t of word i holding residue i of
+// row m + t.
+__device__ __forceinline__ void crt_load4(const CrtParams& P, int64_t col, int64_t m, uint32_t (&w)[kMaxModuli]) {
   const uint8_t* rp = P.res + col * P.res_ld + m;
 #pragma unroll
-  for (int i = 0; i < kMaxModuli; ++i) r[i] = i < P.n ? rp[i * P.res_plane] : 0u;
+  for (int i = 0; i < kMaxModuli; ++i) w[i] = i < P.n ? *reinterpret_cast<const uint32_t*>(rp + i * P.res_plane) : 0u;
+}
+__device__ __forceinline__ void crt_byte(const uint32_t (&w)[kMaxModuli], int t, uint32_t (&r)[kMaxModuli]) {
+#pragma unroll
+  for (int i = 0; i < kMaxModuli; ++i) r[i] = __byte_perm(w[i], 0u, 0x4440 + t);
 }
 
 // The exact integer from its residues, in FP64 (about one rounding).
@@ -757,11 +765,12 @@ __device__ __forceinline__ double crt_combine(const CrtParams& P, const CrtEntry
   return neg ? -v : v;
 }
 
-// Each CTA takes groups of residue columns (one real D column, or one complex
-// one: its two residue columns) and each thread, for every row it owns,
-// issues the residue loads of the whole group before combining them.  (Four
-// real columns per group kept more loads in flight but took 113 registers and
-// ran the CCSD-like reconstruction 8% slower: 2.81 ms against 2.59.)
+// Each CTA takes residue columns (one real D column, or one complex one: its
+// two residue columns) and each thread, for every four consecutive rows it
+// owns, loads one word per plane -- the residues of all four rows -- before
+// combining them.  (One byte load per plane and row kept four times as many
+// loads in flight for the same bytes; four columns per group took 113
+// registers and ran 8% slower.)
 template <bool CPLX>
 __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtParams P) {
   extern __shared__ __align__(16) unsigned char crt_smem[];
@@ -778,47 +787,34 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ CrtPar
     tab[e] = t;
   }
   __syncthreads();
-  constexpr int G = 1;              // D entries per group
   constexpr int RC = CPLX ? 2 : 1;  // residue columns per D entry
-  const int64_t ngroups = (P.cols + G - 1) / G;
-  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    int ce[G];
-    int64_t dno[G];
-    bool cok[G];
-    bool any = false;
+  for (int64_t n = blockIdx.x; n < P.cols; n += gridDim.x) {
+    const int ce = P.colexp[CPLX ? 2 * n : n];
+    if (ce >= kNonFiniteExp) continue;  // flagged column: the fix-up's
+    const int64_t dno = P.dn[n];
+    for (int64_t m0 = 4 * (int64_t)threadIdx.x; m0 < P.rows; m0 += 4 * (int64_t)blockDim.x) {
+      uint32_t w[RC][kMaxModuli];
 #pragma unroll
-    for (int c = 0; c < G; ++c) {
-      const int64_t n = grp * G + c;
-      cok[c] = n < P.cols;
-      ce[c] = cok[c] ? P.colexp[CPLX ? 2 * n : n] : 0;
-      cok[c] = cok[c] && ce[c] < kNonFiniteExp;  // flagged column: the fix-up's
-      dno[c] = cok[c] ? P.dn[n] : 0;
-      any = any || cok[c];
-    }
-    if (!any) continue;
-    for (int64_t m = threadIdx.x; m < P.rows; m += blockDim.x) {
-      const int re = P.rowexp[m];
-      if (re >= kNonFiniteExp) continue;  // flagged row: the fix-up's
-      uint32_t r[G * RC][kMaxModuli];
+      for (int j = 0; j < RC; ++j) crt_load4(P, n * RC + j, m0, w[j]);
 #pragma unroll
-      for (int c = 0; c < G; ++c)
-#pragma unroll
-        for (int j = 0; j < RC; ++j) {
-          if (cok[c]) crt_load(P, (grp * G + c) * RC + j, m, r[c * RC + j]);
-        }
-      const int64_t dmo = P.dm[m];
-#pragma unroll
-      for (int c = 0; c < G; ++c) {
-        if (!cok[c]) continue;
-        const int e = re + ce[c] - P.shift;
-        const int64_t o = dmo + dno[c];
+      for (int t = 0; t < 4; ++t) {
+        const int64_t m = m0 + t;
+        if (m >= P.rows) break;
+        const int re = P.rowexp[m];
+        if (re >= kNonFiniteExp) continue;  // flagged row: the fix-up's
+        const int e = re + ce - P.shift;
+        const int64_t o = P.dm[m] + dno;
+        uint32_t r[kMaxModuli];
+        crt_byte(w[0], t, r);
         if constexpr (!CPLX) {
           double* D = (double*)P.D;
-          const double v = P.ar * scale2(crt_combine(P, tab, r[c]), e);
+          const double v = P.ar * scale2(crt_combine(P, tab, r), e);
           D[o] = P.br == 0.0 ? v : fma(P.br, D[o], v);
         } else {
+          const double xr = scale2(crt_combine(P, tab, r), e);
+          crt_byte(w[RC - 1], t, r);
+          const double xi = scale2(crt_combine(P, tab, r), e);
           double2* D = (double2*)P.D;
-          const double xr = scale2(crt_combine(P, tab, r[2 * c]), e), xi = scale2(crt_combine(P, tab, r[2 * c + 1]), e);
           double2 v;
           v.x = P.ar * xr - P.ai * xi;
           v.y = P.ar * xi + P.ai * xr;
