@@ -151,8 +151,8 @@ def fixed_problem(xt, dev, dtk, segl, segr, seed):
 @pytest.mark.parametrize("dtk,tol", [(O.R8, 1e-12), (O.R4, 1e-4)])
 @pytest.mark.parametrize("tile_n", [128, 256])
 def test_wide_blocks_and_long_block_sums(xt, dev, dtk, tol, tile_n):
-    """Output blocks wider than one band of N tiles (items are issued band by
-    band), and one output block whose pairs sum 1056 K blocks of INT8 planes
+    """Output blocks of many N tiles (items are issued N tile by N tile),
+    and one output block whose pairs sum 1056 K blocks of INT8 planes
     (more than one exact INT32 pass holds, so passes end at pair
     boundaries), against the per-block loop of plain contractions."""
     import torch
