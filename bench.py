@@ -705,7 +705,7 @@ SELECTOR_CORPUS = os.path.join(ROOT, "tests", "golden", "selector_corpus.npz")
 
 def selector_case(X):
     """Learned plan selector on the recorded corpus: trained with the
-    library's CUDA kernels on the first 80% of the corpus, judged on the rest
+    library's CUDA kernels on the first 80% of the corpus, evaluated on the rest
     by runtime regret against the best measured plan, beside the size rule;
     plus the selection latency of the host inference used by METHOD_AUTO and
     the GPU batch inference kernel's throughput."""
