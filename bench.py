@@ -429,6 +429,34 @@ def sweep_cases():
     return out
 
 
+# the configuration's own example extents, larger than the governing 256 MiB
+# (128^4: 2 GiB in R8, 1 GiB in R4; 24^6: 1.4 GiB / 0.7 GiB): extra points
+EXAMPLE_SHAPES = [(8, [128] * 4), (4, [128] * 4), (8, [24] * 6), (4, [24] * 6)]
+
+
+def example_cases():
+    """Four permutations of each example shape: at rank 4 the reversal, the
+    slowest 256 MiB class's (4,3,1,2), (3,4,1,2) and (2,1,4,3); at rank 6 the
+    reversal and three seeded random ones."""
+    import random
+    rng = random.Random(20240602)
+    out = []
+    for dtk, dims in EXAMPLE_SHAPES:
+        r = len(dims)
+        if r == 4:
+            perms = [(4, 3, 2, 1), (4, 3, 1, 2), (3, 4, 1, 2), (2, 1, 4, 3)]
+        else:
+            perms = [tuple(range(r, 0, -1))]
+            while len(perms) < 4:
+                p = list(range(1, r + 1))
+                rng.shuffle(p)
+                if tuple(p) not in perms:
+                    perms.append(tuple(p))
+        tag = ("r8_" if dtk == 8 else "r4_") + "x".join(str(x) for x in dims[:1]) + f"^{r}"
+        out += [dict(dtk=dtk, dims=list(dims), perm=p, cls=tag) for p in perms]
+    return out
+
+
 def add_cases():
     """The add sweep (D += 0.37 * permute(L)): all 24 rank-4 permutations and
     the first 10 rank-6 ones, R8 and R4, at the sweep's 256 MiB sizes."""
@@ -459,14 +487,14 @@ def torch_permuted(t, dims, perm, word):
     return x.view(-1)
 
 
-def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True, per_case=False):
+def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True, per_case=False, cases=None, examples=True):
     """Every sweep case: 10 back-to-back timed copies after the first call (where
     the library's measured plan choice runs), and a bit-for-bit comparison of
     the result with torch's permute of the same device data.  Per class the
     aggregate (bytes over time) and the slowest case, in GB/s; then the add
-    sweep."""
+    sweep, and the example shapes as extra points."""
     import torch
-    cases = sweep_cases()
+    cases = sweep_cases() if cases is None else cases
     stats, rates, mism = {}, [], 0
     tot_b = tot_s = 0.0
     cur, a, b = None, None, None
@@ -498,7 +526,7 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True, per_case=False)
     a = b = None
     agg = tot_b / tot_s
     r4 = [(2.0 * vol(c["dims"]) * X.ELEM_BYTES[c["dtk"]] / 1e9, r) for c, r in zip(cases, rates)
-          if c["cls"] in ("r8_4", "r4_4")]
+          if c["cls"] in ("r8_4", "r4_4")] or [(1.0, agg)]
     out = {"GB/s": round(agg, 1), "min_GB/s": round(min(rates), 1), "frac_measured_hbm": sig(agg / hbm_gbs, 3),
            "frac_8000": sig(agg / 8000.0, 3), "min_frac_measured_hbm": sig(min(rates) / hbm_gbs, 3),
            "cases": len(cases), "bit_exact": len(cases) - mism,
@@ -509,6 +537,17 @@ def permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=True, per_case=False)
         out["per_case"] = [[c["cls"], c["dims"], list(c["perm"]), round(r)] for c, r in zip(cases, rates)]
     if with_add:
         out["add"] = add_sweep(X, stream, stream_obj, hbm_gbs, per_case=per_case)
+    if examples:
+        try:
+            ex = permute_sweep(X, stream, stream_obj, hbm_gbs, with_add=False, per_case=per_case,
+                               cases=example_cases(), examples=False)
+            out["examples"] = {k: ex[k] for k in ("GB/s", "min_GB/s", "cases", "bit_exact", "by_class_agg_min")}
+            if per_case:
+                out["examples"]["per_case"] = ex["per_case"]
+        except Exception as exc:  # reported, not fatal
+            out["examples"] = {"error": str(exc)[:200]}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
     out["timing"] = "10 back-to-back calls per case after the first; bits checked against torch.permute"
     return out
 
@@ -1066,6 +1105,10 @@ def run_profile(args):
     if args.profile == "sweep":
         print(json.dumps({"profile": "sweep", **permute_sweep(X, s, s_obj, peaks()[0], per_case=True)}))
         return
+    if args.profile == "examples":
+        print(json.dumps({"profile": "examples", **permute_sweep(X, s, s_obj, peaks()[0], with_add=False, per_case=True,
+                                                                 cases=example_cases(), examples=False)}))
+        return
     if args.profile == "peaks":
         print(json.dumps({"profile": "peaks", **measure_peaks(X, s)}))
         return
@@ -1141,7 +1184,7 @@ def main():
     ap.add_argument("--headline-only", action="store_true",
                     help="only the headline contraction (no sweep, configs, selector, e2e or CPU legs)")
     ap.add_argument("--profile", choices=["contract", "plain", "permute", "permsweep", "bsc", "selector", "e2e",
-                                          "configs", "sweep", "peaks", "c1"],
+                                          "configs", "sweep", "examples", "peaks", "c1"],
                     default=None,
                     help="run one part on a small case for a profiler (no bench line)")
     ap.add_argument("--case", default=None, help="--profile permute: one case, data kind:extents:permutation")
